@@ -1,0 +1,222 @@
+/*
+ * rkdg.h -- C ABI of librkdg.so, the B200 (sm_100a) RKDG residual and
+ * time-step path for the 2D Euler equations on unstructured triangles.
+ *
+ * Every entry point is plain C: pointers, sizes and status codes; nothing
+ * throws across the boundary.  Each function returns RKDG_OK (0) or an
+ * error code; rkdg_last_error() gives the message of the calling thread's
+ * last failure.  Contexts share no global state, so different contexts may
+ * be driven from different host threads.
+ *
+ * Data layout at the boundary is the reference's (multi_gpuRkdg/):
+ *   - DOFs and residuals are four SoA blocks freedom_{rho,rhou,rhov,rhoE},
+ *     each [basis i][cell] with leading dimension ld >= ntri, i.e. the host
+ *     array is [var][basis][ld] (src/cudarkdgsolver.cu:253-264, 336-339);
+ *   - "reference basis" is the reference's per-element orthogonal basis,
+ *     built by Gram-Schmidt in physical coordinates
+ *     (src/triangleinfo.cpp:281-602); basis row 0 is the cell mean;
+ *   - residuals are R = R_volume - R_edge before the mass division, the
+ *     reference's rhs_edge_* (src/kernelfunctions.cu:584-637).
+ * Internally the state lives in HBM in a reference-element orthonormal basis
+ * (RKDG_BASIS_NATIVE), which represents the same functions.
+ */
+#ifndef RKDG_H
+#define RKDG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define RKDG_OK 0
+#define RKDG_ERR_INVALID 1     /* bad argument, mesh or configuration          */
+#define RKDG_ERR_CUDA 2        /* CUDA runtime error (message has details)     */
+#define RKDG_ERR_NOMEM 3       /* device or host allocation failed / budget    */
+#define RKDG_ERR_STATE 4       /* non-physical state (NaN, rho<=0, p<=0) seen  */
+#define RKDG_ERR_NODEVICE 5    /* no usable sm_100 device                      */
+#define RKDG_ERR_IO 6          /* file could not be read or written            */
+#define RKDG_ERR_BUSY 7        /* resource (slot, budget) not available now    */
+
+/* ---- enumerations ------------------------------------------------------ */
+#define RKDG_FLUX_LLF 0        /* local Lax-Friedrichs, alpha from cell means */
+#define RKDG_FLUX_HLLC 1       /* HLLC with Roe-averaged wave speeds          */
+#define RKDG_LIMITER_NONE 0
+#define RKDG_LIMITER_TVB 1     /* TVB minmod on characteristic variables      */
+#define RKDG_FP64 0            /* FP64 state and arithmetic                   */
+#define RKDG_FP32 1            /* FP32 state/arithmetic, FP64 geometry and dt */
+#define RKDG_BASIS_REFERENCE 0 /* the reference's per-element basis           */
+#define RKDG_BASIS_NATIVE 1    /* reference-element orthonormal basis         */
+
+/* boundary tags of an edge; the values are the reference's cell tags
+ * (inc/defines.h:48-54) */
+#define RKDG_BC_INTERIOR 0
+#define RKDG_BC_FARFIELD 1     /* given state (far field / supersonic inflow) */
+#define RKDG_BC_OUTFLOW 2      /* zero-gradient copy                          */
+#define RKDG_BC_REFLECTION 3   /* slip wall                                   */
+
+/* ---- mesh -------------------------------------------------------------- */
+/* A triangle mesh.  Edge k of a triangle is the edge opposite its vertex k
+ * (edge 0 = v1->v2, 1 = v2->v0, 2 = v0->v1), vertices counter-clockwise.
+ * tri_neighbour[3t+k] is the triangle across edge k or -1 on a boundary; if
+ * NULL it is built from shared vertex ids (no periodicity then).  Periodic
+ * meshes pass explicit neighbours and per-triangle (unwrapped) vertices.
+ * bc[3t+k] tags boundary edges (RKDG_BC_*); if NULL, the reference's rule is
+ * used: far field when the reflected (ghost) triangle's barycentre lies
+ * outside |x|,|y| <= 15, else wall (src/unstructuredgrid.cpp:729-760). */
+typedef struct rkdg_mesh_desc {
+    int32_t ntri;
+    int32_t nvert;
+    const double* vertices;      /* [nvert][2]                       */
+    const int32_t* tri_vertex;   /* [ntri][3]                        */
+    const int32_t* tri_neighbour;/* [ntri][3] or NULL                */
+    const int8_t* bc;            /* [ntri][3] or NULL                */
+} rkdg_mesh_desc;
+
+/* Discretisation and physics.  Replaces the compile-time constants of
+ * inc/defines.h:17-32 and the keys of input/main.conf read by
+ * CCUDARkdgSolver::initConfig (src/cudarkdgsolver.cu:93-156). */
+typedef struct rkdg_params {
+    int32_t order;        /* 1 (P1) or 2 (P2)                                */
+    int32_t nq;           /* volume rule: 3 (deg 2), 6 (deg 4) or 7 (deg 5)  */
+    int32_t ng;           /* Gauss points per edge: 2 or 3                   */
+    int32_t flux;         /* RKDG_FLUX_*                                     */
+    int32_t limiter;      /* RKDG_LIMITER_*                                  */
+    int32_t rk;           /* 2 or 3 (SSP Runge-Kutta stages)                 */
+    int32_t precision;    /* RKDG_FP64 or RKDG_FP32                          */
+    int32_t reorder;      /* 1: Morton-reorder elements in HBM for locality  */
+    double gamma;
+    double cfl;           /* dt = cfl / max (|u|+c) perimeter/area           */
+    double tvb_m;         /* TVB constant M                                  */
+    double farfield[4];   /* conservative far-field / inflow state           */
+} rkdg_params;
+
+/* Fills p with the reference's defaults: P2, 7/3-point rules, LLF, no
+ * limiter, SSP-RK3, FP64, gamma 1.4, cfl 0.18 (src/cudarkdgsolver.cu:3-32). */
+void rkdg_default_params(rkdg_params* p);
+
+typedef struct rkdg_ctx rkdg_ctx;
+
+/* ---- lifetime ---------------------------------------------------------- */
+/* Builds connectivity (O(T) edge hashing), FP64 geometry and device arrays,
+ * and binds the calling thread's current CUDA device.
+ * Replaces CCUDARkdgSolver::run + runNext (src/cudarkdgsolver.cu:158-230):
+ * CUnstructuredGrid::initializeGrid/initializeGridNext, initializeTriangleInfos,
+ * markLocalBoundaryTriangles, CCUDAArrays::allocateMemory and
+ * copyTriangleInfosToGPU. */
+int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx** out);
+
+/* Replaces ~CCUDARkdgSolver / ~CCUDAArrays (src/cudaarrays.cpp:227-292). */
+int rkdg_destroy(rkdg_ctx* ctx);
+
+/* Thread-local message of the last failing call on this thread. */
+const char* rkdg_last_error(void);
+
+/* Sizes: triangles, basis functions per variable, device bytes held. */
+int rkdg_get_sizes(const rkdg_ctx* ctx, int32_t* ntri, int32_t* nbasis, size_t* device_bytes);
+
+/* The cudaStream_t (as void*) every call of this context is ordered on. */
+int rkdg_get_stream(const rkdg_ctx* ctx, void** stream);
+
+/* ---- state ------------------------------------------------------------- */
+/* Free-stream initial condition: cell mean = farfield state, higher modes 0.
+ * Replaces CCUDARkdgSolver::initRKDG (src/cudarkdgsolver.cu:326-368). */
+int rkdg_init_freestream(rkdg_ctx* ctx);
+
+/* Host <-> device state in the reference layout [4][nbasis][ld].  basis is
+ * RKDG_BASIS_REFERENCE or RKDG_BASIS_NATIVE.  rkdg_get_state replaces
+ * CCUDARkdgSolver::copyFreedomToHost (src/cudarkdgsolver.cu:253-264). */
+int rkdg_set_state(rkdg_ctx* ctx, const double* U, int32_t ld, int32_t basis);
+int rkdg_get_state(rkdg_ctx* ctx, double* U, int32_t ld, int32_t basis);
+
+/* ---- hot path ---------------------------------------------------------- */
+/* R(U) of the current state, [4][nbasis][ld], not divided by the mass.
+ * One evaluation of the chain calculateConVars -> boundaryCondition ->
+ * calculateVolumeRHS -> calculateLFCoeff -> calculateEdgeFG ->
+ * calculateFlux x2 -> calculateEdgeRHS (src/cudarkdgsolver.cu:382-553,
+ * src/rkdgadvance.cpp:135-159), here one fused kernel. */
+int rkdg_residual(rkdg_ctx* ctx, double* R, int32_t ld, int32_t basis);
+
+/* CFL time step of the current state.  Replaces CCUDARkdgSolver::getTimeStep
+ * + the dt read-back (src/cudarkdgsolver.cu:370-380, src/rkdgadvance.cpp:165-168). */
+int rkdg_compute_dt(rkdg_ctx* ctx, double* dt);
+
+/* Saves the current state as U^n (src/rkdgadvance.cpp:104-107). */
+int rkdg_save_old(rkdg_ctx* ctx);
+
+/* Stage s (0-based) of the SSP-RK scheme against the saved U^n:
+ * R(U) and the stage update fused (and the limiter when enabled).
+ * Replaces one RK iteration of src/rkdgadvance.cpp:132-195
+ * (rkdgStepOne/Two/Three, src/cudarkdgsolver.cu:555-599). */
+int rkdg_stage(rkdg_ctx* ctx, int32_t s, double dt);
+
+/* Applies the TVB limiter to the current state. */
+int rkdg_limit(rkdg_ctx* ctx);
+
+/* One full time step.  dt <= 0 uses the CFL time step of the current state.
+ * dt_used and monitor (max |d rho_mean|, max |d rhoE_mean|, the reference's
+ * residual monitor, src/kernelfunctions.cu:751-867) may be NULL.
+ * Replaces one iteration of RkdgAdvance::advance (src/rkdgadvance.cpp:91-243). */
+int rkdg_step(rkdg_ctx* ctx, double dt, double* dt_used, double* monitor);
+
+/* nsteps steps on the device with no host round trip (CUDA graph of the
+ * whole step), stopping early at t_final when t_final > 0 (dt clipped to
+ * land on it).  Returns the simulated time reached and steps taken.
+ * Replaces RkdgAdvance::advance's loop (src/rkdgadvance.cpp:91-243). */
+int rkdg_advance(rkdg_ctx* ctx, int32_t nsteps, double t_final, double* t, int32_t* steps_done);
+
+/* Simulated time and step counter of the context (device-resident). */
+int rkdg_get_time(rkdg_ctx* ctx, double* t, int32_t* steps);
+int rkdg_set_time(rkdg_ctx* ctx, double t);
+
+/* FP64 conservation totals sum_e area_e * mean_e for the 4 variables,
+ * deterministic (fixed-order reduction). */
+int rkdg_conservation_totals(rkdg_ctx* ctx, double totals[4]);
+
+/* Benchmark helper: launches the fused kernel of stage s (0-based) `reps`
+ * times back to back on the context's stream, writing to a scratch buffer
+ * (the state is not advanced), and returns the mean device time per launch
+ * in milliseconds measured with CUDA events on that stream.  No reference
+ * counterpart (the reference times nothing on the device). */
+int rkdg_time_stage(rkdg_ctx* ctx, int32_t s, int32_t reps, double* ms_per_launch);
+
+/* ---- output ------------------------------------------------------------ */
+/* Writes the cell means as the reference's Tecplot solution.plt
+ * (CCUDARkdgSolver::outputSolution, src/cudarkdgsolver.cu:860-1001). */
+int rkdg_write_solution(rkdg_ctx* ctx, const char* path);
+
+/* ---- mesh files -------------------------------------------------------- */
+/* Reads the reference's mesh set: the mesh configuration file
+ * (trianglenum, verticenum, edgenum and the five file names) and the five
+ * files it names, relative to base_dir (CUnstructuredGrid::initializeGrid
+ * and readers, src/unstructuredgrid.cpp:14-60, 193-288).  Header lines are
+ * detected rather than assumed, so files with or without the '#...' first
+ * line are accepted; ids may be 0- or 1-based.  The arrays are allocated
+ * with malloc and owned by the caller (free with rkdg_free_mesh). */
+int rkdg_read_mesh(const char* base_dir, const char* mesh_conf, rkdg_mesh_desc* out);
+void rkdg_free_mesh(rkdg_mesh_desc* mesh);
+
+/* Host-only: the connectivity rkdg_create would build (no device needed).
+ * neighbour [ntri][3], shared [ntri][3] (the neighbour-local index of each
+ * shared edge, -1 on boundaries: the reference's sharedEdge,
+ * src/unstructuredgrid.cpp:934-976) and bc [ntri][3]; any output may be NULL. */
+int rkdg_build_connectivity(const rkdg_mesh_desc* mesh, int32_t* neighbour, int8_t* shared,
+                            int8_t* bc);
+
+/* Host-only: the locality (Morton) order the context stores elements in;
+ * perm[new] = caller index.  The single-device replacement of the
+ * reference's partition file (src/unstructuredgrid.cpp:290-305). */
+int rkdg_locality_order(const rkdg_mesh_desc* mesh, int32_t* perm);
+
+/* ---- native basis (for projections done by the caller) ----------------- */
+/* Values of the first nbasis native basis functions at npts reference-
+ * element points (xi, eta) on the triangle (0,0),(1,0),(0,1); out[npts][nbasis]. */
+int rkdg_native_basis(int32_t nbasis, int32_t npts, const double* xi, const double* eta,
+                      double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RKDG_H */

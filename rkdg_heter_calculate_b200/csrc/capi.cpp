@@ -1,0 +1,694 @@
+// C ABI of librkdg.so (include/rkdg.h): context lifetime, state transfer,
+// the fused stage path, the device-resident time loop and solution output.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "rkdg_internal.hpp"
+
+namespace rkdg {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+}  // namespace rkdg
+
+using namespace rkdg;
+
+struct rkdg_ctx {
+    rkdg_params p{};
+    int T = 0, ld = 0, nb = 0;
+    int device = 0;
+    int block = 128;
+    HostMesh mesh;  // internal (possibly reordered) order
+    std::vector<double> area;
+    DeviceArrays d;
+    cudaStream_t stream = nullptr;
+    int cur = 0;   // buffer holding the current state
+    int old = 0;   // buffer holding U^n for manual stages
+    bool conv_ready = false;
+    bool wave_valid = false;
+    bool have_state = false;
+    cudaGraphExec_t graph = nullptr;
+    StepCtl* h_ctl = nullptr;  // pinned mirror of the device control block
+};
+
+namespace {
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return RKDG_OK;
+    } catch (const Error& e) {
+        set_error(e.msg);
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_error("host allocation failed");
+        return RKDG_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        set_error(e.what());
+        return RKDG_ERR_INVALID;
+    }
+}
+
+void* dev_alloc(rkdg_ctx* c, size_t bytes) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error{RKDG_ERR_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " +
+                                        cudaGetErrorString(e)};
+    }
+    c->d.bytes += bytes;
+    return p;
+}
+
+size_t state_bytes(const rkdg_ctx* c) {
+    const size_t word = c->p.precision == RKDG_FP32 ? 4 : 8;
+    return (size_t)4 * c->nb * word * c->ld;
+}
+
+void check_params(const rkdg_params& p) {
+    if (p.order != 1 && p.order != 2) throw Error{RKDG_ERR_INVALID, "order must be 1 or 2"};
+    if (p.nq != 3 && p.nq != 6 && p.nq != 7) throw Error{RKDG_ERR_INVALID, "nq must be 3, 6 or 7"};
+    if (p.ng != 2 && p.ng != 3) throw Error{RKDG_ERR_INVALID, "ng must be 2 or 3"};
+    if (p.flux != RKDG_FLUX_LLF && p.flux != RKDG_FLUX_HLLC) throw Error{RKDG_ERR_INVALID, "unknown flux"};
+    if (p.limiter != RKDG_LIMITER_NONE && p.limiter != RKDG_LIMITER_TVB)
+        throw Error{RKDG_ERR_INVALID, "unknown limiter"};
+    if (p.rk != 2 && p.rk != 3) throw Error{RKDG_ERR_INVALID, "rk must be 2 or 3"};
+    if (p.precision != RKDG_FP64 && p.precision != RKDG_FP32)
+        throw Error{RKDG_ERR_INVALID, "unknown precision"};
+    if (!(p.gamma > 1.0) || !(p.cfl > 0.0)) throw Error{RKDG_ERR_INVALID, "gamma > 1 and cfl > 0 required"};
+    if (!(p.farfield[0] > 0.0)) throw Error{RKDG_ERR_INVALID, "far-field density must be positive"};
+}
+
+void sync(rkdg_ctx* c) { RKDG_CUDA_TRY(cudaStreamSynchronize(c->stream)); }
+
+void ensure_staging(rkdg_ctx* c) {
+    if (!c->d.staging) c->d.staging = (double*)dev_alloc(c, sizeof(double) * 4 * c->nb * (size_t)c->T);
+}
+
+void ensure_conversion(rkdg_ctx* c) {
+    if (c->conv_ready) return;
+    HostGeometry g = build_geometry(c->mesh, c->p.order, true, false);
+    c->d.conv_in = (double*)dev_alloc(c, sizeof(double) * 36 * (size_t)c->T);
+    c->d.conv_out = (double*)dev_alloc(c, sizeof(double) * 36 * (size_t)c->T);
+    RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.conv_in, g.conv_in.data(), sizeof(double) * 36 * c->T,
+                                  cudaMemcpyHostToDevice, c->stream));
+    RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.conv_out, g.conv_out.data(), sizeof(double) * 36 * c->T,
+                                  cudaMemcpyHostToDevice, c->stream));
+    sync(c);
+    c->conv_ready = true;
+}
+
+void pull_ctl(rkdg_ctx* c) {
+    RKDG_CUDA_TRY(cudaMemcpyAsync(c->h_ctl, c->d.ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, c->stream));
+    sync(c);
+}
+
+void push_ctl(rkdg_ctx* c) {
+    RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.ctl, c->h_ctl, sizeof(StepCtl), cudaMemcpyHostToDevice, c->stream));
+}
+
+void require_state(const rkdg_ctx* c) {
+    if (!c->have_state) throw Error{RKDG_ERR_INVALID, "no state: call rkdg_set_state or rkdg_init_freestream"};
+}
+
+// moves the current state into buffer 0 (the step path keeps U^n there)
+void normalise_buffers(rkdg_ctx* c) {
+    if (c->cur != 0) {
+        RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.U[0], c->d.U[c->cur], state_bytes(c),
+                                      cudaMemcpyDeviceToDevice, c->stream));
+        c->cur = 0;
+    }
+    c->old = 0;
+}
+
+void ensure_wave(rkdg_ctx* c) {
+    if (c->wave_valid) return;
+    launch_wave(c->T, c->ld, c->d.U[c->cur], c->p.order, c->p.precision, c->d.jinv, c->p.gamma,
+                c->d.ctl, c->stream);
+    c->wave_valid = true;
+}
+
+StageArgs base_args(const rkdg_ctx* c) {
+    StageArgs a{};
+    a.T = c->T;
+    a.ld = c->ld;
+    a.jinv = c->d.jinv;
+    a.conn = c->d.conn;
+    a.ctl = c->d.ctl;
+    a.gamma = c->p.gamma;
+    for (int v = 0; v < 4; ++v) a.far[v] = c->p.farfield[v];
+    return a;
+}
+
+void stage_coeffs(int rk, int s, double& a, double& b) {
+    if (s == 0) {
+        a = 0, b = 1;
+    } else if (rk == 2) {
+        a = 0.5, b = 0.5;
+    } else if (s == 1) {
+        a = 0.75, b = 0.25;
+    } else {
+        a = 1.0 / 3.0, b = 2.0 / 3.0;
+    }
+}
+
+void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out) {
+    StageArgs a = base_args(c);
+    stage_coeffs(c->p.rk, s, a.a, a.b);
+    a.U = c->d.U[in];
+    a.U0 = s == 0 ? nullptr : c->d.U[u0];
+    a.Unew = c->d.U[out];
+    a.last_stage = s == c->p.rk - 1;
+    launch_stage(a, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
+    if (c->p.limiter == RKDG_LIMITER_TVB)
+        launch_limiter(c->T, c->ld, c->d.U[out], c->d.conn, c->d.lim, c->d.jinv, c->p.order,
+                       c->p.nq, c->p.ng, c->p.precision, c->p.gamma, c->p.farfield, c->p.tvb_m,
+                       c->stream);
+}
+
+// one full step on the stream with the state in buffer 0 (graph-capturable)
+void enqueue_step(rkdg_ctx* c) {
+    launch_step_begin(c->d.ctl, c->stream);
+    if (c->p.rk == 3) {
+        launch_one_stage(c, 0, 0, 0, 1);
+        launch_one_stage(c, 1, 1, 0, 2);
+        launch_one_stage(c, 2, 2, 0, 0);
+    } else {
+        launch_one_stage(c, 0, 0, 0, 1);
+        launch_one_stage(c, 1, 1, 0, 0);
+    }
+}
+
+void check_error_flag(rkdg_ctx* c) {
+    if (c->h_ctl->error) throw Error{RKDG_ERR_STATE, "non-physical state (NaN or non-positive density/pressure)"};
+}
+
+void destroy_ctx(rkdg_ctx* c) {
+    if (!c) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(c->device);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void* p : {c->d.U[0], c->d.U[1], c->d.U[2]}) cudaFree(p);
+    cudaFree(c->d.jinv);
+    cudaFree(c->d.conn);
+    cudaFree(c->d.lim);
+    cudaFree(c->d.perm);
+    cudaFree(c->d.conv_in);
+    cudaFree(c->d.conv_out);
+    cudaFree(c->d.staging);
+    cudaFree(c->d.partial);
+    cudaFree(c->d.ctl);
+    if (c->h_ctl) cudaFreeHost(c->h_ctl);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    cudaSetDevice(prev);
+    delete c;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rkdg_last_error(void) { return g_last_error.c_str(); }
+
+void rkdg_default_params(rkdg_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->order = 2;
+    p->nq = 7;
+    p->ng = 3;
+    p->flux = RKDG_FLUX_LLF;
+    p->limiter = RKDG_LIMITER_NONE;
+    p->rk = 3;
+    p->precision = RKDG_FP64;
+    p->reorder = 1;
+    p->gamma = 1.4;
+    p->cfl = 0.18;
+    p->tvb_m = 50.0;
+    // the reference's default far field: Mach 0.4, alpha 5 deg, rho = p = 1
+    // (src/cudarkdgsolver.cu:3-32, src/rkdgadvance.cpp:31-34)
+    const double ut = std::sqrt(1.4) * 0.4, al = 5.0 * std::atan(1.0) * 4 / 180;
+    p->farfield[0] = 1.0;
+    p->farfield[1] = ut * std::cos(al);
+    p->farfield[2] = ut * std::sin(al);
+    p->farfield[3] = 0.5 * ut * ut + 1.0 / 0.4;
+}
+
+int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx** out) {
+    rkdg_ctx* c = nullptr;
+    int rc = guarded([&] {
+        if (!mesh || !params || !out) throw Error{RKDG_ERR_INVALID, "rkdg_create: null argument"};
+        *out = nullptr;
+        check_params(*params);
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Error{RKDG_ERR_NODEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e)};
+        }
+        cudaDeviceProp prop;
+        RKDG_CUDA_TRY(cudaGetDeviceProperties(&prop, dev));
+        if (prop.major < 10)
+            throw Error{RKDG_ERR_NODEVICE, "device " + std::to_string(dev) + " is sm_" +
+                                               std::to_string(prop.major * 10 + prop.minor) +
+                                               "; this library is built for sm_100a"};
+        c = new rkdg_ctx();
+        c->device = dev;
+        c->p = *params;
+        c->nb = params->order == 1 ? 3 : 6;
+        HostMesh m = build_mesh(*mesh);
+        if (params->reorder) m = permute_mesh(m, morton_order(m));
+        c->mesh = std::move(m);
+        c->T = c->mesh.T;
+        c->ld = (c->T + 127) / 128 * 128;
+        HostGeometry g = build_geometry(c->mesh, params->order, false,
+                                        params->limiter == RKDG_LIMITER_TVB);
+        c->area = g.area;
+        RKDG_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        RKDG_CUDA_TRY(cudaMallocHost(&c->h_ctl, sizeof(StepCtl)));
+        std::memset(c->h_ctl, 0, sizeof(StepCtl));
+        upload_tables(params->nq, params->ng);
+
+        const int T = c->T, ld = c->ld;
+        for (int b = 0; b < 3; ++b) {
+            c->d.U[b] = dev_alloc(c, state_bytes(c));
+            RKDG_CUDA_TRY(cudaMemsetAsync(c->d.U[b], 0, state_bytes(c), c->stream));
+        }
+        std::vector<double> jp((size_t)4 * ld, 0.0);
+        for (int t = 0; t < T; ++t) {
+            jp[2 * (size_t)t] = g.jinv[4 * (size_t)t];
+            jp[2 * (size_t)t + 1] = g.jinv[4 * (size_t)t + 1];
+            jp[2 * ((size_t)ld + t)] = g.jinv[4 * (size_t)t + 2];
+            jp[2 * ((size_t)ld + t) + 1] = g.jinv[4 * (size_t)t + 3];
+        }
+        c->d.jinv = (double*)dev_alloc(c, sizeof(double) * jp.size());
+        RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.jinv, jp.data(), sizeof(double) * jp.size(),
+                                      cudaMemcpyHostToDevice, c->stream));
+        std::vector<int4> cn(ld, make_int4(-1, -1, -1, 0));
+        for (int t = 0; t < T; ++t)
+            cn[t] = make_int4(c->mesh.nbr[3 * t], c->mesh.nbr[3 * t + 1], c->mesh.nbr[3 * t + 2],
+                              (int)pack_info(&c->mesh.shared[3 * t], &c->mesh.bc[3 * t]));
+        c->d.conn = (int4*)dev_alloc(c, sizeof(int4) * ld);
+        RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.conn, cn.data(), sizeof(int4) * ld, cudaMemcpyHostToDevice,
+                                      c->stream));
+        c->d.perm = (int32_t*)dev_alloc(c, sizeof(int32_t) * T);
+        RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.perm, c->mesh.perm.data(), sizeof(int32_t) * T,
+                                      cudaMemcpyHostToDevice, c->stream));
+        if (params->limiter == RKDG_LIMITER_TVB) {
+            c->d.lim = (double*)dev_alloc(c, sizeof(double) * g.lim.size());
+            RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.lim, g.lim.data(), sizeof(double) * g.lim.size(),
+                                          cudaMemcpyHostToDevice, c->stream));
+        }
+        c->d.partial = (double*)dev_alloc(c, sizeof(double) * 4 * (totals_partial_count(T) + 1));
+        c->d.ctl = (StepCtl*)dev_alloc(c, sizeof(StepCtl));
+        c->h_ctl->cfl = params->cfl;
+        push_ctl(c);
+        sync(c);
+        *out = c;
+    });
+    if (rc != RKDG_OK && c) destroy_ctx(c);
+    return rc;
+}
+
+int rkdg_destroy(rkdg_ctx* ctx) {
+    return guarded([&] { destroy_ctx(ctx); });
+}
+
+int rkdg_get_sizes(const rkdg_ctx* c, int32_t* ntri, int32_t* nbasis, size_t* bytes) {
+    return guarded([&] {
+        if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        if (ntri) *ntri = c->T;
+        if (nbasis) *nbasis = c->nb;
+        if (bytes) *bytes = c->d.bytes;
+    });
+}
+
+int rkdg_get_stream(const rkdg_ctx* c, void** stream) {
+    return guarded([&] {
+        if (!c || !stream) throw Error{RKDG_ERR_INVALID, "null argument"};
+        *stream = (void*)c->stream;
+    });
+}
+
+int rkdg_set_state(rkdg_ctx* c, const double* U, int32_t ld, int32_t basis) {
+    return guarded([&] {
+        if (!c || !U || ld < c->T) throw Error{RKDG_ERR_INVALID, "rkdg_set_state: bad arguments"};
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        ensure_staging(c);
+        if (basis == RKDG_BASIS_REFERENCE) ensure_conversion(c);
+        else if (basis != RKDG_BASIS_NATIVE) throw Error{RKDG_ERR_INVALID, "unknown basis"};
+        RKDG_CUDA_TRY(cudaMemcpy2DAsync(c->d.staging, sizeof(double) * c->T, U, sizeof(double) * ld,
+                                        sizeof(double) * c->T, 4 * c->nb, cudaMemcpyHostToDevice,
+                                        c->stream));
+        c->cur = 0;
+        c->old = 0;
+        launch_import(c->T, c->ld, c->d.staging, c->T,
+                      basis == RKDG_BASIS_REFERENCE ? c->d.conv_in : nullptr, c->d.perm, c->d.U[0],
+                      c->p.order, c->p.precision, c->stream);
+        c->have_state = true;
+        c->wave_valid = false;
+        ensure_wave(c);
+        sync(c);
+    });
+}
+
+int rkdg_init_freestream(rkdg_ctx* c) {
+    return guarded([&] {
+        if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        std::vector<double> U((size_t)4 * c->nb * c->T, 0.0);
+        for (int v = 0; v < 4; ++v)
+            std::fill(U.begin() + (size_t)v * c->nb * c->T, U.begin() + ((size_t)v * c->nb + 1) * c->T,
+                      c->p.farfield[v]);
+        int rc = rkdg_set_state(c, U.data(), c->T, RKDG_BASIS_NATIVE);
+        if (rc != RKDG_OK) throw Error{rc, g_last_error};
+    });
+}
+
+int rkdg_get_state(rkdg_ctx* c, double* U, int32_t ld, int32_t basis) {
+    return guarded([&] {
+        if (!c || !U || ld < c->T) throw Error{RKDG_ERR_INVALID, "rkdg_get_state: bad arguments"};
+        require_state(c);
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        ensure_staging(c);
+        if (basis == RKDG_BASIS_REFERENCE) ensure_conversion(c);
+        else if (basis != RKDG_BASIS_NATIVE) throw Error{RKDG_ERR_INVALID, "unknown basis"};
+        launch_export(c->T, c->ld, c->d.U[c->cur], basis == RKDG_BASIS_REFERENCE ? c->d.conv_out : nullptr,
+                      c->d.perm, c->d.staging, c->T, c->p.order, c->p.precision, 0, c->d.jinv,
+                      c->stream);
+        RKDG_CUDA_TRY(cudaMemcpy2DAsync(U, sizeof(double) * ld, c->d.staging, sizeof(double) * c->T,
+                                        sizeof(double) * c->T, 4 * c->nb, cudaMemcpyDeviceToHost,
+                                        c->stream));
+        sync(c);
+    });
+}
+
+int rkdg_residual(rkdg_ctx* c, double* R, int32_t ld, int32_t basis) {
+    return guarded([&] {
+        if (!c || !R || ld < c->T) throw Error{RKDG_ERR_INVALID, "rkdg_residual: bad arguments"};
+        require_state(c);
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        ensure_staging(c);
+        if (basis == RKDG_BASIS_REFERENCE) ensure_conversion(c);
+        else if (basis != RKDG_BASIS_NATIVE) throw Error{RKDG_ERR_INVALID, "unknown basis"};
+        // scratch: a buffer that holds neither the current nor the saved state
+        int scratch = 0;
+        while (scratch == c->cur || scratch == c->old) ++scratch;
+        StageArgs a = base_args(c);
+        a.U = c->d.U[c->cur];
+        a.U0 = nullptr;
+        a.Unew = c->d.U[scratch];
+        a.a = 0;
+        a.b = 1;
+        launch_residual(a, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
+        launch_export(c->T, c->ld, c->d.U[scratch], basis == RKDG_BASIS_REFERENCE ? c->d.conv_in : nullptr,
+                      c->d.perm, c->d.staging, c->T, c->p.order, c->p.precision, 1, c->d.jinv,
+                      c->stream);
+        RKDG_CUDA_TRY(cudaMemcpy2DAsync(R, sizeof(double) * ld, c->d.staging, sizeof(double) * c->T,
+                                        sizeof(double) * c->T, 4 * c->nb, cudaMemcpyDeviceToHost,
+                                        c->stream));
+        sync(c);
+    });
+}
+
+int rkdg_compute_dt(rkdg_ctx* c, double* dt) {
+    return guarded([&] {
+        if (!c || !dt) throw Error{RKDG_ERR_INVALID, "rkdg_compute_dt: bad arguments"};
+        require_state(c);
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        c->wave_valid = false;
+        ensure_wave(c);
+        pull_ctl(c);
+        check_error_flag(c);
+        double w;
+        std::memcpy(&w, &c->h_ctl->wave_bits, sizeof(w));
+        *dt = c->p.cfl / w;
+    });
+}
+
+int rkdg_save_old(rkdg_ctx* c) {
+    return guarded([&] {
+        if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        require_state(c);
+        c->old = c->cur;
+    });
+}
+
+int rkdg_stage(rkdg_ctx* c, int32_t s, double dt) {
+    return guarded([&] {
+        if (!c || s < 0 || s >= c->p.rk) throw Error{RKDG_ERR_INVALID, "rkdg_stage: bad stage index"};
+        require_state(c);
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        // the stage reads dt from the control block
+        pull_ctl(c);
+        c->h_ctl->dt = dt;
+        c->h_ctl->done = 0;
+        push_ctl(c);
+        int out;
+        if (s == c->p.rk - 1 && s > 0 && c->old != c->cur) {
+            out = c->old;  // in place on U^n: each element reads its own U^n first
+        } else {
+            out = 0;
+            while (out == c->cur || out == c->old) ++out;
+        }
+        launch_one_stage(c, s, c->cur, c->old, out);
+        c->cur = out;
+        // only a last stage leaves the CFL measure of the state it wrote
+        c->wave_valid = (s == c->p.rk - 1);
+        sync(c);
+    });
+}
+
+int rkdg_limit(rkdg_ctx* c) {
+    return guarded([&] {
+        if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        require_state(c);
+        if (c->p.limiter != RKDG_LIMITER_TVB) throw Error{RKDG_ERR_INVALID, "context created without limiter"};
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        launch_limiter(c->T, c->ld, c->d.U[c->cur], c->d.conn, c->d.lim, c->d.jinv, c->p.order,
+                       c->p.nq, c->p.ng, c->p.precision, c->p.gamma, c->p.farfield, c->p.tvb_m,
+                       c->stream);
+        sync(c);
+    });
+}
+
+int rkdg_step(rkdg_ctx* c, double dt, double* dt_used, double* monitor) {
+    return guarded([&] {
+        if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        require_state(c);
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        normalise_buffers(c);
+        ensure_wave(c);
+        pull_ctl(c);
+        c->h_ctl->dt_fixed = dt > 0 ? dt : 0.0;
+        c->h_ctl->t_final = 0.0;
+        c->h_ctl->done = 0;
+        push_ctl(c);
+        enqueue_step(c);
+        c->wave_valid = true;
+        pull_ctl(c);
+        check_error_flag(c);
+        if (dt_used) *dt_used = c->h_ctl->dt;
+        if (monitor) {
+            std::memcpy(&monitor[0], &c->h_ctl->mon_bits[0], sizeof(double));
+            std::memcpy(&monitor[1], &c->h_ctl->mon_bits[1], sizeof(double));
+        }
+    });
+}
+
+int rkdg_advance(rkdg_ctx* c, int32_t nsteps, double t_final, double* t, int32_t* steps_done) {
+    return guarded([&] {
+        if (!c || nsteps < 0) throw Error{RKDG_ERR_INVALID, "rkdg_advance: bad arguments"};
+        require_state(c);
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        normalise_buffers(c);
+        ensure_wave(c);
+        pull_ctl(c);
+        const int step0 = c->h_ctl->step;
+        c->h_ctl->dt_fixed = 0.0;
+        c->h_ctl->t_final = t_final > 0 ? t_final : 0.0;
+        c->h_ctl->done = 0;
+        push_ctl(c);
+        if (!c->graph) {
+            cudaGraph_t g;
+            RKDG_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueue_step(c);
+            } catch (...) {
+                cudaStreamEndCapture(c->stream, &g);
+                throw;
+            }
+            RKDG_CUDA_TRY(cudaStreamEndCapture(c->stream, &g));
+            RKDG_CUDA_TRY(cudaGraphInstantiate(&c->graph, g, 0));
+            cudaGraphDestroy(g);
+        }
+        // launch in chunks; with a final time, stop once the device says done
+        int left = nsteps;
+        const int chunk = t_final > 0 ? 64 : nsteps;
+        while (left > 0) {
+            int n = std::min(left, chunk > 0 ? chunk : 1);
+            for (int i = 0; i < n; ++i) RKDG_CUDA_TRY(cudaGraphLaunch(c->graph, c->stream));
+            left -= n;
+            if (t_final > 0 && left > 0) {
+                pull_ctl(c);
+                if (c->h_ctl->done || c->h_ctl->error) break;
+            }
+        }
+        c->wave_valid = true;
+        pull_ctl(c);
+        check_error_flag(c);
+        if (t) *t = c->h_ctl->t;
+        if (steps_done) *steps_done = c->h_ctl->step - step0;
+    });
+}
+
+int rkdg_time_stage(rkdg_ctx* c, int32_t s, int32_t reps, double* ms) {
+    return guarded([&] {
+        if (!c || !ms || s < 0 || s >= c->p.rk || reps <= 0)
+            throw Error{RKDG_ERR_INVALID, "rkdg_time_stage: bad arguments"};
+        require_state(c);
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        normalise_buffers(c);
+        pull_ctl(c);
+        if (!(c->h_ctl->dt > 0)) c->h_ctl->dt = 1e-6;
+        c->h_ctl->done = 0;
+        push_ctl(c);
+        // input buffer 0 (the state), U^n = buffer 0, output buffer 1: a
+        // stage that writes neither its input nor U^n, so launches repeat
+        StageArgs a = base_args(c);
+        stage_coeffs(c->p.rk, s, a.a, a.b);
+        a.U = c->d.U[0];
+        a.U0 = s == 0 ? nullptr : c->d.U[0];
+        a.Unew = c->d.U[1];
+        a.last_stage = 0;
+        cudaEvent_t e0, e1;
+        RKDG_CUDA_TRY(cudaEventCreate(&e0));
+        RKDG_CUDA_TRY(cudaEventCreate(&e1));
+        launch_stage(a, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
+        RKDG_CUDA_TRY(cudaEventRecord(e0, c->stream));
+        for (int i = 0; i < reps; ++i)
+            launch_stage(a, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
+        RKDG_CUDA_TRY(cudaEventRecord(e1, c->stream));
+        RKDG_CUDA_TRY(cudaEventSynchronize(e1));
+        float t = 0;
+        RKDG_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *ms = (double)t / reps;
+    });
+}
+
+int rkdg_get_time(rkdg_ctx* c, double* t, int32_t* steps) {
+    return guarded([&] {
+        if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        pull_ctl(c);
+        if (t) *t = c->h_ctl->t;
+        if (steps) *steps = c->h_ctl->step;
+    });
+}
+
+int rkdg_set_time(rkdg_ctx* c, double t) {
+    return guarded([&] {
+        if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        pull_ctl(c);
+        c->h_ctl->t = t;
+        c->h_ctl->done = 0;
+        push_ctl(c);
+        sync(c);
+    });
+}
+
+int rkdg_conservation_totals(rkdg_ctx* c, double totals[4]) {
+    return guarded([&] {
+        if (!c || !totals) throw Error{RKDG_ERR_INVALID, "bad arguments"};
+        require_state(c);
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        const int n = totals_partial_count(c->T);
+        double* out4 = c->d.partial + (size_t)4 * n;
+        launch_totals(c->T, c->ld, c->d.U[c->cur], c->p.order, c->p.precision, c->d.jinv,
+                      c->d.partial, out4, c->stream);
+        RKDG_CUDA_TRY(cudaMemcpyAsync(totals, out4, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        sync(c);
+    });
+}
+
+int rkdg_write_solution(rkdg_ctx* c, const char* path) {
+    return guarded([&] {
+        if (!c || !path) throw Error{RKDG_ERR_INVALID, "bad arguments"};
+        require_state(c);
+        const int T = c->T, nb = c->nb;
+        std::vector<double> U((size_t)4 * nb * T);
+        int rc = rkdg_get_state(c, U.data(), T, RKDG_BASIS_NATIVE);
+        if (rc != RKDG_OK) throw Error{rc, g_last_error};
+        std::ofstream f(path);
+        if (!f) throw Error{RKDG_ERR_IO, std::string("cannot open ") + path};
+        // CCUDARkdgSolver::outputSolution (src/cudarkdgsolver.cu:860-1001):
+        // Tecplot FETRIANGLE, BLOCK packing, nodal X/Y then cell-centred
+        // rho, u, v, p, Ma, FLAG; six values per line with a line break after
+        // the first value; 1-based connectivity.
+        const double gamma = c->p.gamma;
+        const std::vector<double>& V = c->mesh.vertices;
+        const int vnum = (int)(V.size() / 2);
+        auto mean = [&](int v, int t) { return U[(size_t)v * nb * T + t]; };
+        f << "TITLE=RKDG" << std::endl;
+        f << "VARIABLES=X , Y , rho , u , v , p, Ma , FLAG" << std::endl;
+        f << "ZONE T= T1 N= " << vnum << " , E= " << T << " , ZONETYPE=FETRIANGLE" << std::endl;
+        f << "DATAPACKING=BLOCK" << std::endl;
+        f << "VARLOCATION=([1-2]=NODAL,[3-8]=CELLCENTERED)" << std::endl;
+        f << "DT=(SINGLE SINGLE SINGLE SINGLE SINGLE SINGLE SINGLE SINGLE)" << std::endl;
+        for (int i = 0; i < vnum; ++i) {
+            f << V[2 * i] << "  ";
+            if (i % 6 == 0) f << std::endl;
+        }
+        for (int i = 0; i < vnum; ++i) {
+            f << V[2 * i + 1] << "  ";
+            if (i % 6 == 0) f << std::endl;
+        }
+        f << std::endl;
+        auto column = [&](auto value) {
+            for (int i = 0; i < T; ++i) {
+                f << value(i) << "  ";
+                if (i % 6 == 0) f << std::endl;
+            }
+            f << std::endl;
+        };
+        column([&](int i) { return mean(0, i); });
+        column([&](int i) { return mean(1, i) / mean(0, i); });
+        column([&](int i) { return mean(2, i) / mean(0, i); });
+        auto pres = [&](int i) {
+            double rho = mean(0, i), u = mean(1, i) / rho, v = mean(2, i) / rho;
+            return (gamma - 1) * (mean(3, i) - 0.5 * rho * (u * u + v * v));
+        };
+        column(pres);
+        column([&](int i) {
+            double rho = mean(0, i), u = mean(1, i) / rho, v = mean(2, i) / rho;
+            return std::sqrt(u * u + v * v) / std::sqrt(gamma * pres(i) / rho);
+        });
+        for (int i = 0; i < T; ++i) {
+            f << "1" << "  ";
+            if (i % 6 == 0) f << std::endl;
+        }
+        f << std::endl;
+        const std::vector<int32_t>& tv = c->mesh.tri_vertex;
+        for (int i = 0; i < T; ++i)
+            f << tv[3 * i] + 1 << "    " << tv[3 * i + 1] + 1 << "    " << tv[3 * i + 2] + 1 << std::endl;
+        if (!f) throw Error{RKDG_ERR_IO, std::string("write failed: ") + path};
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,890 @@
+// sm_100a kernels of the RKDG residual and time-step path.
+//
+// One fused kernel per Runge-Kutta stage replaces the reference's chain of
+// nine launches per stage (src/kernelfunctions.cu:84-748): each thread owns
+// one triangle, evaluates its state at the volume points, projects the
+// contravariant Euler fluxes onto the basis gradients, evaluates the
+// Riemann flux at the Gauss points of its three edges against the
+// neighbours' traces (owner-computes: deterministic, no atomics), and
+// applies the SSP-RK stage update in its epilogue.  Nothing but the state is
+// written to HBM: traces, fluxes and residuals live in registers.
+//
+// HBM layout (element-interleaved packs for 128-bit accesses):
+//   state  : row r = 4*i + v (basis i, variable v), packs of W = 16/sizeof(Real)
+//            rows; pack p of element e at ((p*ld + e) * W)  -> one 16-byte
+//            load per pack, a warp reads 512 contiguous bytes;
+//   jinv   : FP64 rows of J^-1, [2][ld] double2 = (r0x, r0y), (r1x, r1y);
+//   conn   : [ld] int4 = (neighbour 0, 1, 2, packed shared-edge/boundary tags).
+// The basis is orthonormal under the area average on the reference
+// triangle, so M = area * I and every geometric factor of the stage comes
+// from J^-1: the scaled normals N_k/area are 2(r0+r1), -2 r0, -2 r1.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "rkdg_internal.hpp"
+
+namespace rkdg {
+
+// -------------------------------------------------------------- tables --
+template <typename Real>
+struct Tab {
+    Real vphi[kMaxNQ][kMaxNB];
+    Real vdxi[kMaxNQ][kMaxNB];  // weight * d psi / d xi
+    Real veta[kMaxNQ][kMaxNB];  // weight * d psi / d eta
+    Real ephi[3][kMaxNG][kMaxNB];
+    Real ew[kMaxNG];
+    Real mphi[3][2];
+    Real minv[2][3];
+};
+
+// rule configurations: index = 2 * (nq == 7 ? 0 : nq == 6 ? 1 : 2) + (ng == 3 ? 0 : 1)
+constexpr int kNumCfg = 6;
+__constant__ Tab<double> c_tab_d[kNumCfg];
+__constant__ Tab<float> c_tab_f[kNumCfg];
+
+__host__ __device__ constexpr int cfg_index(int nq, int ng) {
+    return 2 * (nq == 7 ? 0 : (nq == 6 ? 1 : 2)) + (ng == 3 ? 0 : 1);
+}
+
+template <typename Real>
+__device__ __forceinline__ const Tab<Real>& tab(int c);
+template <>
+__device__ __forceinline__ const Tab<double>& tab<double>(int c) { return c_tab_d[c]; }
+template <>
+__device__ __forceinline__ const Tab<float>& tab<float>(int c) { return c_tab_f[c]; }
+
+void upload_tables(int nq, int ng) {
+    RuleTables t = make_tables(nq, ng);
+    Tab<double> d{};
+    Tab<float> f{};
+    for (int q = 0; q < kMaxNQ; ++q)
+        for (int i = 0; i < kMaxNB; ++i) {
+            d.vphi[q][i] = t.vphi[q][i];
+            d.vdxi[q][i] = t.vdxi_w[q][i];
+            d.veta[q][i] = t.veta_w[q][i];
+            f.vphi[q][i] = (float)t.vphi[q][i];
+            f.vdxi[q][i] = (float)t.vdxi_w[q][i];
+            f.veta[q][i] = (float)t.veta_w[q][i];
+        }
+    for (int k = 0; k < 3; ++k)
+        for (int g = 0; g < kMaxNG; ++g)
+            for (int i = 0; i < kMaxNB; ++i) {
+                d.ephi[k][g][i] = t.ephi[k][g][i];
+                f.ephi[k][g][i] = (float)t.ephi[k][g][i];
+            }
+    for (int g = 0; g < kMaxNG; ++g) {
+        d.ew[g] = t.ew[g];
+        f.ew[g] = (float)t.ew[g];
+    }
+    for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 2; ++j) {
+            d.mphi[k][j] = t.mphi[k][j];
+            f.mphi[k][j] = (float)t.mphi[k][j];
+            d.minv[j][k] = t.minv[j][k];
+            f.minv[j][k] = (float)t.minv[j][k];
+        }
+    const int c = cfg_index(nq, ng);
+    RKDG_CUDA_TRY(cudaMemcpyToSymbol(c_tab_d, &d, sizeof(d), sizeof(d) * c));
+    RKDG_CUDA_TRY(cudaMemcpyToSymbol(c_tab_f, &f, sizeof(f), sizeof(f) * c));
+}
+
+// --------------------------------------------------------- state packs --
+template <typename Real, int NB>
+__device__ __forceinline__ void load_state(const Real* __restrict__ U, int ld, int e,
+                                           Real u[NB][4]) {
+    if constexpr (sizeof(Real) == 8) {
+        const double2* p = reinterpret_cast<const double2*>(U);
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+            double2 a = __ldg(p + (size_t)(2 * i) * ld + e);
+            double2 b = __ldg(p + (size_t)(2 * i + 1) * ld + e);
+            u[i][0] = a.x;
+            u[i][1] = a.y;
+            u[i][2] = b.x;
+            u[i][3] = b.y;
+        }
+    } else {
+        const float4* p = reinterpret_cast<const float4*>(U);
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+            float4 a = __ldg(p + (size_t)i * ld + e);
+            u[i][0] = a.x;
+            u[i][1] = a.y;
+            u[i][2] = a.z;
+            u[i][3] = a.w;
+        }
+    }
+}
+
+template <typename Real, int NB>
+__device__ __forceinline__ void load_mean(const Real* __restrict__ U, int ld, int e, Real m[4]) {
+    Real u[1][4];
+    load_state<Real, 1>(U, ld, e, u);
+    m[0] = u[0][0], m[1] = u[0][1], m[2] = u[0][2], m[3] = u[0][3];
+}
+
+template <typename Real, int NB>
+__device__ __forceinline__ void store_state(Real* __restrict__ U, int ld, int e,
+                                            const Real u[NB][4]) {
+    if constexpr (sizeof(Real) == 8) {
+        double2* p = reinterpret_cast<double2*>(U);
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+            p[(size_t)(2 * i) * ld + e] = make_double2(u[i][0], u[i][1]);
+            p[(size_t)(2 * i + 1) * ld + e] = make_double2(u[i][2], u[i][3]);
+        }
+    } else {
+        float4* p = reinterpret_cast<float4*>(U);
+#pragma unroll
+        for (int i = 0; i < NB; ++i) p[(size_t)i * ld + e] = make_float4(u[i][0], u[i][1], u[i][2], u[i][3]);
+    }
+}
+
+// ------------------------------------------------------------- physics --
+// Ghost state of a boundary edge (the reference's boundaryCondition kernel,
+// src/kernelfunctions.cu:184-268, applied inline): 1 far field, 2 outflow
+// copy, 3 slip wall mirroring the momentum about the unit normal.
+template <typename Real>
+__device__ __forceinline__ void ghost(int tag, const Real u[4], const Real far[4], Real nx, Real ny,
+                                      Real g[4]) {
+    if (tag == RKDG_BC_FARFIELD) {
+        g[0] = far[0], g[1] = far[1], g[2] = far[2], g[3] = far[3];
+    } else if (tag == RKDG_BC_OUTFLOW) {
+        g[0] = u[0], g[1] = u[1], g[2] = u[2], g[3] = u[3];
+    } else {
+        g[0] = u[0];
+        g[3] = u[3];
+        g[1] = u[1] * (ny * ny - nx * nx) - Real(2) * nx * ny * u[2];
+        g[2] = u[2] * (nx * nx - ny * ny) - Real(2) * nx * ny * u[1];
+    }
+}
+
+// Normal Euler flux through the scaled normal (Nx, Ny): F Nx + G Ny.
+template <typename Real>
+__device__ __forceinline__ void normal_flux(const Real u[4], Real Nx, Real Ny, Real gm1, Real f[4],
+                                            Real& p) {
+    Real ri = Real(1) / u[0];
+    Real vx = u[1] * ri, vy = u[2] * ri;
+    p = gm1 * (u[3] - Real(0.5) * (u[1] * vx + u[2] * vy));
+    Real qn = vx * Nx + vy * Ny;
+    f[0] = u[0] * qn;
+    f[1] = u[1] * qn + p * Nx;
+    f[2] = u[2] * qn + p * Ny;
+    f[3] = (u[3] + p) * qn;
+}
+
+// HLLC through the unit normal (nx, ny) (Toro, Riemann Solvers and Numerical
+// Methods for Fluid Dynamics, 3rd ed., sec. 10.4) with the Roe-average wave
+// speeds of Batten, Clarke, Lambert & Causon (SIAM J. Sci. Comput. 18, 1997).
+template <typename Real>
+__device__ __forceinline__ void hllc(const Real uL[4], const Real uR[4], Real nx, Real ny,
+                                     Real gamma, Real f[4]) {
+    const Real gm1 = gamma - Real(1);
+    Real rL = uL[0], rR = uR[0];
+    Real iL = Real(1) / rL, iR = Real(1) / rR;
+    Real vxL = uL[1] * iL, vyL = uL[2] * iL, vxR = uR[1] * iR, vyR = uR[2] * iR;
+    Real pL = gm1 * (uL[3] - Real(0.5) * rL * (vxL * vxL + vyL * vyL));
+    Real pR = gm1 * (uR[3] - Real(0.5) * rR * (vxR * vxR + vyR * vyR));
+    Real qL = vxL * nx + vyL * ny, qR = vxR * nx + vyR * ny;
+    Real cL = sqrt(gamma * pL * iL), cR = sqrt(gamma * pR * iR);
+    Real HL = (uL[3] + pL) * iL, HR = (uR[3] + pR) * iR;
+    Real sL = sqrt(rL), sR = sqrt(rR), is = Real(1) / (sL + sR);
+    Real vxt = (sL * vxL + sR * vxR) * is, vyt = (sL * vyL + sR * vyR) * is;
+    Real Ht = (sL * HL + sR * HR) * is;
+    Real qt = vxt * nx + vyt * ny;
+    Real ct = sqrt(gm1 * (Ht - Real(0.5) * (vxt * vxt + vyt * vyt)));
+    Real SL = fmin(qL - cL, qt - ct), SR = fmax(qR + cR, qt + ct);
+    Real SM = (pR - pL + rL * qL * (SL - qL) - rR * qR * (SR - qR)) /
+              (rL * (SL - qL) - rR * (SR - qR));
+    if (SL >= Real(0)) {
+        f[0] = rL * qL;
+        f[1] = uL[1] * qL + pL * nx;
+        f[2] = uL[2] * qL + pL * ny;
+        f[3] = (uL[3] + pL) * qL;
+    } else if (SR <= Real(0)) {
+        f[0] = rR * qR;
+        f[1] = uR[1] * qR + pR * nx;
+        f[2] = uR[2] * qR + pR * ny;
+        f[3] = (uR[3] + pR) * qR;
+    } else {
+        const bool left = SM >= Real(0);
+        const Real* u = left ? uL : uR;
+        Real r = left ? rL : rR, ir = left ? iL : iR, vx = left ? vxL : vxR, vy = left ? vyL : vyR;
+        Real p = left ? pL : pR, q = left ? qL : qR, S = left ? SL : SR;
+        Real k = r * (S - q) / (S - SM);
+        Real us0 = k, us1 = k * (vx + (SM - q) * nx), us2 = k * (vy + (SM - q) * ny);
+        Real us3 = k * (u[3] * ir + (SM - q) * (SM + p / (r * (S - q))));
+        f[0] = r * q + S * (us0 - u[0]);
+        f[1] = u[1] * q + p * nx + S * (us1 - u[1]);
+        f[2] = u[2] * q + p * ny + S * (us2 - u[2]);
+        f[3] = (u[3] + p) * q + S * (us3 - u[3]);
+    }
+}
+
+// ---------------------------------------------------------- reductions --
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide max of up to three non-negative doubles, then one atomicMax
+// each on their bit patterns (ordered like the values for x >= 0; a NaN
+// compares above +inf and so propagates).
+__device__ __forceinline__ void block_max3_atomic(double a, double b, double c,
+                                                  unsigned long long* da,
+                                                  unsigned long long* db,
+                                                  unsigned long long* dc) {
+    __shared__ double sm[3][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    a = warp_max(a);
+    b = warp_max(b);
+    c = warp_max(c);
+    if (lane == 0) {
+        sm[0][wid] = a;
+        sm[1][wid] = b;
+        sm[2][wid] = c;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        a = lane < nw ? sm[0][lane] : 0.0;
+        b = lane < nw ? sm[1][lane] : 0.0;
+        c = lane < nw ? sm[2][lane] : 0.0;
+        a = warp_max(a);
+        b = warp_max(b);
+        c = warp_max(c);
+        if (lane == 0) {
+            if (da) atomicMax(da, (unsigned long long)__double_as_longlong(a));
+            if (db) atomicMax(db, (unsigned long long)__double_as_longlong(b));
+            if (dc) atomicMax(dc, (unsigned long long)__double_as_longlong(c));
+        }
+    }
+}
+
+// (|u| + c) * perimeter / area of a cell mean (src/kernelfunctions.cu:19-25),
+// with perimeter / area = sum_k |N_k / area|; FP64.
+__device__ __forceinline__ double wave_measure(double rho, double mu, double mv, double E,
+                                               double gamma, double2 r0, double2 r1, bool& bad) {
+    double u = mu / rho, v = mv / rho;
+    double p = (gamma - 1) * (E - 0.5 * rho * (u * u + v * v));
+    double a = sqrt(gamma * p / rho);
+    double l0 = 2.0 * hypot(r0.x + r1.x, r0.y + r1.y);
+    double l1 = 2.0 * hypot(r0.x, r0.y);
+    double l2 = 2.0 * hypot(r1.x, r1.y);
+    bad = !(rho > 0.0) || !(p > 0.0);
+    double w = (sqrt(u * u + v * v) + a) * (l0 + l1 + l2);
+    return bad ? __longlong_as_double(0x7ff8000000000000LL) : w;
+}
+
+// ------------------------------------------------------------ the stage --
+enum { MODE_STAGE = 0, MODE_RESIDUAL = 1 };
+
+template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE>
+__global__ void __launch_bounds__(128) stage_kernel(const StageArgs a) {
+    constexpr int CFG = cfg_index(NQ, NG);
+    const Tab<Real>& tb = tab<Real>(CFG);
+    __shared__ Real s_ephi[3][NG][NB];  // neighbour-side edge table (runtime edge index)
+    for (int x = threadIdx.x; x < 3 * NG * NB; x += blockDim.x) {
+        int k = x / (NG * NB), g = (x / NB) % NG, i = x % NB;
+        s_ephi[k][g][i] = tb.ephi[k][g][i];
+    }
+    __syncthreads();
+    if (MODE == MODE_STAGE && a.ctl->done) return;
+
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = e < a.T;
+    const int ee = active ? e : 0;  // inactive lanes still join the block reduction
+
+    const Real* __restrict__ U = static_cast<const Real*>(a.U);
+    Real u[NB][4];
+    load_state<Real, NB>(U, a.ld, ee, u);
+    const double2* jinv2 = reinterpret_cast<const double2*>(a.jinv);
+    const double2 r0 = __ldg(jinv2 + ee), r1 = __ldg(jinv2 + a.ld + ee);
+    const int4 cn = __ldg(a.conn + ee);
+    const Real gamma = (Real)a.gamma, gm1 = gamma - Real(1);
+    const Real j00 = (Real)r0.x, j01 = (Real)r0.y, j10 = (Real)r1.x, j11 = (Real)r1.y;
+
+    Real R[NB][4];
+#pragma unroll
+    for (int i = 0; i < NB; ++i)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) R[i][v] = Real(0);
+
+    // ---- volume integral: sum_q w_q (J^-1 (F, G)) . grad_xi psi_i
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        Real w[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            Real s = Real(0);
+#pragma unroll
+            for (int i = 0; i < NB; ++i) s += tb.vphi[q][i] * u[i][v];
+            w[v] = s;
+        }
+        Real ri = Real(1) / w[0];
+        Real vx = w[1] * ri, vy = w[2] * ri;
+        Real p = gm1 * (w[3] - Real(0.5) * (w[1] * vx + w[2] * vy));
+        Real F[4] = {w[1], w[1] * vx + p, w[2] * vx, (w[3] + p) * vx};
+        Real G[4] = {w[2], w[1] * vy, w[2] * vy + p, (w[3] + p) * vy};
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            Real fx = j00 * F[v] + j01 * G[v];
+            Real fy = j10 * F[v] + j11 * G[v];
+#pragma unroll
+            for (int i = 1; i < NB; ++i) R[i][v] += fx * tb.vdxi[q][i] + fy * tb.veta[q][i];
+        }
+    }
+
+    // ---- edge integrals (owner computes all three of its edges)
+    Real far[4] = {(Real)a.far[0], (Real)a.far[1], (Real)a.far[2], (Real)a.far[3]};
+    Real mL[4] = {u[0][0], u[0][1], u[0][2], u[0][3]};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int ne = k == 0 ? cn.x : (k == 1 ? cn.y : cn.z);
+        const unsigned info = (unsigned)cn.w;
+        const int se = (info >> (2 * k)) & 3u;
+        const int tag = (info >> (6 + 2 * k)) & 3u;
+        // scaled normal N_k / area and its length, FP64 geometry
+        double Nxd, Nyd;
+        if (k == 0) {
+            Nxd = 2.0 * (r0.x + r1.x);
+            Nyd = 2.0 * (r0.y + r1.y);
+        } else if (k == 1) {
+            Nxd = -2.0 * r0.x;
+            Nyd = -2.0 * r0.y;
+        } else {
+            Nxd = -2.0 * r1.x;
+            Nyd = -2.0 * r1.y;
+        }
+        const double lend = sqrt(Nxd * Nxd + Nyd * Nyd);
+        const Real Nx = (Real)Nxd, Ny = (Real)Nyd, len = (Real)lend;
+        const Real nx = (Real)(Nxd / lend), ny = (Real)(Nyd / lend);
+
+        Real un[NB][4];
+        Real mR[4];
+        const bool interior = ne >= 0;
+        if (interior) {
+            load_state<Real, NB>(U, a.ld, ne, un);
+            mR[0] = un[0][0], mR[1] = un[0][1], mR[2] = un[0][2], mR[3] = un[0][3];
+        } else {
+#pragma unroll
+            for (int i = 0; i < NB; ++i)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) un[i][v] = Real(0);
+            ghost<Real>(tag, mL, far, nx, ny, mR);
+        }
+        // LLF coefficient from the average of the two cell means
+        // (src/kernelfunctions.cu:370-387), scaled by |N|
+        Real alpha = Real(0);
+        if (FLUX == RKDG_FLUX_LLF) {
+            Real rho = Real(0.5) * (mL[0] + mR[0]);
+            Real ir = Real(1) / rho;
+            Real vx = Real(0.5) * (mL[1] + mR[1]) * ir;
+            Real vy = Real(0.5) * (mL[2] + mR[2]) * ir;
+            Real E = Real(0.5) * (mL[3] + mR[3]);
+            Real p = gm1 * (E - Real(0.5) * rho * (vx * vx + vy * vy));
+            alpha = fabs(vx * Nx + vy * Ny) + sqrt(gamma * p * ir) * len;
+        }
+#pragma unroll
+        for (int g = 0; g < NG; ++g) {
+            Real uL[4], uR[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                Real s = Real(0);
+#pragma unroll
+                for (int i = 0; i < NB; ++i) s += tb.ephi[k][g][i] * u[i][v];
+                uL[v] = s;
+            }
+            if (interior) {
+                // the neighbour's point NG-1-g on its edge se pairs with ours
+                // (src/kernelfunctions.cu:545-549)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    Real s = Real(0);
+#pragma unroll
+                    for (int i = 0; i < NB; ++i) s += s_ephi[se][NG - 1 - g][i] * un[i][v];
+                    uR[v] = s;
+                }
+            } else {
+                ghost<Real>(tag, uL, far, nx, ny, uR);
+            }
+            Real fh[4];
+            if (FLUX == RKDG_FLUX_LLF) {
+                Real fL[4], fR[4], pL, pR;
+                normal_flux<Real>(uL, Nx, Ny, gm1, fL, pL);
+                normal_flux<Real>(uR, Nx, Ny, gm1, fR, pR);
+#pragma unroll
+                for (int v = 0; v < 4; ++v) fh[v] = Real(0.5) * (fL[v] + fR[v] - alpha * (uR[v] - uL[v]));
+            } else {
+                hllc<Real>(uL, uR, nx, ny, gamma, fh);
+#pragma unroll
+                for (int v = 0; v < 4; ++v) fh[v] *= len;
+            }
+            const Real wg = tb.ew[g];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                Real c = wg * fh[v];
+#pragma unroll
+                for (int i = 0; i < NB; ++i) R[i][v] -= c * tb.ephi[k][g][i];
+            }
+        }
+    }
+
+    Real* __restrict__ Uout = static_cast<Real*>(a.Unew);
+    if (MODE == MODE_RESIDUAL) {
+        if (active) store_state<Real, NB>(Uout, a.ld, e, R);
+        return;
+    }
+
+    // ---- stage update: Unew = a U0 + b (U + dt L(U))
+    const double dtd = a.ctl->dt;
+    const Real dt = (Real)dtd, ca = (Real)a.a, cb = (Real)a.b;
+    Real u0m[4] = {Real(0), Real(0), Real(0), Real(0)};
+    if (a.U0 != nullptr) {
+        Real u0[NB][4];
+        load_state<Real, NB>(static_cast<const Real*>(a.U0), a.ld, ee, u0);
+#pragma unroll
+        for (int i = 0; i < NB; ++i)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) R[i][v] = ca * u0[i][v] + cb * (u[i][v] + dt * R[i][v]);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) u0m[v] = u0[0][v];
+    } else {
+#pragma unroll
+        for (int i = 0; i < NB; ++i)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) R[i][v] = cb * (u[i][v] + dt * R[i][v]);
+    }
+    if (active) store_state<Real, NB>(Uout, a.ld, e, R);
+
+    if (a.last_stage) {
+        // next step's CFL measure, residual monitor, state check (FP64)
+        double wv = 0.0, m0 = 0.0, m1 = 0.0;
+        if (active) {
+            bool bad;
+            wv = wave_measure((double)R[0][0], (double)R[0][1], (double)R[0][2], (double)R[0][3],
+                              a.gamma, r0, r1, bad);
+            if (bad) atomicOr(&a.ctl->error, 1);
+            m0 = fabs((double)R[0][0] - (double)u0m[0]);
+            m1 = fabs((double)R[0][3] - (double)u0m[3]);
+        }
+        block_max3_atomic(wv, m0, m1, &a.ctl->wave_bits, &a.ctl->mon_bits[0], &a.ctl->mon_bits[1]);
+    }
+}
+
+// CFL measure of the current state (first step, rkdg_compute_dt).
+template <typename Real>
+__global__ void __launch_bounds__(256) wave_kernel(int T, int ld, const Real* __restrict__ U,
+                                                   const double* __restrict__ jinv, double gamma,
+                                                   StepCtl* ctl) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double w = 0.0;
+    if (e < T) {
+        Real m[4];
+        load_mean<Real, 1>(U, ld, e, m);
+        const double2* j2 = reinterpret_cast<const double2*>(jinv);
+        bool bad;
+        w = wave_measure((double)m[0], (double)m[1], (double)m[2], (double)m[3], gamma, j2[e],
+                         j2[ld + e], bad);
+        if (bad) atomicOr(&ctl->error, 1);
+    }
+    block_max3_atomic(w, 0.0, 0.0, &ctl->wave_bits, nullptr, nullptr);
+}
+
+// dt of the step: CFL (or fixed), clipped to land on t_final; advances t.
+__global__ void step_begin_kernel(StepCtl* ctl) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (ctl->done) return;
+    double dt = ctl->dt_fixed > 0 ? ctl->dt_fixed : ctl->cfl / __longlong_as_double((long long)ctl->wave_bits);
+    bool last = false;
+    if (ctl->t_final > 0) {
+        double rem = ctl->t_final - ctl->t;
+        if (!(rem > 0)) {
+            ctl->done = 1;
+            return;
+        }
+        if (dt >= rem) {
+            dt = rem;
+            last = true;
+        }
+    }
+    if (!(dt > 0) || !isfinite(dt)) {  // non-physical state: stop, report
+        ctl->error |= 1;
+        ctl->done = 1;
+        return;
+    }
+    ctl->dt = dt;
+    ctl->t = last ? ctl->t_final : ctl->t + dt;
+    ctl->step += 1;
+    ctl->wave_bits = 0ull;
+    ctl->mon_bits[0] = 0ull;
+    ctl->mon_bits[1] = 0ull;
+}
+
+// ------------------------------------------------------------ limiter --
+// TVB minmod on characteristic variables for the P1 part (Cockburn & Shu,
+// J. Comput. Phys. 141 (1998) 199-224, sec. 2.4/3.3).  In place: only
+// modes >= 1 change, and neighbours read only cell means.
+template <typename Real, int NB>
+__global__ void __launch_bounds__(128) limiter_kernel(int T, int ld, Real* __restrict__ U,
+                                                      const int4* __restrict__ conn,
+                                                      const double* __restrict__ lim,
+                                                      const double* __restrict__ jinv,
+                                                      double gammad, double f0, double f1,
+                                                      double f2, double f3, double tvb_m, int cfg) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= T) return;
+    const Tab<Real>& tb = tab<Real>(cfg);
+    const double2* j2 = reinterpret_cast<const double2*>(jinv);
+    const double2 r0 = __ldg(j2 + e), r1 = __ldg(j2 + ld + e);
+    Real u[3][4];
+    load_state<Real, 3>(U, ld, e, u);
+    const int4 cn = __ldg(conn + e);
+    const Real gamma = (Real)gammad;
+    const Real far[4] = {(Real)f0, (Real)f1, (Real)f2, (Real)f3};
+    Real mean[4] = {u[0][0], u[0][1], u[0][2], u[0][3]};
+    Real nbm[3][4], tilde[3][4];
+    const double* L = lim + (size_t)18 * e;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        int ne = k == 0 ? cn.x : (k == 1 ? cn.y : cn.z);
+        if (ne >= 0) {
+            load_mean<Real, 1>(U, ld, ne, nbm[k]);
+        } else {
+            // ghost mean across a boundary edge, mirrored about the unit
+            // normal of edge k (N_k / area = 2(r0+r1), -2 r0, -2 r1)
+            int tag = ((unsigned)cn.w >> (6 + 2 * k)) & 3u;
+            double Nx = k == 0 ? r0.x + r1.x : (k == 1 ? -r0.x : -r1.x);
+            double Ny = k == 0 ? r0.y + r1.y : (k == 1 ? -r0.y : -r1.y);
+            double il = 1.0 / sqrt(Nx * Nx + Ny * Ny);
+            ghost<Real>(tag, mean, far, (Real)(Nx * il), (Real)(Ny * il), nbm[k]);
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) tilde[k][v] = tb.mphi[k][0] * u[1][v] + tb.mphi[k][1] * u[2][v];
+    }
+    bool limited = false;
+    Real delta[3][4];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const Real al = (Real)L[6 * k], be = (Real)L[6 * k + 1];
+        const int j = (int)L[6 * k + 2];
+        const Real nx = (Real)L[6 * k + 3], ny = (Real)L[6 * k + 4];
+        const Real thr = (Real)(tvb_m * L[6 * k + 5]);
+        Real dbar[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            Real nj = j == 0 ? nbm[0][v] : (j == 1 ? nbm[1][v] : nbm[2][v]);
+            dbar[v] = al * (nbm[k][v] - mean[v]) + be * (nj - mean[v]);
+        }
+        // eigenvectors of the Euler flux Jacobian in direction n at the mean
+        Real rho = mean[0], ir = Real(1) / rho, vx = mean[1] * ir, vy = mean[2] * ir;
+        Real p = (gamma - Real(1)) * (mean[3] - Real(0.5) * rho * (vx * vx + vy * vy));
+        Real c = sqrt(gamma * p * ir), H = (mean[3] + p) * ir;
+        Real q = vx * nx + vy * ny, qt = -vx * ny + vy * nx, k2 = Real(0.5) * (vx * vx + vy * vy);
+        Real b1 = (gamma - Real(1)) / (c * c), b2 = b1 * k2, ic = Real(1) / c;
+        Real Lm[4][4] = {{Real(0.5) * (b2 + q * ic), Real(0.5) * (-b1 * vx - nx * ic),
+                          Real(0.5) * (-b1 * vy - ny * ic), Real(0.5) * b1},
+                         {Real(1) - b2, b1 * vx, b1 * vy, -b1},
+                         {-qt, -ny, nx, Real(0)},
+                         {Real(0.5) * (b2 - q * ic), Real(0.5) * (-b1 * vx + nx * ic),
+                          Real(0.5) * (-b1 * vy + ny * ic), Real(0.5) * b1}};
+        Real Rc[4][4] = {{Real(1), vx - c * nx, vy - c * ny, H - q * c},
+                         {Real(1), vx, vy, k2},
+                         {Real(0), -ny, nx, qt},
+                         {Real(1), vx + c * nx, vy + c * ny, H + q * c}};  // rows = right vectors
+        Real wl[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            Real wt = Lm[r][0] * tilde[k][0] + Lm[r][1] * tilde[k][1] + Lm[r][2] * tilde[k][2] +
+                      Lm[r][3] * tilde[k][3];
+            Real wd = Real(1.5) * (Lm[r][0] * dbar[0] + Lm[r][1] * dbar[1] + Lm[r][2] * dbar[2] +
+                                   Lm[r][3] * dbar[3]);
+            Real out;
+            if (fabs(wt) <= thr) {
+                out = wt;
+            } else {
+                out = (wt > Real(0) && wd > Real(0)) ? fmin(wt, wd)
+                      : (wt < Real(0) && wd < Real(0)) ? fmax(wt, wd)
+                                                       : Real(0);
+                if (out != wt) limited = true;
+            }
+            wl[r] = out;
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+            delta[k][v] = Rc[0][v] * wl[0] + Rc[1][v] * wl[1] + Rc[2][v] * wl[2] + Rc[3][v] * wl[3];
+    }
+    if (!limited) return;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        Real s = delta[0][v] + delta[1][v] + delta[2][v];
+        if (s != Real(0)) {
+            Real pos = Real(0), neg = Real(0);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                pos += fmax(Real(0), delta[k][v]);
+                neg += fmax(Real(0), -delta[k][v]);
+            }
+            Real tp = pos > Real(0) ? fmin(Real(1), neg / pos) : Real(1);
+            Real tn = neg > Real(0) ? fmin(Real(1), pos / neg) : Real(1);
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                delta[k][v] = tp * fmax(Real(0), delta[k][v]) - tn * fmax(Real(0), -delta[k][v]);
+        }
+    }
+    Real out[NB][4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        out[0][v] = mean[v];
+        out[1][v] = tb.minv[0][0] * delta[0][v] + tb.minv[0][1] * delta[1][v] + tb.minv[0][2] * delta[2][v];
+        out[2][v] = tb.minv[1][0] * delta[0][v] + tb.minv[1][1] * delta[1][v] + tb.minv[1][2] * delta[2][v];
+#pragma unroll
+        for (int i = 3; i < NB; ++i) out[i][v] = Real(0);
+    }
+    store_state<Real, NB>(U, ld, e, out);
+}
+
+// ---------------------------------------------------- basis conversion --
+// Caller layout [4][NB][ldh] FP64 (caller element order) <-> HBM packs
+// (internal order), with an optional per-element basis change.
+template <typename Real, int NB>
+__global__ void import_kernel(int T, int ld, const double* __restrict__ st, int ldh,
+                              const double* __restrict__ conv, const int32_t* __restrict__ perm,
+                              Real* __restrict__ U) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= T) return;
+    const int c = perm ? perm[e] : e;
+    double a[NB][4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+        for (int i = 0; i < NB; ++i) a[i][v] = st[((size_t)v * NB + i) * ldh + c];
+    Real b[NB][4];
+    if (conv) {
+        const double* C = conv + (size_t)36 * e;
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                double s = 0;
+#pragma unroll
+                for (int i = 0; i < NB; ++i) s += a[i][v] * C[6 * i + j];
+                b[j][v] = (Real)s;
+            }
+    } else {
+#pragma unroll
+        for (int i = 0; i < NB; ++i)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) b[i][v] = (Real)a[i][v];
+    }
+    store_state<Real, NB>(U, ld, e, b);
+}
+
+template <typename Real, int NB>
+__global__ void export_kernel(int T, int ld, const Real* __restrict__ U,
+                              const double* __restrict__ conv, const int32_t* __restrict__ perm,
+                              double* __restrict__ st, int ldh, int residual_scale,
+                              const double* __restrict__ jinv) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= T) return;
+    const int c = perm ? perm[e] : e;
+    Real b[NB][4];
+    load_state<Real, NB>(U, ld, e, b);
+    double scale = 1.0;
+    if (residual_scale) {  // area = 1 / (2 det J^-1)
+        const double2* j2 = reinterpret_cast<const double2*>(jinv);
+        double2 r0 = j2[e], r1 = j2[ld + e];
+        scale = 0.5 / (r0.x * r1.y - r0.y * r1.x);
+    }
+#pragma unroll
+    for (int i = 0; i < NB; ++i)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            double s;
+            if (conv) {
+                const double* M = conv + (size_t)36 * e + 6 * i;
+                s = 0;
+#pragma unroll
+                for (int j = 0; j < NB; ++j) s += M[j] * (double)b[j][v];
+            } else {
+                s = (double)b[i][v];
+            }
+            st[((size_t)v * NB + i) * ldh + c] = scale * s;
+        }
+}
+
+// --------------------------------------------------- conservation totals --
+constexpr int kTotBlock = 256;
+int totals_partial_count(int T) { return (T + kTotBlock - 1) / kTotBlock; }
+
+template <typename Real>
+__global__ void __launch_bounds__(kTotBlock) totals_partial_kernel(int T, int ld,
+                                                                   const Real* __restrict__ U,
+                                                                   const double* __restrict__ jinv,
+                                                                   double* __restrict__ partial) {
+    __shared__ double s[4][kTotBlock];
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double v4[4] = {0, 0, 0, 0};
+    if (e < T) {
+        Real m[4];
+        load_mean<Real, 1>(U, ld, e, m);
+        const double2* j2 = reinterpret_cast<const double2*>(jinv);
+        double2 r0 = j2[e], r1 = j2[ld + e];
+        double area = 0.5 / (r0.x * r1.y - r0.y * r1.x);
+        for (int v = 0; v < 4; ++v) v4[v] = area * (double)m[v];
+    }
+    for (int v = 0; v < 4; ++v) s[v][threadIdx.x] = v4[v];
+    __syncthreads();
+    for (int o = kTotBlock / 2; o > 0; o >>= 1) {  // fixed-order tree: deterministic
+        if (threadIdx.x < o)
+            for (int v = 0; v < 4; ++v) s[v][threadIdx.x] += s[v][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int v = 0; v < 4; ++v) partial[(size_t)4 * blockIdx.x + v] = s[v][0];
+}
+
+__global__ void __launch_bounds__(kTotBlock) totals_final_kernel(int n, const double* __restrict__ partial,
+                                                                 double* __restrict__ out) {
+    __shared__ double s[4][kTotBlock];
+    double acc[4] = {0, 0, 0, 0};
+    for (int i = threadIdx.x; i < n; i += kTotBlock)
+        for (int v = 0; v < 4; ++v) acc[v] += partial[(size_t)4 * i + v];
+    for (int v = 0; v < 4; ++v) s[v][threadIdx.x] = acc[v];
+    __syncthreads();
+    for (int o = kTotBlock / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            for (int v = 0; v < 4; ++v) s[v][threadIdx.x] += s[v][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int v = 0; v < 4; ++v) out[v] = s[v][0];
+}
+
+// ----------------------------------------------------------- launchers --
+namespace {
+
+template <typename Real, int NB, int NQ, int NG, int MODE>
+void dispatch_flux(const StageArgs& a, int flux, int block, cudaStream_t s) {
+    const int grid = (a.T + block - 1) / block;
+    if (flux == RKDG_FLUX_HLLC)
+        stage_kernel<Real, NB, NQ, NG, RKDG_FLUX_HLLC, MODE><<<grid, block, 0, s>>>(a);
+    else
+        stage_kernel<Real, NB, NQ, NG, RKDG_FLUX_LLF, MODE><<<grid, block, 0, s>>>(a);
+}
+
+template <typename Real, int NB, int MODE>
+void dispatch_rule(const StageArgs& a, int nq, int ng, int flux, int block, cudaStream_t s) {
+    if (nq == 7 && ng == 3) return dispatch_flux<Real, NB, 7, 3, MODE>(a, flux, block, s);
+    if (nq == 6 && ng == 3) return dispatch_flux<Real, NB, 6, 3, MODE>(a, flux, block, s);
+    if (nq == 3 && ng == 2) return dispatch_flux<Real, NB, 3, 2, MODE>(a, flux, block, s);
+    if (nq == 7 && ng == 2) return dispatch_flux<Real, NB, 7, 2, MODE>(a, flux, block, s);
+    if (nq == 6 && ng == 2) return dispatch_flux<Real, NB, 6, 2, MODE>(a, flux, block, s);
+    if (nq == 3 && ng == 3) return dispatch_flux<Real, NB, 3, 3, MODE>(a, flux, block, s);
+    throw Error{RKDG_ERR_INVALID, "unsupported quadrature combination"};
+}
+
+template <int MODE>
+void dispatch(const StageArgs& a, int order, int nq, int ng, int flux, int prec, int block,
+              cudaStream_t s) {
+    if (block != 64 && block != 128) block = 128;
+    if (prec == RKDG_FP32) {
+        if (order == 1) dispatch_rule<float, 3, MODE>(a, nq, ng, flux, block, s);
+        else dispatch_rule<float, 6, MODE>(a, nq, ng, flux, block, s);
+    } else {
+        if (order == 1) dispatch_rule<double, 3, MODE>(a, nq, ng, flux, block, s);
+        else dispatch_rule<double, 6, MODE>(a, nq, ng, flux, block, s);
+    }
+    RKDG_CUDA_TRY(cudaGetLastError());
+}
+
+}  // namespace
+
+void launch_stage(const StageArgs& a, int order, int nq, int ng, int flux, int prec, int block,
+                  cudaStream_t stream) {
+    dispatch<MODE_STAGE>(a, order, nq, ng, flux, prec, block, stream);
+}
+
+void launch_residual(const StageArgs& a, int order, int nq, int ng, int flux, int prec, int block,
+                     cudaStream_t stream) {
+    dispatch<MODE_RESIDUAL>(a, order, nq, ng, flux, prec, block, stream);
+}
+
+void launch_wave(int T, int ld, const void* U, int order, int prec, const double* jinv,
+                 double gamma, StepCtl* ctl, cudaStream_t stream) {
+    (void)order;
+    RKDG_CUDA_TRY(cudaMemsetAsync(&ctl->wave_bits, 0, sizeof(unsigned long long), stream));
+    const int grid = (T + 255) / 256;
+    if (prec == RKDG_FP32)
+        wave_kernel<float><<<grid, 256, 0, stream>>>(T, ld, static_cast<const float*>(U), jinv, gamma, ctl);
+    else
+        wave_kernel<double><<<grid, 256, 0, stream>>>(T, ld, static_cast<const double*>(U), jinv, gamma, ctl);
+    RKDG_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_step_begin(StepCtl* ctl, cudaStream_t stream) {
+    step_begin_kernel<<<1, 32, 0, stream>>>(ctl);
+    RKDG_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_limiter(int T, int ld, void* U, const int4* conn, const double* lim,
+                    const double* jinv, int order, int nq, int ng, int prec, double gamma,
+                    const double* far, double tvb_m, cudaStream_t stream) {
+    const int grid = (T + 127) / 128;
+    const int cfg = cfg_index(nq, ng);  // midpoint tables are in every uploaded configuration
+    if (prec == RKDG_FP32) {
+        if (order == 1)
+            limiter_kernel<float, 3><<<grid, 128, 0, stream>>>(T, ld, static_cast<float*>(U), conn, lim, jinv, gamma, far[0], far[1], far[2], far[3], tvb_m, cfg);
+        else
+            limiter_kernel<float, 6><<<grid, 128, 0, stream>>>(T, ld, static_cast<float*>(U), conn, lim, jinv, gamma, far[0], far[1], far[2], far[3], tvb_m, cfg);
+    } else {
+        if (order == 1)
+            limiter_kernel<double, 3><<<grid, 128, 0, stream>>>(T, ld, static_cast<double*>(U), conn, lim, jinv, gamma, far[0], far[1], far[2], far[3], tvb_m, cfg);
+        else
+            limiter_kernel<double, 6><<<grid, 128, 0, stream>>>(T, ld, static_cast<double*>(U), conn, lim, jinv, gamma, far[0], far[1], far[2], far[3], tvb_m, cfg);
+    }
+    RKDG_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_import(int T, int ld, const double* staging, int ldh, const double* conv,
+                   const int32_t* perm, void* U, int order, int prec, cudaStream_t stream) {
+    const int grid = (T + 127) / 128;
+    if (prec == RKDG_FP32) {
+        if (order == 1) import_kernel<float, 3><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<float*>(U));
+        else import_kernel<float, 6><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<float*>(U));
+    } else {
+        if (order == 1) import_kernel<double, 3><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<double*>(U));
+        else import_kernel<double, 6><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<double*>(U));
+    }
+    RKDG_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_export(int T, int ld, const void* U, const double* conv, const int32_t* perm,
+                   double* staging, int ldh, int order, int prec, int residual_scale,
+                   const double* jinv, cudaStream_t stream) {
+    const int grid = (T + 127) / 128;
+    if (prec == RKDG_FP32) {
+        if (order == 1) export_kernel<float, 3><<<grid, 128, 0, stream>>>(T, ld, static_cast<const float*>(U), conv, perm, staging, ldh, residual_scale, jinv);
+        else export_kernel<float, 6><<<grid, 128, 0, stream>>>(T, ld, static_cast<const float*>(U), conv, perm, staging, ldh, residual_scale, jinv);
+    } else {
+        if (order == 1) export_kernel<double, 3><<<grid, 128, 0, stream>>>(T, ld, static_cast<const double*>(U), conv, perm, staging, ldh, residual_scale, jinv);
+        else export_kernel<double, 6><<<grid, 128, 0, stream>>>(T, ld, static_cast<const double*>(U), conv, perm, staging, ldh, residual_scale, jinv);
+    }
+    RKDG_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_totals(int T, int ld, const void* U, int order, int prec, const double* jinv,
+                   double* partial, double* out4, cudaStream_t stream) {
+    (void)order;
+    const int n = totals_partial_count(T);
+    if (prec == RKDG_FP32)
+        totals_partial_kernel<float><<<n, kTotBlock, 0, stream>>>(T, ld, static_cast<const float*>(U), jinv, partial);
+    else
+        totals_partial_kernel<double><<<n, kTotBlock, 0, stream>>>(T, ld, static_cast<const double*>(U), jinv, partial);
+    totals_final_kernel<<<1, kTotBlock, 0, stream>>>(n, partial, out4);
+    RKDG_CUDA_TRY(cudaGetLastError());
+}
+
+}  // namespace rkdg

@@ -1,0 +1,156 @@
+// Internal declarations shared by the host C++ and CUDA translation units of
+// librkdg.so.  Nothing here crosses the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "rkdg.h"
+
+namespace rkdg {
+
+constexpr int kMaxNB = 6;   // P2
+constexpr int kMaxNQ = 7;   // degree-5 volume rule
+constexpr int kMaxNG = 3;   // 3-point Gauss-Legendre per edge
+
+// ---------------------------------------------------------------- errors --
+void set_error(const std::string& msg);
+struct Error {
+    int code;
+    std::string msg;
+};
+#define RKDG_CUDA_TRY(expr)                                                              \
+    do {                                                                                 \
+        cudaError_t e_ = (expr);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            throw ::rkdg::Error{RKDG_ERR_CUDA, std::string(#expr) + ": " +               \
+                                                   cudaGetErrorString(e_)};              \
+    } while (0)
+
+// ----------------------------------------------------------- quadrature --
+// Reference-element tables of the native basis (orthonormal under the area
+// average on the triangle (0,0),(1,0),(0,1), hierarchical: the first 3
+// functions span P1).  Volume points carry their normalised weight folded
+// into the gradient tables.
+struct RuleTables {
+    // volume: value and weighted gradients, [q][i]
+    double vphi[kMaxNQ][kMaxNB];
+    double vdxi_w[kMaxNQ][kMaxNB];
+    double veta_w[kMaxNQ][kMaxNB];
+    double vw[kMaxNQ];
+    // edges: value at point g of edge k, [k][g][i]; normalised weights [g]
+    double ephi[3][kMaxNG][kMaxNB];
+    double ew[kMaxNG];
+    // P1 part at the three edge midpoints [k][1..2] and its least-squares
+    // inverse (2 x 3) for the limiter
+    double mphi[3][2];
+    double minv[2][3];
+};
+
+void volume_rule(int nq, double l[][3], double* w);
+void edge_rule(int ng, double* s, double* w);
+// native basis: coefficients on monomials 1, xi, eta, xi^2, xi*eta, eta^2
+const double (*native_coeff())[6];
+void native_eval(int nbasis, double xi, double eta, double* val, double* dxi, double* deta);
+RuleTables make_tables(int nq, int ng);
+
+// ------------------------------------------------------------- geometry --
+// Per-element FP64 quantities computed on the host once.
+struct HostGeometry {
+    std::vector<double> jinv;   // [T][4]: rows of J^-1, (r0x, r0y, r1x, r1y)
+    std::vector<double> area;   // [T]
+    std::vector<double> conv_in;   // [T][6][6] native <- reference: b_j = sum_i a_i C[i][j]
+    std::vector<double> conv_out;  // [T][6][6] reference <- native: a_i = sum_j b_j D[i][j]
+    std::vector<double> lim;       // [T][3][6] limiter geometry per edge (see kernels)
+};
+
+// ------------------------------------------------------------------ mesh --
+struct HostMesh {
+    int T = 0;
+    std::vector<double> xy;       // [T][3][2] per-triangle vertex coordinates
+    std::vector<int32_t> nbr;     // [T][3]
+    std::vector<int8_t> bc;       // [T][3]
+    std::vector<int8_t> shared;   // [T][3] neighbour-local edge index (or -1)
+    std::vector<int32_t> perm;    // internal index -> caller index
+    std::vector<int32_t> tri_vertex;  // [T][3] caller's vertex ids (output only)
+    std::vector<double> vertices;     // [V][2] caller's vertices (output only)
+};
+
+// Builds HostMesh from the C descriptor in caller order; validates it.
+HostMesh build_mesh(const rkdg_mesh_desc& d);
+// Morton order of the centroids; returns perm (new -> old).
+std::vector<int32_t> morton_order(const HostMesh& m);
+HostMesh permute_mesh(const HostMesh& m, const std::vector<int32_t>& perm);
+HostGeometry build_geometry(const HostMesh& m, int order, bool with_conversion, bool with_limiter);
+// Packed connectivity word: bits 0-5 shared edge (2 bits per edge),
+// bits 6-11 boundary tag (2 bits per edge).
+uint32_t pack_info(const int8_t* shared3, const int8_t* bc3);
+
+// ------------------------------------------------------------- device --
+struct StepCtl {
+    double t;                  // simulated time after the last step
+    double t_final;            // <= 0: no final time
+    double dt;                 // dt of the current step
+    double dt_fixed;           // > 0: use this dt instead of the CFL one
+    double cfl;
+    unsigned long long wave_bits;   // max (|u|+c) perimeter/area of the state, as bits
+    unsigned long long mon_bits[2]; // residual monitor, as bits
+    int step;
+    int done;
+    int error;                 // bit 0: non-physical state seen
+    int pad;
+};
+
+struct DeviceArrays {
+    void* U[3] = {nullptr, nullptr, nullptr};  // state buffers (A holds U^n)
+    double* jinv = nullptr;     // [2][ld][2]
+    int4* conn = nullptr;       // [ld]
+    double* lim = nullptr;      // [3][ld][6] limiter geometry (when enabled)
+    int32_t* perm = nullptr;    // [T]
+    double* conv_in = nullptr;  // [T][36]
+    double* conv_out = nullptr; // [T][36]
+    double* staging = nullptr;  // [4][6][T] dense FP64 host-layout staging
+    double* partial = nullptr;  // block partial sums for deterministic totals
+    StepCtl* ctl = nullptr;
+    size_t bytes = 0;
+};
+
+struct StageArgs {
+    int T, ld;
+    const void* U;       // stage input
+    const void* U0;      // U^n (may equal nullptr when a == 0)
+    void* Unew;          // stage output (residual output in residual mode)
+    const double* jinv;
+    const int4* conn;
+    StepCtl* ctl;
+    double a, b;         // Unew = a U0 + b (U + dt L(U))
+    double gamma;
+    double far[4];
+    int last_stage;      // compute wave max / monitor / error in the epilogue
+};
+
+// Launchers (kernels.cu).  All asynchronous on `stream`.
+void upload_tables(int nq, int ng);
+void launch_stage(const StageArgs& a, int order, int nq, int ng, int flux, int prec,
+                  int block, cudaStream_t stream);
+void launch_residual(const StageArgs& a, int order, int nq, int ng, int flux, int prec,
+                     int block, cudaStream_t stream);
+void launch_wave(int T, int ld, const void* U, int order, int prec, const double* jinv,
+                 double gamma, StepCtl* ctl, cudaStream_t stream);
+void launch_step_begin(StepCtl* ctl, cudaStream_t stream);
+void launch_limiter(int T, int ld, void* U, const int4* conn, const double* lim,
+                    const double* jinv, int order, int nq, int ng, int prec, double gamma,
+                    const double* far, double tvb_m, cudaStream_t stream);
+void launch_import(int T, int ld, const double* staging, int ldh, const double* conv,
+                   const int32_t* perm, void* U, int order, int prec, cudaStream_t stream);
+void launch_export(int T, int ld, const void* U, const double* conv, const int32_t* perm,
+                   double* staging, int ldh, int order, int prec, int residual_scale,
+                   const double* jinv, cudaStream_t stream);
+void launch_totals(int T, int ld, const void* U, int order, int prec, const double* jinv,
+                   double* partial, double* out4, cudaStream_t stream);
+int totals_partial_count(int T);
+
+}  // namespace rkdg
