@@ -82,6 +82,7 @@ typedef struct rkdg_params {
     int32_t order;        /* 1 (P1) or 2 (P2)                                */
     int32_t nq;           /* volume rule: 3 (deg 2), 6 (deg 4) or 7 (deg 5)  */
     int32_t ng;           /* Gauss points per edge: 2 or 3                   */
+                          /* supported: P2 with nq 7|6, ng 3; P1 nq 3, ng 2 */
     int32_t flux;         /* RKDG_FLUX_*                                     */
     int32_t limiter;      /* RKDG_LIMITER_*                                  */
     int32_t rk;           /* 2 or 3 (SSP Runge-Kutta stages)                 */

@@ -470,42 +470,43 @@ static inline void ghost_state(int tag, const double u[4], const double far[4], 
 }
 
 /* HLLC flux through unit normal n (Toro, Riemann Solvers and Numerical
- * Methods for Fluid Dynamics, 3rd ed., sec. 10.4), wave speeds of Batten,
- * Clarke, Lambert & Causon (SIAM J. Sci. Comput. 18, 1997) from Roe averages. */
+ * Methods for Fluid Dynamics, 3rd ed., sec. 10.4): Davis wave-speed bounds
+ * S_L = min(q_L - c_L, q_R - c_R), S_R = max(q_L + c_L, q_R + c_R) (eq. 10.48),
+ * contact speed S_M (eq. 10.37) and the star flux in its pressure form
+ * F*_K = (S_M (S_K U_K - F_K) + S_K p* (0, n_x, n_y, S_M)) / (S_K - S_M)
+ * with p* = p_K + rho_K (S_K - q_K)(S_M - q_K) (eqs. 10.36, 10.41-10.43,
+ * as written by Toro in sec. 10.6). */
 static void hllc_flux(const double uL[4], const double uR[4], double nx, double ny, double gamma,
                       double f[4]) {
-    double rL = uL[0], rR = uR[0];
-    double vxL = uL[1] / rL, vyL = uL[2] / rL, vxR = uR[1] / rR, vyR = uR[2] / rR;
-    double pL = (gamma - 1) * (uL[3] - 0.5 * rL * (vxL * vxL + vyL * vyL));
-    double pR = (gamma - 1) * (uR[3] - 0.5 * rR * (vxR * vxR + vyR * vyR));
+    double rL = uL[0], rR = uR[0], iL = 1.0 / rL, iR = 1.0 / rR;
+    double vxL = uL[1] * iL, vyL = uL[2] * iL, vxR = uR[1] * iR, vyR = uR[2] * iR;
+    double pL = (gamma - 1) * (uL[3] - 0.5 * (uL[1] * vxL + uL[2] * vyL));
+    double pR = (gamma - 1) * (uR[3] - 0.5 * (uR[1] * vxR + uR[2] * vyR));
     double qL = vxL * nx + vyL * ny, qR = vxR * nx + vyR * ny;
-    double cL = sqrt(gamma * pL / rL), cR = sqrt(gamma * pR / rR);
-    double HL = (uL[3] + pL) / rL, HR = (uR[3] + pR) / rR;
-    double sL = sqrt(rL), sR = sqrt(rR), isum = 1.0 / (sL + sR);
-    double vxt = (sL * vxL + sR * vxR) * isum, vyt = (sL * vyL + sR * vyR) * isum;
-    double Ht = (sL * HL + sR * HR) * isum;
-    double qt = vxt * nx + vyt * ny;
-    double ct = sqrt((gamma - 1) * (Ht - 0.5 * (vxt * vxt + vyt * vyt)));
-    double SL = fmin(qL - cL, qt - ct), SR = fmax(qR + cR, qt + ct);
-    double SM = (pR - pL + rL * qL * (SL - qL) - rR * qR * (SR - qR)) /
-                (rL * (SL - qL) - rR * (SR - qR));
+    double cL = sqrt(gamma * pL * iL), cR = sqrt(gamma * pR * iR);
+    double SL = fmin(qL - cL, qR - cR), SR = fmax(qL + cL, qR + cR);
     double FL[4] = {rL * qL, uL[1] * qL + pL * nx, uL[2] * qL + pL * ny, (uL[3] + pL) * qL};
     double FR[4] = {rR * qR, uR[1] * qR + pR * nx, uR[2] * qR + pR * ny, (uR[3] + pR) * qR};
     if (SL >= 0) {
         memcpy(f, FL, sizeof(FL));
-    } else if (SR <= 0) {
-        memcpy(f, FR, sizeof(FR));
-    } else if (SM >= 0) {
-        double k = rL * (SL - qL) / (SL - SM);
-        double us[4] = {k, k * (vxL + (SM - qL) * nx), k * (vyL + (SM - qL) * ny),
-                        k * (uL[3] / rL + (SM - qL) * (SM + pL / (rL * (SL - qL))))};
-        for (int v = 0; v < 4; ++v) f[v] = FL[v] + SL * (us[v] - uL[v]);
-    } else {
-        double k = rR * (SR - qR) / (SR - SM);
-        double us[4] = {k, k * (vxR + (SM - qR) * nx), k * (vyR + (SM - qR) * ny),
-                        k * (uR[3] / rR + (SM - qR) * (SM + pR / (rR * (SR - qR))))};
-        for (int v = 0; v < 4; ++v) f[v] = FR[v] + SR * (us[v] - uR[v]);
+        return;
     }
+    if (SR <= 0) {
+        memcpy(f, FR, sizeof(FR));
+        return;
+    }
+    double dL = rL * (SL - qL), dR = rR * (SR - qR);
+    double SM = (pR - pL + dL * qL - dR * qR) / (dL - dR);
+    const int left = SM >= 0;
+    const double* u = left ? uL : uR;
+    const double* F = left ? FL : FR;
+    double d = left ? dL : dR, p = left ? pL : pR, q = left ? qL : qR, S = left ? SL : SR;
+    double ps = p + d * (SM - q);
+    double k = 1.0 / (S - SM);
+    f[0] = SM * (S * u[0] - F[0]) * k;
+    f[1] = (SM * (S * u[1] - F[1]) + S * ps * nx) * k;
+    f[2] = (SM * (S * u[2] - F[2]) + S * ps * ny) * k;
+    f[3] = (SM * (S * u[3] - F[3]) + S * ps * SM) * k;
 }
 
 /* R(U) of one element (reference basis, not mass-divided): the chain

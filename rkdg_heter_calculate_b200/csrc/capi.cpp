@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <memory>
@@ -40,6 +41,8 @@ struct rkdg_ctx {
     bool have_state = false;
     cudaGraphExec_t graph = nullptr;
     StepCtl* h_ctl = nullptr;  // pinned mirror of the device control block
+    TileArgs tiles{};
+    int variant = 1;  // 1 tile-staged (default), 0 owner-computes
 };
 
 namespace {
@@ -82,6 +85,11 @@ void check_params(const rkdg_params& p) {
     if (p.order != 1 && p.order != 2) throw Error{RKDG_ERR_INVALID, "order must be 1 or 2"};
     if (p.nq != 3 && p.nq != 6 && p.nq != 7) throw Error{RKDG_ERR_INVALID, "nq must be 3, 6 or 7"};
     if (p.ng != 2 && p.ng != 3) throw Error{RKDG_ERR_INVALID, "ng must be 2 or 3"};
+    const bool rule_ok = (p.order == 2 && p.ng == 3 && (p.nq == 7 || p.nq == 6)) ||
+                         (p.order == 1 && p.nq == 3 && p.ng == 2);
+    if (!rule_ok)
+        throw Error{RKDG_ERR_INVALID,
+                    "supported rules: P2 with nq 7 or 6 and ng 3; P1 with nq 3 and ng 2"};
     if (p.flux != RKDG_FLUX_LLF && p.flux != RKDG_FLUX_HLLC) throw Error{RKDG_ERR_INVALID, "unknown flux"};
     if (p.limiter != RKDG_LIMITER_NONE && p.limiter != RKDG_LIMITER_TVB)
         throw Error{RKDG_ERR_INVALID, "unknown limiter"};
@@ -172,7 +180,7 @@ void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out) {
     a.U0 = s == 0 ? nullptr : c->d.U[u0];
     a.Unew = c->d.U[out];
     a.last_stage = s == c->p.rk - 1;
-    launch_stage(a, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
+    launch_stage(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
     if (c->p.limiter == RKDG_LIMITER_TVB)
         launch_limiter(c->T, c->ld, c->d.U[out], c->d.conn, c->d.lim, c->d.jinv, c->p.order,
                        c->p.nq, c->p.ng, c->p.precision, c->p.gamma, c->p.farfield, c->p.tvb_m,
@@ -213,6 +221,11 @@ void destroy_ctx(rkdg_ctx* c) {
     cudaFree(c->d.staging);
     cudaFree(c->d.partial);
     cudaFree(c->d.ctl);
+    cudaFree(c->d.tcode);
+    cudaFree(c->d.halo_ptr);
+    cudaFree(c->d.halo);
+    cudaFree(c->d.task_ptr);
+    cudaFree(c->d.task);
     if (c->h_ctl) cudaFreeHost(c->h_ctl);
     if (c->stream) cudaStreamDestroy(c->stream);
     cudaSetDevice(prev);
@@ -313,6 +326,34 @@ int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx*
             RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.lim, g.lim.data(), sizeof(double) * g.lim.size(),
                                           cudaMemcpyHostToDevice, c->stream));
         }
+        {
+            TileTables tt = build_tiles(c->mesh);
+            c->d.tcode = (int4*)dev_alloc(c, sizeof(int32_t) * tt.code.size());
+            c->d.halo_ptr = (int32_t*)dev_alloc(c, sizeof(int32_t) * tt.halo_ptr.size());
+            c->d.halo = (int2*)dev_alloc(c, sizeof(int32_t) * std::max<size_t>(2, tt.halo.size()));
+            c->d.task_ptr = (int32_t*)dev_alloc(c, sizeof(int32_t) * tt.task_ptr.size());
+            c->d.task = (uint16_t*)dev_alloc(c, sizeof(uint16_t) * std::max<size_t>(1, tt.task.size()));
+            RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.tcode, tt.code.data(), sizeof(int32_t) * tt.code.size(),
+                                          cudaMemcpyHostToDevice, c->stream));
+            RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.halo_ptr, tt.halo_ptr.data(), sizeof(int32_t) * tt.halo_ptr.size(),
+                                          cudaMemcpyHostToDevice, c->stream));
+            if (!tt.halo.empty())
+                RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.halo, tt.halo.data(), sizeof(int32_t) * tt.halo.size(),
+                                              cudaMemcpyHostToDevice, c->stream));
+            RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.task_ptr, tt.task_ptr.data(), sizeof(int32_t) * tt.task_ptr.size(),
+                                          cudaMemcpyHostToDevice, c->stream));
+            RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.task, tt.task.data(), sizeof(uint16_t) * tt.task.size(),
+                                          cudaMemcpyHostToDevice, c->stream));
+            c->tiles.code = c->d.tcode;
+            c->tiles.halo_ptr = c->d.halo_ptr;
+            c->tiles.halo = c->d.halo;
+            c->tiles.task_ptr = c->d.task_ptr;
+            c->tiles.task = c->d.task;
+            c->tiles.max_halo = tt.max_halo;
+            c->tiles.ntiles = tt.ntiles;
+            sync(c);  // host tables go out of scope
+        }
+        if (const char* v = std::getenv("RKDG_STAGE_VARIANT")) c->variant = std::atoi(v) == 0 ? 0 : 1;
         c->d.partial = (double*)dev_alloc(c, sizeof(double) * 4 * (totals_partial_count(T) + 1));
         c->d.ctl = (StepCtl*)dev_alloc(c, sizeof(StepCtl));
         c->h_ctl->cfl = params->cfl;
@@ -413,7 +454,7 @@ int rkdg_residual(rkdg_ctx* c, double* R, int32_t ld, int32_t basis) {
         a.Unew = c->d.U[scratch];
         a.a = 0;
         a.b = 1;
-        launch_residual(a, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
+        launch_residual(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
         launch_export(c->T, c->ld, c->d.U[scratch], basis == RKDG_BASIS_REFERENCE ? c->d.conv_in : nullptr,
                       c->d.perm, c->d.staging, c->T, c->p.order, c->p.precision, 1, c->d.jinv,
                       c->stream);
@@ -577,10 +618,10 @@ int rkdg_time_stage(rkdg_ctx* c, int32_t s, int32_t reps, double* ms) {
         cudaEvent_t e0, e1;
         RKDG_CUDA_TRY(cudaEventCreate(&e0));
         RKDG_CUDA_TRY(cudaEventCreate(&e1));
-        launch_stage(a, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
+        launch_stage(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
         RKDG_CUDA_TRY(cudaEventRecord(e0, c->stream));
         for (int i = 0; i < reps; ++i)
-            launch_stage(a, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
+            launch_stage(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
         RKDG_CUDA_TRY(cudaEventRecord(e1, c->stream));
         RKDG_CUDA_TRY(cudaEventSynchronize(e1));
         float t = 0;

@@ -160,11 +160,21 @@ __device__ __forceinline__ void ghost(int tag, const Real u[4], const Real far[4
     }
 }
 
+// Reciprocal, quotient and square root: IEEE in FP64 (the parity path);
+// in FP32 the MUFU approximations (about 2 ulp), which the FP32 precision
+// form's tolerance absorbs.
+__device__ __forceinline__ double rcp_(double x) { return 1.0 / x; }
+__device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double div_(double a, double b) { return a / b; }
+__device__ __forceinline__ float div_(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+__device__ __forceinline__ float sqrt_(float x) { return x * rsqrtf(x); }
+
 // Normal Euler flux through the scaled normal (Nx, Ny): F Nx + G Ny.
 template <typename Real>
 __device__ __forceinline__ void normal_flux(const Real u[4], Real Nx, Real Ny, Real gm1, Real f[4],
                                             Real& p) {
-    Real ri = Real(1) / u[0];
+    Real ri = rcp_(u[0]);
     Real vx = u[1] * ri, vy = u[2] * ri;
     p = gm1 * (u[3] - Real(0.5) * (u[1] * vx + u[2] * vy));
     Real qn = vx * Nx + vy * Ny;
@@ -175,51 +185,49 @@ __device__ __forceinline__ void normal_flux(const Real u[4], Real Nx, Real Ny, R
 }
 
 // HLLC through the unit normal (nx, ny) (Toro, Riemann Solvers and Numerical
-// Methods for Fluid Dynamics, 3rd ed., sec. 10.4) with the Roe-average wave
-// speeds of Batten, Clarke, Lambert & Causon (SIAM J. Sci. Comput. 18, 1997).
+// Methods for Fluid Dynamics, 3rd ed., sec. 10.4): Davis wave-speed bounds
+// (eq. 10.48), contact speed S_M (eq. 10.37), star flux in its pressure form
+// F*_K = (S_M (S_K U_K - F_K) + S_K p* (0, nx, ny, S_M)) / (S_K - S_M),
+// p* = p_K + rho_K (S_K - q_K)(S_M - q_K): four reciprocals/quotients and two
+// square roots per point.
 template <typename Real>
 __device__ __forceinline__ void hllc(const Real uL[4], const Real uR[4], Real nx, Real ny,
                                      Real gamma, Real f[4]) {
     const Real gm1 = gamma - Real(1);
     Real rL = uL[0], rR = uR[0];
-    Real iL = Real(1) / rL, iR = Real(1) / rR;
+    Real iL = rcp_(rL), iR = rcp_(rR);
     Real vxL = uL[1] * iL, vyL = uL[2] * iL, vxR = uR[1] * iR, vyR = uR[2] * iR;
-    Real pL = gm1 * (uL[3] - Real(0.5) * rL * (vxL * vxL + vyL * vyL));
-    Real pR = gm1 * (uR[3] - Real(0.5) * rR * (vxR * vxR + vyR * vyR));
+    Real pL = gm1 * (uL[3] - Real(0.5) * (uL[1] * vxL + uL[2] * vyL));
+    Real pR = gm1 * (uR[3] - Real(0.5) * (uR[1] * vxR + uR[2] * vyR));
     Real qL = vxL * nx + vyL * ny, qR = vxR * nx + vyR * ny;
-    Real cL = sqrt(gamma * pL * iL), cR = sqrt(gamma * pR * iR);
-    Real HL = (uL[3] + pL) * iL, HR = (uR[3] + pR) * iR;
-    Real sL = sqrt(rL), sR = sqrt(rR), is = Real(1) / (sL + sR);
-    Real vxt = (sL * vxL + sR * vxR) * is, vyt = (sL * vyL + sR * vyR) * is;
-    Real Ht = (sL * HL + sR * HR) * is;
-    Real qt = vxt * nx + vyt * ny;
-    Real ct = sqrt(gm1 * (Ht - Real(0.5) * (vxt * vxt + vyt * vyt)));
-    Real SL = fmin(qL - cL, qt - ct), SR = fmax(qR + cR, qt + ct);
-    Real SM = (pR - pL + rL * qL * (SL - qL) - rR * qR * (SR - qR)) /
-              (rL * (SL - qL) - rR * (SR - qR));
+    Real cL = sqrt_(gamma * pL * iL), cR = sqrt_(gamma * pR * iR);
+    Real SL = fmin(qL - cL, qR - cR), SR = fmax(qL + cL, qR + cR);
     if (SL >= Real(0)) {
         f[0] = rL * qL;
         f[1] = uL[1] * qL + pL * nx;
         f[2] = uL[2] * qL + pL * ny;
         f[3] = (uL[3] + pL) * qL;
-    } else if (SR <= Real(0)) {
+        return;
+    }
+    if (SR <= Real(0)) {
         f[0] = rR * qR;
         f[1] = uR[1] * qR + pR * nx;
         f[2] = uR[2] * qR + pR * ny;
         f[3] = (uR[3] + pR) * qR;
-    } else {
-        const bool left = SM >= Real(0);
-        const Real* u = left ? uL : uR;
-        Real r = left ? rL : rR, ir = left ? iL : iR, vx = left ? vxL : vxR, vy = left ? vyL : vyR;
-        Real p = left ? pL : pR, q = left ? qL : qR, S = left ? SL : SR;
-        Real k = r * (S - q) / (S - SM);
-        Real us0 = k, us1 = k * (vx + (SM - q) * nx), us2 = k * (vy + (SM - q) * ny);
-        Real us3 = k * (u[3] * ir + (SM - q) * (SM + p / (r * (S - q))));
-        f[0] = r * q + S * (us0 - u[0]);
-        f[1] = u[1] * q + p * nx + S * (us1 - u[1]);
-        f[2] = u[2] * q + p * ny + S * (us2 - u[2]);
-        f[3] = (u[3] + p) * q + S * (us3 - u[3]);
+        return;
     }
+    Real dL = rL * (SL - qL), dR = rR * (SR - qR);
+    Real SM = div_(pR - pL + dL * qL - dR * qR, dL - dR);
+    const bool left = SM >= Real(0);
+    const Real* u = left ? uL : uR;
+    Real d = left ? dL : dR, p = left ? pL : pR, q = left ? qL : qR, S = left ? SL : SR;
+    Real ps = p + d * (SM - q);
+    Real k = rcp_(S - SM);
+    Real F0 = u[0] * q, F1 = u[1] * q + p * nx, F2 = u[2] * q + p * ny, F3 = (u[3] + p) * q;
+    f[0] = SM * (S * u[0] - F0) * k;
+    f[1] = (SM * (S * u[1] - F1) + S * ps * nx) * k;
+    f[2] = (SM * (S * u[2] - F2) + S * ps * ny) * k;
+    f[3] = (SM * (S * u[3] - F3) + S * ps * SM) * k;
 }
 
 // ---------------------------------------------------------- reductions --
@@ -323,7 +331,7 @@ __global__ void __launch_bounds__(128) stage_kernel(const StageArgs a) {
             for (int i = 0; i < NB; ++i) s += tb.vphi[q][i] * u[i][v];
             w[v] = s;
         }
-        Real ri = Real(1) / w[0];
+        Real ri = rcp_(w[0]);
         Real vx = w[1] * ri, vy = w[2] * ri;
         Real p = gm1 * (w[3] - Real(0.5) * (w[1] * vx + w[2] * vy));
         Real F[4] = {w[1], w[1] * vx + p, w[2] * vx, (w[3] + p) * vx};
@@ -380,12 +388,12 @@ __global__ void __launch_bounds__(128) stage_kernel(const StageArgs a) {
         Real alpha = Real(0);
         if (FLUX == RKDG_FLUX_LLF) {
             Real rho = Real(0.5) * (mL[0] + mR[0]);
-            Real ir = Real(1) / rho;
+            Real ir = rcp_(rho);
             Real vx = Real(0.5) * (mL[1] + mR[1]) * ir;
             Real vy = Real(0.5) * (mL[2] + mR[2]) * ir;
             Real E = Real(0.5) * (mL[3] + mR[3]);
             Real p = gm1 * (E - Real(0.5) * rho * (vx * vx + vy * vy));
-            alpha = fabs(vx * Nx + vy * Ny) + sqrt(gamma * p * ir) * len;
+            alpha = fabs(vx * Nx + vy * Ny) + sqrt_(gamma * p * ir) * len;
         }
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
@@ -473,6 +481,8 @@ __global__ void __launch_bounds__(128) stage_kernel(const StageArgs a) {
         block_max3_atomic(wv, m0, m1, &a.ctl->wave_bits, &a.ctl->mon_bits[0], &a.ctl->mon_bits[1]);
     }
 }
+
+#include "stage_tiled.cuh"
 
 // CFL measure of the current state (first step, rkdg_compute_dt).
 template <typename Real>
@@ -766,50 +776,77 @@ __global__ void __launch_bounds__(kTotBlock) totals_final_kernel(int n, const do
 // ----------------------------------------------------------- launchers --
 namespace {
 
+template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE>
+void launch_variant(const StageArgs& a, const TileArgs& t, int variant, int block, cudaStream_t s) {
+    if (variant == 1) {
+        const size_t smem = TiledSmem<Real, NB, NQ, NG>::bytes(t.max_halo);
+        // dynamic + static shared memory above 48 KB needs the opt-in; the
+        // static part (tables, block reduction) is ~1.2 KB, so opt in early.
+        // Per instantiation; raised when a context with a larger halo appears.
+        static size_t configured = 0;
+        if (configured == 0)  // residency is register-limited: give shared memory the carveout
+            RKDG_CUDA_TRY(cudaFuncSetAttribute(tiled_stage_kernel<Real, NB, NQ, NG, FLUX, MODE>,
+                                               cudaFuncAttributePreferredSharedMemoryCarveout,
+                                               (int)cudaSharedmemCarveoutMaxShared));
+        if (smem > configured) {
+            RKDG_CUDA_TRY(cudaFuncSetAttribute(tiled_stage_kernel<Real, NB, NQ, NG, FLUX, MODE>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            configured = smem;
+        }
+        tiled_stage_kernel<Real, NB, NQ, NG, FLUX, MODE><<<t.ntiles, kTile, smem, s>>>(a, t);
+    } else {
+        const int grid = (a.T + block - 1) / block;
+        stage_kernel<Real, NB, NQ, NG, FLUX, MODE><<<grid, block, 0, s>>>(a);
+    }
+}
+
 template <typename Real, int NB, int NQ, int NG, int MODE>
-void dispatch_flux(const StageArgs& a, int flux, int block, cudaStream_t s) {
-    const int grid = (a.T + block - 1) / block;
+void dispatch_flux(const StageArgs& a, const TileArgs& t, int variant, int flux, int block,
+                   cudaStream_t s) {
     if (flux == RKDG_FLUX_HLLC)
-        stage_kernel<Real, NB, NQ, NG, RKDG_FLUX_HLLC, MODE><<<grid, block, 0, s>>>(a);
+        launch_variant<Real, NB, NQ, NG, RKDG_FLUX_HLLC, MODE>(a, t, variant, block, s);
     else
-        stage_kernel<Real, NB, NQ, NG, RKDG_FLUX_LLF, MODE><<<grid, block, 0, s>>>(a);
+        launch_variant<Real, NB, NQ, NG, RKDG_FLUX_LLF, MODE>(a, t, variant, block, s);
 }
 
 template <typename Real, int NB, int MODE>
-void dispatch_rule(const StageArgs& a, int nq, int ng, int flux, int block, cudaStream_t s) {
-    if (nq == 7 && ng == 3) return dispatch_flux<Real, NB, 7, 3, MODE>(a, flux, block, s);
-    if (nq == 6 && ng == 3) return dispatch_flux<Real, NB, 6, 3, MODE>(a, flux, block, s);
-    if (nq == 3 && ng == 2) return dispatch_flux<Real, NB, 3, 2, MODE>(a, flux, block, s);
-    if (nq == 7 && ng == 2) return dispatch_flux<Real, NB, 7, 2, MODE>(a, flux, block, s);
-    if (nq == 6 && ng == 2) return dispatch_flux<Real, NB, 6, 2, MODE>(a, flux, block, s);
-    if (nq == 3 && ng == 3) return dispatch_flux<Real, NB, 3, 3, MODE>(a, flux, block, s);
+void dispatch_rule(const StageArgs& a, const TileArgs& t, int variant, int nq, int ng, int flux,
+                   int block, cudaStream_t s) {
+    // the rule pairs in use: P2 with 7/3 (the reference's) or 6/3 points,
+    // P1 with 3/2 points (rkdg_create rejects the others)
+    if constexpr (NB == 6) {
+        if (nq == 7 && ng == 3) return dispatch_flux<Real, NB, 7, 3, MODE>(a, t, variant, flux, block, s);
+        if (nq == 6 && ng == 3) return dispatch_flux<Real, NB, 6, 3, MODE>(a, t, variant, flux, block, s);
+    } else {
+        if (nq == 3 && ng == 2) return dispatch_flux<Real, NB, 3, 2, MODE>(a, t, variant, flux, block, s);
+    }
     throw Error{RKDG_ERR_INVALID, "unsupported quadrature combination"};
 }
 
 template <int MODE>
-void dispatch(const StageArgs& a, int order, int nq, int ng, int flux, int prec, int block,
-              cudaStream_t s) {
+void dispatch(const StageArgs& a, const TileArgs& t, int variant, int order, int nq, int ng,
+              int flux, int prec, int block, cudaStream_t s) {
     if (block != 64 && block != 128) block = 128;
     if (prec == RKDG_FP32) {
-        if (order == 1) dispatch_rule<float, 3, MODE>(a, nq, ng, flux, block, s);
-        else dispatch_rule<float, 6, MODE>(a, nq, ng, flux, block, s);
+        if (order == 1) dispatch_rule<float, 3, MODE>(a, t, variant, nq, ng, flux, block, s);
+        else dispatch_rule<float, 6, MODE>(a, t, variant, nq, ng, flux, block, s);
     } else {
-        if (order == 1) dispatch_rule<double, 3, MODE>(a, nq, ng, flux, block, s);
-        else dispatch_rule<double, 6, MODE>(a, nq, ng, flux, block, s);
+        if (order == 1) dispatch_rule<double, 3, MODE>(a, t, variant, nq, ng, flux, block, s);
+        else dispatch_rule<double, 6, MODE>(a, t, variant, nq, ng, flux, block, s);
     }
     RKDG_CUDA_TRY(cudaGetLastError());
 }
 
 }  // namespace
 
-void launch_stage(const StageArgs& a, int order, int nq, int ng, int flux, int prec, int block,
-                  cudaStream_t stream) {
-    dispatch<MODE_STAGE>(a, order, nq, ng, flux, prec, block, stream);
+void launch_stage(const StageArgs& a, const TileArgs& t, int variant, int order, int nq, int ng,
+                  int flux, int prec, int block, cudaStream_t stream) {
+    dispatch<MODE_STAGE>(a, t, variant, order, nq, ng, flux, prec, block, stream);
 }
 
-void launch_residual(const StageArgs& a, int order, int nq, int ng, int flux, int prec, int block,
-                     cudaStream_t stream) {
-    dispatch<MODE_RESIDUAL>(a, order, nq, ng, flux, prec, block, stream);
+void launch_residual(const StageArgs& a, const TileArgs& t, int variant, int order, int nq, int ng,
+                     int flux, int prec, int block, cudaStream_t stream) {
+    dispatch<MODE_RESIDUAL>(a, t, variant, order, nq, ng, flux, prec, block, stream);
 }
 
 void launch_wave(int T, int ld, const void* U, int order, int prec, const double* jinv,

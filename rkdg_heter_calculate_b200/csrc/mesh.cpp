@@ -372,6 +372,48 @@ HostGeometry build_geometry(const HostMesh& m, int order, bool with_conversion, 
     return g;
 }
 
+TileTables build_tiles(const HostMesh& m) {
+    const int T = m.T, B = kTile;
+    TileTables t;
+    t.ntiles = (T + B - 1) / B;
+    t.code.assign((size_t)4 * T, 0);
+    t.halo_ptr.assign(t.ntiles + 1, 0);
+    t.task_ptr.assign(t.ntiles + 1, 0);
+    int maxh = 0;
+    for (int tile = 0; tile < t.ntiles; ++tile) {
+        const int e0 = tile * B, e1 = std::min(T, e0 + B);
+        int nh = 0;
+        for (int k = 0; k < 3; ++k)  // tasks and halo slots sorted by edge, then element
+            for (int e = e0; e < e1; ++e) {
+                const int le = e - e0;
+                const int n = m.nbr[3 * e + k];
+                int code;
+                bool task = true;
+                if (n < 0) {
+                    code = EDGE_BOUNDARY | ((m.bc[3 * e + k] & 3) << 2);
+                } else if (n >= e0 && n < e1) {
+                    const int se = m.shared[3 * e + k];
+                    const bool owner = e < n;
+                    code = (owner ? EDGE_IN_OWNER : EDGE_IN_OTHER) | (se << 2) | ((n - e0) << 4);
+                    task = owner;
+                } else {
+                    const int se = m.shared[3 * e + k];
+                    code = EDGE_HALO | (se << 2) | (nh << 4);
+                    t.halo.push_back(n);
+                    t.halo.push_back(se);
+                    ++nh;
+                }
+                t.code[(size_t)4 * e + k] = code;
+                if (task) t.task.push_back((uint16_t)(le * 4 + k));
+            }
+        maxh = std::max(maxh, nh);
+        t.halo_ptr[tile + 1] = (int32_t)(t.halo.size() / 2);
+        t.task_ptr[tile + 1] = (int32_t)t.task.size();
+    }
+    t.max_halo = std::max(4, (maxh + 3) / 4 * 4);
+    return t;
+}
+
 }  // namespace rkdg
 
 // ------------------------------------------------------------ file input --

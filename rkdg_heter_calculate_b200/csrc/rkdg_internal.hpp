@@ -89,6 +89,30 @@ HostGeometry build_geometry(const HostMesh& m, int order, bool with_conversion, 
 // bits 6-11 boundary tag (2 bits per edge).
 uint32_t pack_info(const int8_t* shared3, const int8_t* bc3);
 
+// ---------------------------------------------------------------- tiles --
+// Work decomposition of the tile-staged stage kernel: a CTA owns kTile
+// consecutive (locality-ordered) elements.  For every element edge k a code
+// says where the trace across it comes from:
+//   bits 0-1 kind: 0 in-tile neighbour, this side computes the flux (lower index)
+//                  1 in-tile neighbour, the other side computes it
+//                  2 out-of-tile (halo) neighbour, this side computes
+//                  3 boundary edge, this side computes
+//   bits 2-3 neighbour-local edge (kinds 0-2) or boundary tag (kind 3)
+//   bits 4.. local index of the in-tile neighbour, or the halo slot
+constexpr int kTile = 128;
+enum { EDGE_IN_OWNER = 0, EDGE_IN_OTHER = 1, EDGE_HALO = 2, EDGE_BOUNDARY = 3 };
+
+struct TileTables {
+    int ntiles = 0;
+    int max_halo = 0;                  // rounded up to a multiple of 4
+    std::vector<int32_t> code;         // [T][4] (code of edges 0..2, unused)
+    std::vector<int32_t> halo_ptr;     // [ntiles + 1]
+    std::vector<int32_t> halo;         // [nhalo][2] (global element, its edge)
+    std::vector<int32_t> task_ptr;     // [ntiles + 1]
+    std::vector<uint16_t> task;        // local element * 4 + edge, sorted by edge
+};
+TileTables build_tiles(const HostMesh& m);
+
 // ------------------------------------------------------------- device --
 struct StepCtl {
     double t;                  // simulated time after the last step
@@ -115,7 +139,23 @@ struct DeviceArrays {
     double* staging = nullptr;  // [4][6][T] dense FP64 host-layout staging
     double* partial = nullptr;  // block partial sums for deterministic totals
     StepCtl* ctl = nullptr;
+    // tile tables
+    int4* tcode = nullptr;
+    int32_t* halo_ptr = nullptr;
+    int2* halo = nullptr;
+    int32_t* task_ptr = nullptr;
+    uint16_t* task = nullptr;
     size_t bytes = 0;
+};
+
+struct TileArgs {
+    const int4* code;
+    const int32_t* halo_ptr;
+    const int2* halo;
+    const int32_t* task_ptr;
+    const uint16_t* task;
+    int max_halo;
+    int ntiles;
 };
 
 struct StageArgs {
@@ -134,10 +174,12 @@ struct StageArgs {
 
 // Launchers (kernels.cu).  All asynchronous on `stream`.
 void upload_tables(int nq, int ng);
-void launch_stage(const StageArgs& a, int order, int nq, int ng, int flux, int prec,
-                  int block, cudaStream_t stream);
-void launch_residual(const StageArgs& a, int order, int nq, int ng, int flux, int prec,
-                     int block, cudaStream_t stream);
+// variant: 0 owner-computes (one thread per element, both sides of every
+// edge), 1 tile-staged (each interior flux once per tile, traces shared)
+void launch_stage(const StageArgs& a, const TileArgs& t, int variant, int order, int nq, int ng,
+                  int flux, int prec, int block, cudaStream_t stream);
+void launch_residual(const StageArgs& a, const TileArgs& t, int variant, int order, int nq,
+                     int ng, int flux, int prec, int block, cudaStream_t stream);
 void launch_wave(int T, int ld, const void* U, int order, int prec, const double* jinv,
                  double gamma, StepCtl* ctl, cudaStream_t stream);
 void launch_step_begin(StepCtl* ctl, cudaStream_t stream);
