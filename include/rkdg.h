@@ -183,6 +183,23 @@ int rkdg_conservation_totals(rkdg_ctx* ctx, double totals[4]);
  * counterpart (the reference times nothing on the device). */
 int rkdg_time_stage(rkdg_ctx* ctx, int32_t s, int32_t reps, double* ms_per_launch);
 
+/* Allocation-free FP64 conservation totals.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory -- an embedding
+ * application whose device memory is all owned by its own allocator, or a
+ * loop that must not allocate once running: the caller passes device arrays
+ * d_means [4][ld] (the cell means of rho, rhou, rhov, rhoE: row 0 of each
+ * freedom block) and d_area [ntri], and receives sum_e area_e * mean_e in
+ * d_totals[4] (device), ordered on `stream` (a cudaStream_t, NULL = legacy
+ * default stream) and reduced in a fixed order (deterministic).  Scratch is
+ * a static 128 KiB device array inside this library, held by every GPU that
+ * loads it until exit; ntri is limited to 1,048,576 (larger meshes are
+ * rejected with RKDG_ERR_INVALID).  The first call on a device looks up that
+ * array's device address (cudaGetSymbolAddress), so make it before any
+ * stream capture.  Calls that overlap on one GPU share the array and race;
+ * serialise them.  Calls no cudaMalloc/cudaFree. */
+int rkdg_conservation_totals_noalloc(int32_t ntri, const double* d_means, int32_t ld,
+                                     const double* d_area, double* d_totals, void* stream);
+
 /* ---- output ------------------------------------------------------------ */
 /* Writes the cell means as the reference's Tecplot solution.plt
  * (CCUDARkdgSolver::outputSolution, src/cudarkdgsolver.cu:860-1001). */

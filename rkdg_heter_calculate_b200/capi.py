@@ -82,6 +82,8 @@ def lib():
             "rkdg_build_connectivity": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(C.c_int32),
                                                   C.POINTER(C.c_int8), C.POINTER(C.c_int8)]),
             "rkdg_locality_order": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(C.c_int32)]),
+            "rkdg_conservation_totals_noalloc": (C.c_int, [C.c_int32, C.c_void_p, C.c_int32,
+                                                           C.c_void_p, C.c_void_p, C.c_void_p]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
