@@ -205,6 +205,44 @@ int rkdg_conservation_totals_noalloc(int32_t ntri, const double* d_means, int32_
  * (CCUDARkdgSolver::outputSolution, src/cudarkdgsolver.cu:860-1001). */
 int rkdg_write_solution(rkdg_ctx* ctx, const char* path);
 
+/* ---- batched independent solves ----------------------------------------- */
+/* Many independent solves on meshes of uneven size and mixed order (P1
+ * and P2) packed into one element space: every RK stage of all solves is
+ * one launch of the tile-staged kernel over the concatenated tiles (a
+ * persistent pass when the autotuner picks fewer CTAs than tiles), each
+ * solve with its own dt, time, final time and monitor, and the whole step
+ * captured as one CUDA graph.  A solve's arithmetic does not depend on the
+ * others: its result equals the same solve run alone, bit for bit.
+ * No reference counterpart: the reference runs one solve per process
+ * (src/main.cpp:24-159). */
+typedef struct rkdg_batch rkdg_batch;
+
+/* orders[s]: 1 or 2 per solve; P2 solves use params->nq (6 or 7 for a
+ * P2-only batch, 6 when P1 and P2 are mixed) and 3 edge points, P1 solves
+ * the 3/2-point rules.  params->precision, flux, rk, gamma, cfl are shared;
+ * farfields [nsolves][4] gives each solve's far-field state (NULL: params). */
+int rkdg_batch_create(int32_t nsolves, const rkdg_mesh_desc* meshes, const int32_t* orders,
+                      const double* farfields, const rkdg_params* params, rkdg_batch** out);
+int rkdg_batch_destroy(rkdg_batch* b);
+/* Native-basis state of one solve, [4][nbasis(solve)][ld] in its caller order. */
+int rkdg_batch_set_state(rkdg_batch* b, int32_t solve, const double* U, int32_t ld);
+int rkdg_batch_get_state(rkdg_batch* b, int32_t solve, double* U, int32_t ld);
+/* nsteps device-resident steps of every solve; t_final[s] > 0 stops solve s
+ * there (NULL: none).  t[s] and steps[s] (may be NULL) receive each solve's
+ * time and step count. */
+int rkdg_batch_advance(rkdg_batch* b, int32_t nsteps, const double* t_final, double* t,
+                       int32_t* steps);
+int rkdg_batch_set_time(rkdg_batch* b, int32_t solve, double t);
+/* Picks the persistent grid size and tile order by timing candidate launch
+ * shapes on this batch; returns the chosen CTA count (0: one per tile) and
+ * tile order (0 solve order, 1 P2 tiles first). */
+int rkdg_batch_autotune(rkdg_batch* b, int32_t* ctas, int32_t* tile_order);
+int rkdg_batch_set_shape(rkdg_batch* b, int32_t ctas, int32_t tile_order);
+/* Mean device milliseconds of one launch of stage s over all solves. */
+int rkdg_batch_time_stage(rkdg_batch* b, int32_t s, int32_t reps, double* ms_per_launch);
+int rkdg_batch_get_sizes(const rkdg_batch* b, int64_t* elements, int32_t* ntiles, size_t* device_bytes);
+int rkdg_batch_get_stream(const rkdg_batch* b, void** stream);
+
 /* ---- mesh files -------------------------------------------------------- */
 /* Reads the reference's mesh set: the mesh configuration file
  * (trianglenum, verticenum, edgenum and the five file names) and the five

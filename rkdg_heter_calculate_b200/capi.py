@@ -84,6 +84,19 @@ def lib():
             "rkdg_locality_order": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(C.c_int32)]),
             "rkdg_conservation_totals_noalloc": (C.c_int, [C.c_int32, C.c_void_p, C.c_int32,
                                                            C.c_void_p, C.c_void_p, C.c_void_p]),
+            "rkdg_batch_create": (C.c_int, [C.c_int32, C.POINTER(MeshDesc), C.POINTER(C.c_int32),
+                                            _dp, C.POINTER(Params), C.POINTER(vp)]),
+            "rkdg_batch_destroy": (C.c_int, [vp]),
+            "rkdg_batch_set_state": (C.c_int, [vp, C.c_int32, _dp, C.c_int32]),
+            "rkdg_batch_get_state": (C.c_int, [vp, C.c_int32, _dp, C.c_int32]),
+            "rkdg_batch_advance": (C.c_int, [vp, C.c_int32, _dp, _dp, C.POINTER(C.c_int32)]),
+            "rkdg_batch_set_time": (C.c_int, [vp, C.c_int32, C.c_double]),
+            "rkdg_batch_autotune": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+            "rkdg_batch_set_shape": (C.c_int, [vp, C.c_int32, C.c_int32]),
+            "rkdg_batch_time_stage": (C.c_int, [vp, C.c_int32, C.c_int32, _dp]),
+            "rkdg_batch_get_sizes": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                                               C.POINTER(C.c_size_t)]),
+            "rkdg_batch_get_stream": (C.c_int, [vp, C.POINTER(vp)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

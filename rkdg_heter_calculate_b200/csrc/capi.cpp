@@ -43,6 +43,7 @@ struct rkdg_ctx {
     StepCtl* h_ctl = nullptr;  // pinned mirror of the device control block
     TileArgs tiles{};
     int variant = 1;  // 1 tile-staged (default), 0 owner-computes
+    int ctas = 0;     // tiled grid size (0: one CTA per tile)
 };
 
 namespace {
@@ -144,8 +145,8 @@ void normalise_buffers(rkdg_ctx* c) {
 
 void ensure_wave(rkdg_ctx* c) {
     if (c->wave_valid) return;
-    launch_wave(c->T, c->ld, c->d.U[c->cur], c->p.order, c->p.precision, c->d.jinv, c->p.gamma,
-                c->d.ctl, c->stream);
+    launch_wave(c->tiles, c->ld, c->d.U[c->cur], c->p.precision, c->d.jinv, c->p.gamma, c->d.ctl, 1,
+                c->stream);
     c->wave_valid = true;
 }
 
@@ -180,7 +181,7 @@ void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out) {
     a.U0 = s == 0 ? nullptr : c->d.U[u0];
     a.Unew = c->d.U[out];
     a.last_stage = s == c->p.rk - 1;
-    launch_stage(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
+    launch_stage(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->variant == 1 ? c->ctas : c->block, c->stream);
     if (c->p.limiter == RKDG_LIMITER_TVB)
         launch_limiter(c->T, c->ld, c->d.U[out], c->d.conn, c->d.lim, c->d.jinv, c->p.order,
                        c->p.nq, c->p.ng, c->p.precision, c->p.gamma, c->p.farfield, c->p.tvb_m,
@@ -189,7 +190,7 @@ void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out) {
 
 // one full step on the stream with the state in buffer 0 (graph-capturable)
 void enqueue_step(rkdg_ctx* c) {
-    launch_step_begin(c->d.ctl, c->stream);
+    launch_step_begin(c->d.ctl, 1, c->stream);
     if (c->p.rk == 3) {
         launch_one_stage(c, 0, 0, 0, 1);
         launch_one_stage(c, 1, 1, 0, 2);
@@ -222,9 +223,8 @@ void destroy_ctx(rkdg_ctx* c) {
     cudaFree(c->d.partial);
     cudaFree(c->d.ctl);
     cudaFree(c->d.tcode);
-    cudaFree(c->d.halo_ptr);
+    cudaFree(c->d.tdesc);
     cudaFree(c->d.halo);
-    cudaFree(c->d.task_ptr);
     cudaFree(c->d.task);
     if (c->h_ctl) cudaFreeHost(c->h_ctl);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -327,27 +327,23 @@ int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx*
                                           cudaMemcpyHostToDevice, c->stream));
         }
         {
-            TileTables tt = build_tiles(c->mesh);
+            TileTables tt = build_tiles(c->mesh, 0, 0, params->order, 0, 0);
             c->d.tcode = (int4*)dev_alloc(c, sizeof(int32_t) * tt.code.size());
-            c->d.halo_ptr = (int32_t*)dev_alloc(c, sizeof(int32_t) * tt.halo_ptr.size());
+            c->d.tdesc = (int4*)dev_alloc(c, sizeof(int32_t) * tt.desc.size());
             c->d.halo = (int2*)dev_alloc(c, sizeof(int32_t) * std::max<size_t>(2, tt.halo.size()));
-            c->d.task_ptr = (int32_t*)dev_alloc(c, sizeof(int32_t) * tt.task_ptr.size());
             c->d.task = (uint16_t*)dev_alloc(c, sizeof(uint16_t) * std::max<size_t>(1, tt.task.size()));
             RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.tcode, tt.code.data(), sizeof(int32_t) * tt.code.size(),
                                           cudaMemcpyHostToDevice, c->stream));
-            RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.halo_ptr, tt.halo_ptr.data(), sizeof(int32_t) * tt.halo_ptr.size(),
+            RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.tdesc, tt.desc.data(), sizeof(int32_t) * tt.desc.size(),
                                           cudaMemcpyHostToDevice, c->stream));
             if (!tt.halo.empty())
                 RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.halo, tt.halo.data(), sizeof(int32_t) * tt.halo.size(),
                                               cudaMemcpyHostToDevice, c->stream));
-            RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.task_ptr, tt.task_ptr.data(), sizeof(int32_t) * tt.task_ptr.size(),
-                                          cudaMemcpyHostToDevice, c->stream));
             RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.task, tt.task.data(), sizeof(uint16_t) * tt.task.size(),
                                           cudaMemcpyHostToDevice, c->stream));
             c->tiles.code = c->d.tcode;
-            c->tiles.halo_ptr = c->d.halo_ptr;
+            c->tiles.desc = c->d.tdesc;
             c->tiles.halo = c->d.halo;
-            c->tiles.task_ptr = c->d.task_ptr;
             c->tiles.task = c->d.task;
             c->tiles.max_halo = tt.max_halo;
             c->tiles.ntiles = tt.ntiles;
@@ -454,7 +450,7 @@ int rkdg_residual(rkdg_ctx* c, double* R, int32_t ld, int32_t basis) {
         a.Unew = c->d.U[scratch];
         a.a = 0;
         a.b = 1;
-        launch_residual(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
+        launch_residual(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->variant == 1 ? c->ctas : c->block, c->stream);
         launch_export(c->T, c->ld, c->d.U[scratch], basis == RKDG_BASIS_REFERENCE ? c->d.conv_in : nullptr,
                       c->d.perm, c->d.staging, c->T, c->p.order, c->p.precision, 1, c->d.jinv,
                       c->stream);
@@ -618,10 +614,10 @@ int rkdg_time_stage(rkdg_ctx* c, int32_t s, int32_t reps, double* ms) {
         cudaEvent_t e0, e1;
         RKDG_CUDA_TRY(cudaEventCreate(&e0));
         RKDG_CUDA_TRY(cudaEventCreate(&e1));
-        launch_stage(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
+        launch_stage(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->variant == 1 ? c->ctas : c->block, c->stream);
         RKDG_CUDA_TRY(cudaEventRecord(e0, c->stream));
         for (int i = 0; i < reps; ++i)
-            launch_stage(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->block, c->stream);
+            launch_stage(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->variant == 1 ? c->ctas : c->block, c->stream);
         RKDG_CUDA_TRY(cudaEventRecord(e1, c->stream));
         RKDG_CUDA_TRY(cudaEventSynchronize(e1));
         float t = 0;

@@ -484,28 +484,39 @@ __global__ void __launch_bounds__(128) stage_kernel(const StageArgs a) {
 
 #include "stage_tiled.cuh"
 
-// CFL measure of the current state (first step, rkdg_compute_dt).
+// CFL measure of the current state per solve (first step, rkdg_compute_dt):
+// one CTA per tile, a block max per tile, one atomicMax into its solve.
 template <typename Real>
-__global__ void __launch_bounds__(256) wave_kernel(int T, int ld, const Real* __restrict__ U,
-                                                   const double* __restrict__ jinv, double gamma,
-                                                   StepCtl* ctl) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kTile) wave_kernel(const TileArgs ta, int ld,
+                                                     const Real* __restrict__ U,
+                                                     const double* __restrict__ jinv, double gamma,
+                                                     StepCtl* ctl) {
+    const int4 d0 = __ldg(ta.desc + 2 * blockIdx.x);
+    const int e = d0.x + threadIdx.x;
+    StepCtl* c = ctl + d0.z;
     double w = 0.0;
-    if (e < T) {
+    if ((int)threadIdx.x < d0.y) {
         Real m[4];
         load_mean<Real, 1>(U, ld, e, m);
         const double2* j2 = reinterpret_cast<const double2*>(jinv);
         bool bad;
         w = wave_measure((double)m[0], (double)m[1], (double)m[2], (double)m[3], gamma, j2[e],
                          j2[ld + e], bad);
-        if (bad) atomicOr(&ctl->error, 1);
+        if (bad) atomicOr(&c->error, 1);
     }
-    block_max3_atomic(w, 0.0, 0.0, &ctl->wave_bits, nullptr, nullptr);
+    block_max3_atomic(w, 0.0, 0.0, &c->wave_bits, nullptr, nullptr);
+}
+
+__global__ void reset_wave_kernel(StepCtl* ctl, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) ctl[i].wave_bits = 0ull;
 }
 
 // dt of the step: CFL (or fixed), clipped to land on t_final; advances t.
-__global__ void step_begin_kernel(StepCtl* ctl) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__global__ void step_begin_kernel(StepCtl* ctls, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    StepCtl* ctl = ctls + i;
     if (ctl->done) return;
     double dt = ctl->dt_fixed > 0 ? ctl->dt_fixed : ctl->cfl / __longlong_as_double((long long)ctl->wave_bits);
     bool last = false;
@@ -776,63 +787,72 @@ __global__ void __launch_bounds__(kTotBlock) totals_final_kernel(int n, const do
 // ----------------------------------------------------------- launchers --
 namespace {
 
+template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
+void launch_tiled(const StageArgs& a, const TileArgs& t, int ctas, cudaStream_t s) {
+    const size_t smem = TiledSmem<Real, NQ2>::bytes(t.max_halo);
+    // dynamic + static shared memory above 48 KB needs the opt-in; the
+    // static part (tables, block reduction) is ~1.2 KB, so opt in early.
+    // Per instantiation; raised when a context with a larger halo appears.
+    static size_t configured = 0;
+    if (configured == 0)  // residency is register-limited: give shared memory the carveout
+        RKDG_CUDA_TRY(cudaFuncSetAttribute(tiled_stage_kernel<Real, NQ2, FLUX, MODE, ORD>,
+                                           cudaFuncAttributePreferredSharedMemoryCarveout,
+                                           (int)cudaSharedmemCarveoutMaxShared));
+    if (smem > configured) {
+        RKDG_CUDA_TRY(cudaFuncSetAttribute(tiled_stage_kernel<Real, NQ2, FLUX, MODE, ORD>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = smem;
+    }
+    const int grid = (ctas > 0 && ctas < t.ntiles) ? ctas : t.ntiles;
+    if (grid > 0) tiled_stage_kernel<Real, NQ2, FLUX, MODE, ORD><<<grid, kTile, smem, s>>>(a, t);
+}
+
+template <typename Real, int FLUX, int MODE>
+void dispatch_tiled(const StageArgs& a, const TileArgs& t, int order, int nq, int ctas,
+                    cudaStream_t s) {
+    if (order == 1) return launch_tiled<Real, 6, FLUX, MODE, 1>(a, t, ctas, s);
+    if (order == 2 && nq == 7) return launch_tiled<Real, 7, FLUX, MODE, 2>(a, t, ctas, s);
+    if (order == 2 && nq == 6) return launch_tiled<Real, 6, FLUX, MODE, 2>(a, t, ctas, s);
+    if (order == 3 && nq == 6) return launch_tiled<Real, 6, FLUX, MODE, 3>(a, t, ctas, s);
+    throw Error{RKDG_ERR_INVALID, "unsupported order/rule combination for the tiled kernel"};
+}
+
 template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE>
-void launch_variant(const StageArgs& a, const TileArgs& t, int variant, int block, cudaStream_t s) {
-    if (variant == 1) {
-        const size_t smem = TiledSmem<Real, NB, NQ, NG>::bytes(t.max_halo);
-        // dynamic + static shared memory above 48 KB needs the opt-in; the
-        // static part (tables, block reduction) is ~1.2 KB, so opt in early.
-        // Per instantiation; raised when a context with a larger halo appears.
-        static size_t configured = 0;
-        if (configured == 0)  // residency is register-limited: give shared memory the carveout
-            RKDG_CUDA_TRY(cudaFuncSetAttribute(tiled_stage_kernel<Real, NB, NQ, NG, FLUX, MODE>,
-                                               cudaFuncAttributePreferredSharedMemoryCarveout,
-                                               (int)cudaSharedmemCarveoutMaxShared));
-        if (smem > configured) {
-            RKDG_CUDA_TRY(cudaFuncSetAttribute(tiled_stage_kernel<Real, NB, NQ, NG, FLUX, MODE>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            configured = smem;
-        }
-        tiled_stage_kernel<Real, NB, NQ, NG, FLUX, MODE><<<t.ntiles, kTile, smem, s>>>(a, t);
-    } else {
-        const int grid = (a.T + block - 1) / block;
-        stage_kernel<Real, NB, NQ, NG, FLUX, MODE><<<grid, block, 0, s>>>(a);
-    }
+void launch_owner(const StageArgs& a, int block, cudaStream_t s) {
+    const int grid = (a.T + block - 1) / block;
+    stage_kernel<Real, NB, NQ, NG, FLUX, MODE><<<grid, block, 0, s>>>(a);
 }
 
-template <typename Real, int NB, int NQ, int NG, int MODE>
-void dispatch_flux(const StageArgs& a, const TileArgs& t, int variant, int flux, int block,
-                   cudaStream_t s) {
-    if (flux == RKDG_FLUX_HLLC)
-        launch_variant<Real, NB, NQ, NG, RKDG_FLUX_HLLC, MODE>(a, t, variant, block, s);
-    else
-        launch_variant<Real, NB, NQ, NG, RKDG_FLUX_LLF, MODE>(a, t, variant, block, s);
-}
-
-template <typename Real, int NB, int MODE>
-void dispatch_rule(const StageArgs& a, const TileArgs& t, int variant, int nq, int ng, int flux,
-                   int block, cudaStream_t s) {
-    // the rule pairs in use: P2 with 7/3 (the reference's) or 6/3 points,
-    // P1 with 3/2 points (rkdg_create rejects the others)
-    if constexpr (NB == 6) {
-        if (nq == 7 && ng == 3) return dispatch_flux<Real, NB, 7, 3, MODE>(a, t, variant, flux, block, s);
-        if (nq == 6 && ng == 3) return dispatch_flux<Real, NB, 6, 3, MODE>(a, t, variant, flux, block, s);
-    } else {
-        if (nq == 3 && ng == 2) return dispatch_flux<Real, NB, 3, 2, MODE>(a, t, variant, flux, block, s);
-    }
+template <typename Real, int FLUX, int MODE>
+void dispatch_owner(const StageArgs& a, int order, int nq, int ng, int block, cudaStream_t s) {
+    if (block != 64 && block != 128) block = 128;
+    if (order == 2 && nq == 7 && ng == 3) return launch_owner<Real, 6, 7, 3, FLUX, MODE>(a, block, s);
+    if (order == 2 && nq == 6 && ng == 3) return launch_owner<Real, 6, 6, 3, FLUX, MODE>(a, block, s);
+    if (order == 1 && nq == 3 && ng == 2) return launch_owner<Real, 3, 3, 2, FLUX, MODE>(a, block, s);
     throw Error{RKDG_ERR_INVALID, "unsupported quadrature combination"};
 }
 
 template <int MODE>
 void dispatch(const StageArgs& a, const TileArgs& t, int variant, int order, int nq, int ng,
               int flux, int prec, int block, cudaStream_t s) {
-    if (block != 64 && block != 128) block = 128;
-    if (prec == RKDG_FP32) {
-        if (order == 1) dispatch_rule<float, 3, MODE>(a, t, variant, nq, ng, flux, block, s);
-        else dispatch_rule<float, 6, MODE>(a, t, variant, nq, ng, flux, block, s);
+    const bool hllc = flux == RKDG_FLUX_HLLC;
+    if (variant == 1) {
+        if (prec == RKDG_FP32) {
+            if (hllc) dispatch_tiled<float, RKDG_FLUX_HLLC, MODE>(a, t, order, nq, block, s);
+            else dispatch_tiled<float, RKDG_FLUX_LLF, MODE>(a, t, order, nq, block, s);
+        } else {
+            if (hllc) dispatch_tiled<double, RKDG_FLUX_HLLC, MODE>(a, t, order, nq, block, s);
+            else dispatch_tiled<double, RKDG_FLUX_LLF, MODE>(a, t, order, nq, block, s);
+        }
     } else {
-        if (order == 1) dispatch_rule<double, 3, MODE>(a, t, variant, nq, ng, flux, block, s);
-        else dispatch_rule<double, 6, MODE>(a, t, variant, nq, ng, flux, block, s);
+        if (order == 3) throw Error{RKDG_ERR_INVALID, "the owner-computes kernel takes one order"};
+        if (prec == RKDG_FP32) {
+            if (hllc) dispatch_owner<float, RKDG_FLUX_HLLC, MODE>(a, order, nq, ng, block, s);
+            else dispatch_owner<float, RKDG_FLUX_LLF, MODE>(a, order, nq, ng, block, s);
+        } else {
+            if (hllc) dispatch_owner<double, RKDG_FLUX_HLLC, MODE>(a, order, nq, ng, block, s);
+            else dispatch_owner<double, RKDG_FLUX_LLF, MODE>(a, order, nq, ng, block, s);
+        }
     }
     RKDG_CUDA_TRY(cudaGetLastError());
 }
@@ -849,21 +869,26 @@ void launch_residual(const StageArgs& a, const TileArgs& t, int variant, int ord
     dispatch<MODE_RESIDUAL>(a, t, variant, order, nq, ng, flux, prec, block, stream);
 }
 
-void launch_wave(int T, int ld, const void* U, int order, int prec, const double* jinv,
-                 double gamma, StepCtl* ctl, cudaStream_t stream) {
-    (void)order;
-    RKDG_CUDA_TRY(cudaMemsetAsync(&ctl->wave_bits, 0, sizeof(unsigned long long), stream));
-    const int grid = (T + 255) / 256;
-    if (prec == RKDG_FP32)
-        wave_kernel<float><<<grid, 256, 0, stream>>>(T, ld, static_cast<const float*>(U), jinv, gamma, ctl);
-    else
-        wave_kernel<double><<<grid, 256, 0, stream>>>(T, ld, static_cast<const double*>(U), jinv, gamma, ctl);
+void launch_wave(const TileArgs& t, int ld, const void* U, int prec, const double* jinv,
+                 double gamma, StepCtl* ctl, int nsolves, cudaStream_t stream) {
+    reset_wave_kernel<<<(nsolves + 127) / 128, 128, 0, stream>>>(ctl, nsolves);
+    if (t.ntiles > 0) {
+        if (prec == RKDG_FP32)
+            wave_kernel<float><<<t.ntiles, kTile, 0, stream>>>(t, ld, static_cast<const float*>(U), jinv, gamma, ctl);
+        else
+            wave_kernel<double><<<t.ntiles, kTile, 0, stream>>>(t, ld, static_cast<const double*>(U), jinv, gamma, ctl);
+    }
     RKDG_CUDA_TRY(cudaGetLastError());
 }
 
-void launch_step_begin(StepCtl* ctl, cudaStream_t stream) {
-    step_begin_kernel<<<1, 32, 0, stream>>>(ctl);
+void launch_step_begin(StepCtl* ctl, int nsolves, cudaStream_t stream) {
+    step_begin_kernel<<<(nsolves + 127) / 128, 128, 0, stream>>>(ctl, nsolves);
     RKDG_CUDA_TRY(cudaGetLastError());
+}
+
+int tiled_max_ctas_per_sm(int prec, int order) {
+    if (prec == RKDG_FP32) return order == 1 ? TiledOccupancy<float, 1>::value : TiledOccupancy<float, 2>::value;
+    return order == 1 ? TiledOccupancy<double, 1>::value : TiledOccupancy<double, 2>::value;
 }
 
 void launch_limiter(int T, int ld, void* U, const int4* conn, const double* lim,

@@ -372,16 +372,17 @@ HostGeometry build_geometry(const HostMesh& m, int order, bool with_conversion, 
     return g;
 }
 
-TileTables build_tiles(const HostMesh& m) {
+TileTables build_tiles(const HostMesh& m, int elem_offset, int sid, int order, int halo_offset,
+                       int task_offset) {
     const int T = m.T, B = kTile;
     TileTables t;
     t.ntiles = (T + B - 1) / B;
     t.code.assign((size_t)4 * T, 0);
-    t.halo_ptr.assign(t.ntiles + 1, 0);
-    t.task_ptr.assign(t.ntiles + 1, 0);
+    t.desc.assign((size_t)8 * t.ntiles, 0);
     int maxh = 0;
     for (int tile = 0; tile < t.ntiles; ++tile) {
         const int e0 = tile * B, e1 = std::min(T, e0 + B);
+        const int h_begin = (int)(t.halo.size() / 2), k_begin = (int)t.task.size();
         int nh = 0;
         for (int k = 0; k < 3; ++k)  // tasks and halo slots sorted by edge, then element
             for (int e = e0; e < e1; ++e) {
@@ -399,7 +400,7 @@ TileTables build_tiles(const HostMesh& m) {
                 } else {
                     const int se = m.shared[3 * e + k];
                     code = EDGE_HALO | (se << 2) | (nh << 4);
-                    t.halo.push_back(n);
+                    t.halo.push_back(elem_offset + n);
                     t.halo.push_back(se);
                     ++nh;
                 }
@@ -407,8 +408,15 @@ TileTables build_tiles(const HostMesh& m) {
                 if (task) t.task.push_back((uint16_t)(le * 4 + k));
             }
         maxh = std::max(maxh, nh);
-        t.halo_ptr[tile + 1] = (int32_t)(t.halo.size() / 2);
-        t.task_ptr[tile + 1] = (int32_t)t.task.size();
+        int32_t* d = &t.desc[(size_t)8 * tile];
+        d[0] = elem_offset + e0;
+        d[1] = e1 - e0;
+        d[2] = sid;
+        d[3] = order;
+        d[4] = halo_offset + h_begin;
+        d[5] = nh;
+        d[6] = task_offset + k_begin;
+        d[7] = (int)t.task.size() - k_begin;
     }
     t.max_halo = std::max(4, (maxh + 3) / 4 * 4);
     return t;

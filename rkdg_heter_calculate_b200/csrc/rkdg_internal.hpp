@@ -102,16 +102,21 @@ uint32_t pack_info(const int8_t* shared3, const int8_t* bc3);
 constexpr int kTile = 128;
 enum { EDGE_IN_OWNER = 0, EDGE_IN_OTHER = 1, EDGE_HALO = 2, EDGE_BOUNDARY = 3 };
 
+// Tiles of one solve.  Element indices are global in the packed element
+// space (elem_offset + local), halo and task ranges index pool arrays at the
+// given offsets, so the tables of many solves concatenate.
+// desc per tile (8 ints): e0, count, solve id, order, halo_begin, nhalo,
+// task_begin, ntask.
 struct TileTables {
     int ntiles = 0;
     int max_halo = 0;                  // rounded up to a multiple of 4
     std::vector<int32_t> code;         // [T][4] (code of edges 0..2, unused)
-    std::vector<int32_t> halo_ptr;     // [ntiles + 1]
+    std::vector<int32_t> desc;         // [ntiles][8]
     std::vector<int32_t> halo;         // [nhalo][2] (global element, its edge)
-    std::vector<int32_t> task_ptr;     // [ntiles + 1]
     std::vector<uint16_t> task;        // local element * 4 + edge, sorted by edge
 };
-TileTables build_tiles(const HostMesh& m);
+TileTables build_tiles(const HostMesh& m, int elem_offset = 0, int sid = 0, int order = 2,
+                       int halo_offset = 0, int task_offset = 0);
 
 // ------------------------------------------------------------- device --
 struct StepCtl {
@@ -141,19 +146,17 @@ struct DeviceArrays {
     StepCtl* ctl = nullptr;
     // tile tables
     int4* tcode = nullptr;
-    int32_t* halo_ptr = nullptr;
+    int4* tdesc = nullptr;
     int2* halo = nullptr;
-    int32_t* task_ptr = nullptr;
     uint16_t* task = nullptr;
     size_t bytes = 0;
 };
 
 struct TileArgs {
-    const int4* code;
-    const int32_t* halo_ptr;
-    const int2* halo;
-    const int32_t* task_ptr;
-    const uint16_t* task;
+    const int4* code;   // [elements] per-edge source codes
+    const int4* desc;   // [ntiles][2] tile descriptors
+    const int2* halo;   // halo pool
+    const uint16_t* task;  // task pool
     int max_halo;
     int ntiles;
 };
@@ -169,20 +172,26 @@ struct StageArgs {
     double a, b;         // Unew = a U0 + b (U + dt L(U))
     double gamma;
     double far[4];
+    const double* far_sid;  // per-solve far-field states [solves][4], or nullptr
     int last_stage;      // compute wave max / monitor / error in the epilogue
 };
 
 // Launchers (kernels.cu).  All asynchronous on `stream`.
 void upload_tables(int nq, int ng);
 // variant: 0 owner-computes (one thread per element, both sides of every
-// edge), 1 tile-staged (each interior flux once per tile, traces shared)
+// edge; single solve, block = threads per block), 1 tile-staged (each
+// interior flux once per tile, traces shared; `block` = CTAs per launch,
+// 0 = one CTA per tile).  `order` 1 or 2, or 3 for a pack of P1 and P2
+// tiles (P2 tiles use nq, P1 tiles the 3/2-point rules).
 void launch_stage(const StageArgs& a, const TileArgs& t, int variant, int order, int nq, int ng,
                   int flux, int prec, int block, cudaStream_t stream);
 void launch_residual(const StageArgs& a, const TileArgs& t, int variant, int order, int nq,
                      int ng, int flux, int prec, int block, cudaStream_t stream);
-void launch_wave(int T, int ld, const void* U, int order, int prec, const double* jinv,
-                 double gamma, StepCtl* ctl, cudaStream_t stream);
-void launch_step_begin(StepCtl* ctl, cudaStream_t stream);
+// CFL measure per solve, one CTA per tile (resets the solves' wave slots first)
+void launch_wave(const TileArgs& t, int ld, const void* U, int prec, const double* jinv,
+                 double gamma, StepCtl* ctl, int nsolves, cudaStream_t stream);
+void launch_step_begin(StepCtl* ctl, int nsolves, cudaStream_t stream);
+int tiled_max_ctas_per_sm(int prec, int order);
 void launch_limiter(int T, int ld, void* U, const int4* conn, const double* lim,
                     const double* jinv, int order, int nq, int ng, int prec, double gamma,
                     const double* far, double tvb_m, cudaStream_t stream);

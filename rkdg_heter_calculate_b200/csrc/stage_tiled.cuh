@@ -1,6 +1,8 @@
 // Tile-staged fused stage kernel (included by kernels.cu).
 //
-// A CTA owns kTile consecutive elements of the locality-ordered mesh.
+// A tile is up to kTile consecutive (locality-ordered) elements of one
+// solve; its descriptor names the element range, the solve, the polynomial
+// order, and its halo and flux-task ranges.  One CTA processes a tile:
 //   phase A  each thread: its element's state, volume integral (registers),
 //            traces at the 3*NG edge points and cell mean -> shared memory;
 //            the CTA together: traces of the out-of-tile (halo) neighbours
@@ -13,13 +15,18 @@
 //   phase C  each thread adds its three edges' fluxes (its own slot, or the
 //            negated flux of the in-tile neighbour that computed it) to the
 //            residual and applies the stage update.
-// Compared with one-thread-per-element owner-computes, in-tile traces are
-// evaluated once and in-tile fluxes computed once, with no atomics: the
-// result is deterministic and independent of how many solves are in flight.
+// The kernel loops over tiles (tile = blockIdx.x + k * gridDim.x), so one
+// launch serves a single solve (one CTA per tile) or a persistent pass over
+// the packed tiles of many solves of uneven size and mixed order, each with
+// its own dt, CFL measure and monitor.  A tile's arithmetic depends only on
+// its own solve's data: results are deterministic and identical whether a
+// solve runs alone or in a batch.
 
-template <typename Real, int NB, int NQ, int NG>
+template <typename Real, int NQ2>
 struct TiledSmem {
+    // sized for the larger (P2, 3 edge points) layout; P1 tiles use a prefix
     static constexpr size_t bytes(int hm) {
+        constexpr int NG = 3;
         return sizeof(double) * 5 * kTile +
                sizeof(Real) * ((size_t)3 * NG * 4 * kTile + 4 * kTile + (size_t)NG * 4 * hm + 4 * hm);
     }
@@ -27,18 +34,17 @@ struct TiledSmem {
 
 // Resident CTAs per SM the register allocation is held to (FP64 P2 would
 // otherwise take ~218 registers and leave 8 warps per SM).
-template <typename Real, int NB>
+template <typename Real, int ORD>
 struct TiledOccupancy {
-    static constexpr int value = sizeof(Real) == 8 ? (NB == 6 ? 3 : 4) : (NB == 6 ? 5 : 8);
+    static constexpr int value = sizeof(Real) == 8 ? (ORD == 1 ? 4 : 3) : (ORD == 1 ? 8 : 5);
 };
 
 template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE>
-__global__ void __launch_bounds__(kTile, TiledOccupancy<Real, NB>::value)
-    tiled_stage_kernel(const StageArgs a, const TileArgs ta) {
+__device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& ta, const int4 d0,
+                                           const int4 d1, unsigned char* smem_raw) {
     constexpr int CFG = cfg_index(NQ, NG);
     constexpr int BT = kTile;
     const Tab<Real>& tb = tab<Real>(CFG);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int HM = ta.max_halo;
     double* s_jinv = reinterpret_cast<double*>(smem_raw);  // [4][BT]
     double* s_area2 = s_jinv + 4 * BT;                     // [BT] twice the area
@@ -51,16 +57,19 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, NB>::value)
         int k = x / (NG * NB), g = (x / NB) % NG, i = x % NB;
         s_ephi[k][g][i] = tb.ephi[k][g][i];
     }
-    if (MODE == MODE_STAGE && a.ctl->done) return;  // uniform over the grid
+    const int sid = d0.z;
+    StepCtl* ctl = a.ctl + sid;
+    if (MODE == MODE_STAGE && ctl->done) return;  // uniform over the CTA
 
     const int tid = threadIdx.x;
-    const int e0 = blockIdx.x * BT;
+    const int e0 = d0.x;
     const int e = e0 + tid;
-    const bool active = e < a.T;
+    const bool active = tid < d0.y;
     const int ee = active ? e : e0;
     const Real* __restrict__ U = static_cast<const Real*>(a.U);
     const Real gamma = (Real)a.gamma, gm1 = gamma - Real(1);
-    Real far[4] = {(Real)a.far[0], (Real)a.far[1], (Real)a.far[2], (Real)a.far[3]};
+    const double* fs = a.far_sid ? a.far_sid + 4 * sid : a.far;
+    Real far[4] = {(Real)fs[0], (Real)fs[1], (Real)fs[2], (Real)fs[3]};
 
     // ------------------------------------------------------------ phase A
     Real R[NB][4];
@@ -118,7 +127,7 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, NB>::value)
     }
     __syncthreads();  // s_ephi visible below; own traces complete
     {
-        const int h0 = ta.halo_ptr[blockIdx.x], nh = ta.halo_ptr[blockIdx.x + 1] - h0;
+        const int h0 = d1.x, nh = d1.y;
         for (int h = tid; h < nh; h += BT) {
             const int2 hh = __ldg(ta.halo + h0 + h);
             Real un[NB][4];
@@ -140,7 +149,7 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, NB>::value)
 
     // ------------------------------------------------------------ phase B
     {
-        const int t0 = ta.task_ptr[blockIdx.x], nt = ta.task_ptr[blockIdx.x + 1] - t0;
+        const int t0 = d1.z, nt = d1.w;
         for (int j = tid; j < nt; j += BT) {
             const int tk = __ldg(ta.task + t0 + j);
             const int le = tk >> 2, k = tk & 3;
@@ -259,7 +268,7 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, NB>::value)
         if (active) store_state<Real, NB>(Uout, a.ld, e, R);
         return;
     }
-    const double dtd = a.ctl->dt;
+    const double dtd = ctl->dt;
     const Real dt = (Real)dtd, ca = (Real)a.a, cb = (Real)a.b;
     Real u0m[4] = {Real(0), Real(0), Real(0), Real(0)};
     {
@@ -288,10 +297,26 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, NB>::value)
             bool bad;
             wv = wave_measure((double)R[0][0], (double)R[0][1], (double)R[0][2], (double)R[0][3],
                               a.gamma, r0, r1, bad);
-            if (bad) atomicOr(&a.ctl->error, 1);
+            if (bad) atomicOr(&ctl->error, 1);
             m0 = fabs((double)R[0][0] - (double)u0m[0]);
             m1 = fabs((double)R[0][3] - (double)u0m[3]);
         }
-        block_max3_atomic(wv, m0, m1, &a.ctl->wave_bits, &a.ctl->mon_bits[0], &a.ctl->mon_bits[1]);
+        block_max3_atomic(wv, m0, m1, &ctl->wave_bits, &ctl->mon_bits[0], &ctl->mon_bits[1]);
+    }
+}
+
+// ORD: 1 = P1 tiles only, 2 = P2 tiles only, 3 = both (dispatch per tile;
+// P2 tiles use the NQ2-point volume rule, P1 tiles the 3/2-point rules).
+template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
+__global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
+    tiled_stage_kernel(const StageArgs a, const TileArgs ta) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    for (int tile = blockIdx.x; tile < ta.ntiles; tile += gridDim.x) {
+        const int4 d0 = __ldg(ta.desc + 2 * tile), d1 = __ldg(ta.desc + 2 * tile + 1);
+        if (ORD == 2 || (ORD == 3 && d0.w == 2))
+            tile_stage<Real, 6, NQ2, 3, FLUX, MODE>(a, ta, d0, d1, smem_raw);
+        else
+            tile_stage<Real, 3, 3, 2, FLUX, MODE>(a, ta, d0, d1, smem_raw);
+        __syncthreads();  // shared memory is reused by the next tile
     }
 }
