@@ -1,26 +1,31 @@
 #!/usr/bin/env python
 """Benchmark of the RKDG residual + time-step path on one B200 (or N replicas).
 
-Workload (default): the unstructured isentropic vortex -- periodic [0,10]^2,
-Delaunay triangulation of a 700 x 700 lattice jittered by U(-0.3h, 0.3h)
-(seed 2, 980,000 triangles), P2, 6-point volume and 3-point edge rules,
-HLLC, SSP-RK3, CFL 0.2; synthetic data (seeded), no external dataset.
+Headline workload (default, --workload batched): 64 independent isentropic-
+vortex solves, vortex strength U[1,5] and free-stream angle U[0, 2 pi)
+(free-stream speed sqrt(2)), seeded (numpy default_rng(4)); periodic
+Delaunay meshes of jittered lattices with triangle counts log-uniform in
+[5k, 200k]; P1 and P2 (Bernoulli 1/2); FP32 state with FP64 geometry and dt;
+HLLC, SSP-RK3, CFL 0.2; 200 steps each; one launch per RK stage over all
+solves, CUDA graph, autotuned launch shape.  Synthetic data, no dataset.
+
+Beside it, the plain FP64 single solve on the unstructured vortex (periodic
+Delaunay of a 700 x 700 lattice jittered by +-0.3h, seed 2, 980,000
+triangles, P2, 6/3-point rules, HLLC, SSP-RK3) and its FP32 form.
 
 One JSON line on rank 0:
-  value        FP32 DOF-stage updates/s with the state resident in HBM
-               (FP32 state/arithmetic, FP64 geometry and dt), K steps timed
-               with CUDA events on the solver's stream, max over ranks;
-  fp64         the same for the plain FP64 path;
-  roofline     achieved HBM GB/s of the fused stage kernel: algorithmic bytes
-               per element-stage B = 4 Nb w (2 + r_s) + 56 (r_s = 2/3 mean
-               over SSP-RK3) times elements, over the event-timed launch;
-  e2e          the same metric through the C ABI with host buffers in the
-               reference's layout and basis: set_state + K steps + get_state;
+  value        batched FP32 DOF-stage updates/s, state resident in HBM, K steps
+               timed with CUDA events on the batch's stream, max over ranks;
+  plain_fp64   single-solve FP64 DOF-stage/s on the 980k mesh (and its FP32 form);
+  roofline     achieved HBM GB/s of the fused stage kernel over all solves:
+               algorithmic bytes per element-stage 4 Nb w (2 + r_s) + 56
+               (r_s = 2/3 mean over SSP-RK3) over the event-timed launch;
+  e2e          the batched metric through the C ABI with host buffers: every
+               solve's set_state + K steps + get_state;
   cpu_baseline the reference's own code (oracle/_ref, compiled from its
                sources for the host) on a bounded sample, all host threads;
-  l2           vortex L2(rho) error vs the exact solution at t_final for FP32
-               and FP64 (the FP64 path is the one parity-checked against the
-               oracle at 1e-12).
+  l2           vortex L2(rho) error vs the exact solution: batched FP32 vs FP64
+               per solve after 200 steps, and the 980k solve at t = 2.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 """
@@ -42,6 +47,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "DOF-stage updates/s"
 UNIT = "DOF-stage/s"
+GAMMA = 1.4
 
 
 def parse():
@@ -50,9 +56,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "vortex"])
+    ap.add_argument("--nsolves", type=int, default=64)
     ap.add_argument("--lattice", type=int, default=700)
-    ap.add_argument("--t-final", type=float, default=2.0, help="vortex time of the L2 error runs")
+    ap.add_argument("--plain-steps", type=int, default=50)
+    ap.add_argument("--t-final", type=float, default=2.0, help="vortex time of the 980k L2 runs")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the single-solve measurements")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--precision", default="both", choices=["both", "fp32", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
@@ -88,25 +98,25 @@ class Dist:
 
             dist.barrier()
 
-    def max(self, x: float) -> float:
+    def _reduce(self, x, op):
         if not self.pg:
             return x
         import torch
         import torch.distributed as dist
 
         t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=op)
         return float(t.item())
+
+    def max(self, x: float) -> float:
+        import torch.distributed as dist
+
+        return self._reduce(x, dist.ReduceOp.MAX) if self.pg else x
 
     def sum(self, x: float) -> float:
-        if not self.pg:
-            return x
-        import torch
         import torch.distributed as dist
 
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+        return self._reduce(x, dist.ReduceOp.SUM) if self.pg else x
 
     def close(self):
         if self.pg:
@@ -173,60 +183,43 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-# ------------------------------------------------------------- workload --
-def vortex_mesh(lattice: int):
-    from rkdg_heter_calculate_b200 import meshgen
-
-    return meshgen.periodic_delaunay(lattice, L=10.0, jitter=0.3, seed=2)
+# ------------------------------------------------------------ workloads --
+def conservative(rho, u, v, p):
+    return (rho, rho * u, rho * v, p / (GAMMA - 1) + 0.5 * rho * (u * u + v * v))
 
 
-FAR = (1.0, 1.0, 1.0, 2.5 + 1.0)  # rho=1, u=v=1, p=1, gamma=1.4: E = p/0.4 + 1
+FAR_C2 = conservative(1.0, 1.0, 1.0, 1.0)
 
 
-def solver_for(mesh, precision):
-    from rkdg_heter_calculate_b200 import CUDARkdgSolver
+def batched_problems(n=64, seed=4):
+    """The 64 uneven vortex solves: (meshes, orders, initial native states,
+    far fields, (beta, uinf, vinf) per solve)."""
+    from rkdg_heter_calculate_b200 import meshgen, vortex
 
-    return CUDARkdgSolver(mesh, order=2, nq=6, ng=3, flux="hllc", rk=3, precision=precision,
-                          gamma=1.4, cfl=0.2, farfield=FAR, reorder=True)
+    rng = np.random.default_rng(seed)
+    betas = rng.uniform(1.0, 5.0, n)
+    thetas = rng.uniform(0.0, 2 * math.pi, n)
+    tris = np.exp(rng.uniform(math.log(5e3), math.log(2e5), n))
+    orders = np.where(rng.random(n) < 0.5, 1, 2).astype(np.int32)
+    mesh_seeds = rng.integers(0, 2 ** 31, n)
+    meshes, states, fars, par = [], [], [], []
+    for i in range(n):
+        lat = max(4, int(round(math.sqrt(tris[i] / 2.0))))
+        m = meshgen.periodic_delaunay(lat, L=10.0, jitter=0.3, seed=int(mesh_seeds[i]))
+        ui, vi = math.sqrt(2) * math.cos(thetas[i]), math.sqrt(2) * math.sin(thetas[i])
+        nb = 3 if orders[i] == 1 else 6
+        b = float(betas[i])
+        U = vortex.project_native(m, lambda X, Y, b=b, ui=ui, vi=vi: vortex.exact(X, Y, 0.0, b, GAMMA, ui, vi), nb, n=4)
+        meshes.append(m)
+        states.append(U)
+        fars.append(conservative(1.0, ui, vi, 1.0))
+        par.append((b, ui, vi))
+    return meshes, orders, states, fars, par
 
 
 def bytes_per_elem_stage(nb: int, word: int, rk: int = 3) -> float:
     r = {3: 2.0 / 3.0, 2: 0.5}[rk]
     return 4 * nb * word * (2 + r) + 56
-
-
-def time_steps(s, U0, K, W, dist, stream_ptr):
-    import torch
-
-    s.setFreedom(U0, basis="native")
-    s.set_time(0.0)
-    s.advance(W)
-    st = torch.cuda.ExternalStream(stream_ptr)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    dist.barrier()
-    torch.cuda.synchronize()
-    e0.record(st)
-    _, n = s.advance(K)
-    e1.record(st)
-    torch.cuda.synchronize()
-    dist.barrier()
-    ms = e0.elapsed_time(e1)
-    assert n == K
-    return dist.max(ms)
-
-
-def stage_roofline(s, T, nb, word, peak_gbs):
-    t0 = s.time_stage(0, 10)
-    t1 = s.time_stage(1, 10)
-    t_avg = (t0 + 2 * t1) / 3.0  # SSP-RK3: one stage without U^n, two with
-    B = bytes_per_elem_stage(nb, word)
-    achieved = T * B / (t_avg * 1e-3) / 1e9
-    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak_gbs, "unit": "GB/s",
-            "frac": round(achieved / peak_gbs, 4), "traffic": None,
-            "kernel": "stage_kernel", "ms_per_launch": {"stage_without_U0": round(t0, 5),
-                                                        "stage_with_U0": round(t1, 5)},
-            "bytes_per_element_stage": B}
 
 
 def measured_peak():
@@ -239,50 +232,170 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def e2e_run(s, U0_native, K, dist, stream_ptr):
-    """set_state (host, reference basis) + K steps + get_state (host)."""
+def event_time(stream_ptr, fn, dist):
     import torch
 
-    s.setFreedom(U0_native, basis="native")
-    Uref = s.copyFreedomToHost(basis="reference")
-    pinned = torch.empty(Uref.shape, dtype=torch.float64, pin_memory=True)
-    host = pinned.numpy()
-    host[...] = Uref
-    out_pinned = torch.empty(Uref.shape, dtype=torch.float64, pin_memory=True)
-    out = out_pinned.numpy()
-    # warm (allocates the conversion tables and staging once)
-    s.setFreedom(host, basis="reference")
-    s.advance(2)
-    s.copyFreedomToHost(basis="reference")
+    st = torch.cuda.ExternalStream(stream_ptr)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
     dist.barrier()
     torch.cuda.synchronize()
-    t = time.perf_counter()
-    s.setFreedom(host, basis="reference")
-    s.set_time(0.0)
-    s.advance(K)
-    from rkdg_heter_calculate_b200 import capi
-
-    capi.check(capi.lib().rkdg_get_state(s.h, capi.dptr(out), s.T, capi.BASIS_REFERENCE))
+    e0.record(st)
+    fn()
+    e1.record(st)
     torch.cuda.synchronize()
-    wall = time.perf_counter() - t
     dist.barrier()
-    return dist.max(wall), host.nbytes
+    return dist.max(e0.elapsed_time(e1))
 
 
-def accuracy(mesh, U0, t_final):
-    from rkdg_heter_calculate_b200 import vortex
+def roofline(t0, t1, alg_bytes, peak, peak_kind, kernel):
+    t_avg = (t0 + 2 * t1) / 3.0  # SSP-RK3: one stage without U^n, two with
+    achieved = alg_bytes / (t_avg * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": None, "kernel": kernel,
+            "peak_kind": peak_kind,
+            "ms_per_launch": {"stage_without_U0": round(t0, 5), "stage_with_U0": round(t1, 5)},
+            "algorithmic_bytes_per_launch": alg_bytes}
 
-    ex = lambda X, Y: vortex.exact(X, Y, t_final)  # noqa: E731
-    out = {"t_final": t_final}
-    for prec in ("fp64", "fp32"):
+
+def pinned_like(a):
+    import torch
+
+    t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+    h = t.numpy()
+    h[...] = a
+    return t, h
+
+
+# ------------------------------------------------------- batched (C4) --
+def run_batched(args, dist, peak, peak_kind):
+    from rkdg_heter_calculate_b200 import capi, vortex
+    from rkdg_heter_calculate_b200.batch import Batch
+
+    K, W = args.steps, args.warmup
+    meshes, orders, states, fars, par = batched_problems(args.nsolves)
+    nbs = [3 if o == 1 else 6 for o in orders]
+    dofs = sum(m.ntri * 4 * nb for m, nb in zip(meshes, nbs))
+    out = {}
+    precs = [p for p in ("fp32", "fp64") if args.precision in ("both", p)]
+    for prec in precs:
+        word = 4 if prec == "fp32" else 8
+        b = Batch(meshes, orders, precision=prec, flux="hllc", rk=3, nq=6, cfl=0.2, farfields=fars)
+        for i, U in enumerate(states):
+            b.set_state(i, U)
+        ctas, torder = b.autotune()
+        for i, U in enumerate(states):
+            b.set_state(i, U)
+            b.set_time(i, 0.0)
+        b.advance(W)
+        sp = b.stream()
+        clocks = None
+        if prec == "fp32":
+            with ClockSampler(dist.local) as cs:
+                ms = event_time(sp, lambda: b.advance(K), dist)
+            clocks = cs.summary()
+        else:
+            ms = event_time(sp, lambda: b.advance(K), dist)
+        value = dist.sum(dofs * 3 * K) / (ms * 1e-3)
+        alg = sum(m.ntri * bytes_per_elem_stage(nb, word) for m, nb in zip(meshes, nbs))
+        roof = roofline(b.time_stage(0, 10), b.time_stage(1, 10), alg, peak, peak_kind,
+                        "tiled_stage_kernel (P1+P2 tiles, one launch per stage)")
+        e2e = None
+        if not args.no_e2e:
+            hosts = [pinned_like(U) for U in states]
+            outs = [pinned_like(np.zeros_like(U)) for U in states]
+            for i, (_, h) in enumerate(hosts):
+                b.set_state(i, h)
+            b.advance(2)
+            dist.barrier()
+            t = time.perf_counter()
+            for i, (_, h) in enumerate(hosts):
+                capi.check(capi.lib().rkdg_batch_set_state(b.h, i, capi.dptr(h), h.shape[2]))
+                b.set_time(i, 0.0)
+            b.advance(K)
+            for i, (_, h) in enumerate(outs):
+                capi.check(capi.lib().rkdg_batch_get_state(b.h, i, capi.dptr(h), h.shape[2]))
+            wall = dist.max(time.perf_counter() - t)
+            nbytes = sum(h.nbytes for _, h in hosts)
+            e2e = {"value": dist.sum(dofs * 3 * K) / wall, "unit": UNIT,
+                   "h2d_bytes_per_step": nbytes / K, "d2h_bytes_per_step": nbytes / K,
+                   "timed": "per solve set_state (pinned host, native basis) + K steps + get_state"}
+        acc = None
+        if not args.no_accuracy:
+            for i, U in enumerate(states):
+                b.set_state(i, U)
+                b.set_time(i, 0.0)
+            t_end, _ = b.advance(200)
+            acc = []
+            for i, m in enumerate(meshes):
+                beta, ui, vi = par[i]
+                acc.append(vortex.l2_error(m, b.state(i), lambda X, Y: vortex.exact(X, Y, t_end[i], beta, GAMMA, ui, vi)))
+        out[prec] = {"value": value, "ms_per_step": ms / K, "roofline": roof, "e2e": e2e,
+                     "clocks": clocks, "shape": {"ctas": ctas, "tile_order": torder},
+                     "l2": acc}
+        b.close()
+    info = {"solves": len(meshes), "triangles": int(sum(m.ntri for m in meshes)),
+            "p1_solves": int((orders == 1).sum()), "p2_solves": int((orders == 2).sum()),
+            "dofs": int(dofs), "min_tris": int(min(m.ntri for m in meshes)),
+            "max_tris": int(max(m.ntri for m in meshes))}
+    return out, info
+
+
+# ------------------------------------------------- single solve (C2) --
+def solver_for(mesh, precision):
+    from rkdg_heter_calculate_b200 import CUDARkdgSolver
+
+    return CUDARkdgSolver(mesh, order=2, nq=6, ng=3, flux="hllc", rk=3, precision=precision,
+                          gamma=GAMMA, cfl=0.2, farfield=FAR_C2, reorder=True)
+
+
+def run_plain(args, dist, peak, peak_kind, K):
+    from rkdg_heter_calculate_b200 import capi, meshgen, vortex
+
+    mesh = meshgen.periodic_delaunay(args.lattice, L=10.0, jitter=0.3, seed=2)
+    T = mesh.ntri
+    U0 = vortex.project_native(mesh, lambda X, Y: vortex.exact(X, Y, 0.0), 6, n=4)
+    out = {}
+    precs = [p for p in ("fp32", "fp64") if args.precision in ("both", p)]
+    for prec in precs:
+        word = 4 if prec == "fp32" else 8
         s = solver_for(mesh, prec)
         s.setFreedom(U0, basis="native")
-        t, n = s.advance(10 ** 7, t_final=t_final)
-        U = s.copyFreedomToHost(basis="native")
-        out[prec] = {"l2_rho": vortex.l2_error(mesh, U, ex), "steps": n, "t": t}
+        s.advance(args.warmup)
+        ms = event_time(s.stream(), lambda: s.advance(K), dist)
+        value = dist.sum(T * 24 * 3 * K) / (ms * 1e-3)
+        roof = roofline(s.time_stage(0, 10), s.time_stage(1, 10), T * bytes_per_elem_stage(6, word),
+                        peak, peak_kind, "tiled_stage_kernel (P2)")
+        e2e = None
+        if not args.no_e2e:
+            s.setFreedom(U0, basis="native")
+            Uref = s.copyFreedomToHost(basis="reference")
+            _, host = pinned_like(Uref)
+            _, res = pinned_like(np.zeros_like(Uref))
+            s.setFreedom(host)
+            s.advance(2)
+            s.copyFreedomToHost()
+            dist.barrier()
+            t = time.perf_counter()
+            s.setFreedom(host)  # reference basis and layout
+            s.set_time(0.0)
+            s.advance(K)
+            capi.check(capi.lib().rkdg_get_state(s.h, capi.dptr(res), T, capi.BASIS_REFERENCE))
+            wall = dist.max(time.perf_counter() - t)
+            e2e = {"value": dist.sum(T * 24 * 3 * K) / wall, "unit": UNIT,
+                   "h2d_bytes_per_step": host.nbytes / K, "d2h_bytes_per_step": host.nbytes / K,
+                   "timed": "set_state (pinned host, reference basis) + K steps + get_state"}
+        acc = None
+        if not args.no_accuracy:
+            s.setFreedom(U0, basis="native")
+            s.set_time(0.0)
+            t, n = s.advance(10 ** 7, t_final=args.t_final)
+            acc = {"l2_rho": vortex.l2_error(mesh, s.copyFreedomToHost(basis="native"),
+                                             lambda X, Y: vortex.exact(X, Y, t)),
+                   "t": t, "steps": n}
+        out[prec] = {"value": value, "ms_per_step": ms / K, "roofline": roof, "e2e": e2e, "l2": acc}
         s.close()
-    out["ratio_fp32_over_fp64"] = out["fp32"]["l2_rho"] / out["fp64"]["l2_rho"]
-    return out
+    return out, T
 
 
 # --------------------------------------------------------- CPU baselines --
@@ -298,7 +411,7 @@ def cpu_reference_sample(seconds: float, threads: int | None = None):
     T = mesh.ntri
     if ref.available():
         ref.set_threads(threads)
-        c = ref.RefCase(mesh, gamma=1.4, alpha_deg=45.0, mach=math.sqrt(2.0 / 1.4), cfl=0.2,
+        c = ref.RefCase(mesh, gamma=GAMMA, alpha_deg=45.0, mach=math.sqrt(2.0 / GAMMA), cfl=0.2,
                         threads_per_block=64)
         c.init_freestream()
         c.advance(1)
@@ -314,9 +427,9 @@ def cpu_reference_sample(seconds: float, threads: int | None = None):
                   f"vortex mesh, {n} steps")
     else:
         oracle.set_threads(threads)
-        o = oracle.Oracle(mesh, order=2, nq=6, ng=3, flux=oracle.HLLC, rk=3, cfl=0.2, farfield=FAR)
+        o = oracle.Oracle(mesh, order=2, nq=6, ng=3, flux=oracle.HLLC, rk=3, cfl=0.2, farfield=FAR_C2)
         U = np.zeros((4, 6, T))
-        U[:, 0, :] = np.array(FAR)[:, None]
+        U[:, 0, :] = np.array(FAR_C2)[:, None]
         o.set_state(U)
         o.step()
         t = time.perf_counter()
@@ -346,7 +459,7 @@ def run_reference_arm(args, dist):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "unstructured isentropic vortex (bounded CPU sample)"},
+            "config": {"workload": "isentropic vortex on periodic Delaunay meshes (bounded CPU sample)"},
             "cpu_baseline": desc,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -362,63 +475,80 @@ def main():
     dist.init()
     import torch  # noqa: F401
 
-    from rkdg_heter_calculate_b200 import vortex
-
-    K, W = args.steps, args.warmup
-    mesh = vortex_mesh(args.lattice)
-    T = mesh.ntri
-    U0 = vortex.project_native(mesh, lambda X, Y: vortex.exact(X, Y, 0.0), 6)
     peak, peak_kind = measured_peak()
-    res = {}
-    clocks = None
-    precs = [(p, w) for p, w in (("fp32", 4), ("fp64", 8)) if args.precision in ("both", p)]
-    for prec, word in precs:
-        s = solver_for(mesh, prec)
-        sp = s.stream()
-        if prec == "fp32":
-            with ClockSampler(dist.local) as cs:
-                ms = time_steps(s, U0, K, W, dist, sp)
-            clocks = cs.summary()
-        else:
-            ms = time_steps(s, U0, K, W, dist, sp)
-        dofs = T * 24
-        value = dist.sum(dofs * 3 * K) / (ms * 1e-3)
-        roof = stage_roofline(s, T, 6, word, peak)
-        roof["peak_kind"] = peak_kind
-        e2e = None
-        if not args.no_e2e:
-            e2e_wall, state_bytes = e2e_run(s, U0, K, dist, sp)
-            e2e = {"value": dist.sum(dofs * 3 * K) / e2e_wall, "unit": UNIT,
-                   "h2d_bytes_per_step": state_bytes / K, "d2h_bytes_per_step": state_bytes / K}
-        res[prec] = {"value": value, "ms_per_step": ms / K, "roofline": roof, "e2e": e2e}
-        s.close()
-    acc = None
-    if not args.no_accuracy:
-        acc = accuracy(mesh, U0, args.t_final)
-    cpu = None
-    if dist.rank == 0 and not args.no_cpu:
-        _, cpu = cpu_reference_sample(args.cpu_seconds)
-    if dist.rank == 0:
+    line = None
+    if args.workload == "batched":
+        res, info = run_batched(args, dist, peak, peak_kind)
+        plain = None
+        if not args.no_plain:
+            plain, T2 = run_plain(args, dist, peak, peak_kind, args.plain_steps)
         head = "fp32" if "fp32" in res else "fp64"
         r = res[head]
-        other = res.get("fp64") if head == "fp32" else None
-        line = {
-            "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": dist.world,
-            "steps": K, "warmup": W, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if head == "fp32" else "f64",
-            "data": "synthetic",
-            "config": {"workload": "unstructured isentropic vortex: periodic Delaunay of a "
-                                   f"{args.lattice}x{args.lattice} lattice jittered +-0.3h (seed 2), "
-                                   f"{T} triangles, P2, 6-pt volume / 3-pt edge, HLLC, SSP-RK3, CFL 0.2",
-                       "triangles": T, "dofs": T * 24, "precision": "FP32 state/arithmetic, FP64 geometry+dt",
-                       "parallelism": f"{dist.world} independent replica(s), no collective",
-                       "l2_flush": "inputs larger than L2 (state 3 x 94 MB FP32 / 188 MB FP64 per step)"},
-            "roofline": r["roofline"], "e2e": r["e2e"],
-            "fp64": other,
-            "fp32_over_fp64": (r["value"] / other["value"]) if other else None,
-            "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": 4 * K,
-            "l2": acc,
-        }
+        cpu = None
+        if dist.rank == 0 and not args.no_cpu:
+            _, cpu = cpu_reference_sample(args.cpu_seconds)
+        if dist.rank == 0:
+            l2 = None
+            if r.get("l2") is not None and "fp64" in res and res["fp64"].get("l2") is not None:
+                ratio = np.array(r["l2"]) / np.array(res["fp64"]["l2"])
+                l2 = {"batched_fp32_over_fp64_max": float(ratio.max()),
+                      "batched_fp32_over_fp64_median": float(np.median(ratio)),
+                      "batched_fp64_l2_rho_median": float(np.median(res["fp64"]["l2"])),
+                      "steps": 200}
+            if plain and plain.get("fp64", {}).get("l2"):
+                l2 = dict(l2 or {})
+                l2["plain_980k_fp64"] = plain["fp64"]["l2"]
+                if plain.get("fp32", {}).get("l2"):
+                    l2["plain_980k_fp32"] = plain["fp32"]["l2"]
+            pf64 = plain["fp64"]["value"] if plain and "fp64" in plain else None
+            line = {
+                "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": dist.world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if head == "fp32" else "f64", "data": "synthetic",
+                "config": {"workload": f"batched uneven solves: {info['solves']} isentropic vortices "
+                                       f"(strength U[1,5], angle U[0,2pi), seed 4) on periodic jittered "
+                                       f"Delaunay meshes, {info['min_tris']}-{info['max_tris']} triangles "
+                                       f"(log-uniform 5k-200k), {info['p1_solves']} P1 + {info['p2_solves']} P2, "
+                                       "FP32 state (FP64 geometry, dt), HLLC, SSP-RK3, CFL 0.2, one launch "
+                                       "per RK stage for all solves, CUDA graph, autotuned shape",
+                           **info, "launch_shape": r["shape"],
+                           "parallelism": f"{dist.world} independent replica(s), no collective",
+                           "l2_flush": "inputs larger than L2 (3 state buffers of the packed solves)"},
+                "roofline": r["roofline"], "e2e": r["e2e"],
+                "batched_fp64": ({k: res["fp64"][k] for k in ("value", "ms_per_step", "roofline")}
+                                 if "fp64" in res and head == "fp32" else None),
+                "plain_fp64": pf64,
+                "batched_fp32_over_plain_fp64": (r["value"] / pf64) if pf64 else None,
+                "plain": ({p: {k: v for k, v in plain[p].items() if k != "l2"} for p in plain}
+                          if plain else None),
+                "cpu_baseline": cpu, "clocks": r["clocks"], "gpu_launches": 4 * args.steps,
+                "l2": l2,
+            }
+    else:
+        res, T = run_plain(args, dist, peak, peak_kind, args.steps)
+        head = "fp32" if "fp32" in res else "fp64"
+        r = res[head]
+        cpu = None
+        if dist.rank == 0 and not args.no_cpu:
+            _, cpu = cpu_reference_sample(args.cpu_seconds)
+        if dist.rank == 0:
+            line = {
+                "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": dist.world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if head == "fp32" else "f64", "data": "synthetic",
+                "config": {"workload": "unstructured isentropic vortex: periodic Delaunay of a "
+                                       f"{args.lattice}x{args.lattice} lattice jittered +-0.3h (seed 2), "
+                                       f"{T} triangles, P2, 6-pt volume / 3-pt edge, HLLC, SSP-RK3, CFL 0.2",
+                           "triangles": T, "parallelism": f"{dist.world} independent replica(s)",
+                           "l2_flush": "inputs larger than L2"},
+                "roofline": r["roofline"], "e2e": r["e2e"],
+                "fp64": res.get("fp64") if head == "fp32" else None,
+                "cpu_baseline": cpu, "gpu_launches": 4 * args.steps,
+                "l2": {p: res[p]["l2"] for p in res},
+            }
+    if line is not None:
         print(json.dumps(line), flush=True)
     dist.close()
 

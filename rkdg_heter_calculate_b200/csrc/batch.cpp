@@ -24,6 +24,7 @@ struct rkdg_batch {
     int64_t total = 0;
     int ld = 0, ntiles = 0, max_halo = 4;
     std::vector<int> order, T, off;
+    std::vector<double> far_host;  // [S][4]
     std::vector<int32_t> desc_solve;  // descriptors in solve order [ntiles][8]
     size_t bytes = 0;
     void* U[3] = {nullptr, nullptr, nullptr};
@@ -282,6 +283,7 @@ int rkdg_batch_create(int32_t nsolves, const rkdg_mesh_desc* meshes, const int32
             for (int v = 0; v < 4; ++v) far[4 * s + v] = farfields ? farfields[4 * s + v] : p.farfield[v];
         b->far = (double*)balloc(b, sizeof(double) * far.size());
         h2d(b, b->far, far);
+        b->far_host = far;
         b->staging = (double*)balloc(b, sizeof(double) * 24 * (size_t)maxT);
         b->ctl = (StepCtl*)balloc(b, sizeof(StepCtl) * nsolves);
         for (int s = 0; s < nsolves; ++s) b->h_ctl[s].cfl = p.cfl;
@@ -313,7 +315,7 @@ int rkdg_batch_set_state(rkdg_batch* b, int32_t s, const double* U, int32_t ld) 
                                         sizeof(double) * T, 4 * nb, cudaMemcpyHostToDevice, b->stream));
         char* base = static_cast<char*>(b->U[0]) + (size_t)16 * b->off[s];
         launch_import(T, b->ld, b->staging, T, nullptr, b->perm + b->off[s], base, b->order[s],
-                      b->p.precision, b->stream);
+                      b->p.precision, &b->far_host[4 * s], b->stream);
         b->have_state[s] = true;
         b->wave_valid = false;
         sync(b);
@@ -328,7 +330,7 @@ int rkdg_batch_get_state(rkdg_batch* b, int32_t s, double* U, int32_t ld) {
         const int T = b->T[s], nb = b->order[s] == 1 ? 3 : 6;
         const char* base = static_cast<const char*>(b->U[0]) + (size_t)16 * b->off[s];
         launch_export(T, b->ld, base, nullptr, b->perm + b->off[s], b->staging, T, b->order[s],
-                      b->p.precision, 0, nullptr, b->stream);
+                      b->p.precision, 0, nullptr, &b->far_host[4 * s], b->stream);
         RKDG_CUDA_TRY(cudaMemcpy2DAsync(U, sizeof(double) * ld, b->staging, sizeof(double) * T,
                                         sizeof(double) * T, 4 * nb, cudaMemcpyDeviceToHost, b->stream));
         sync(b);
@@ -354,7 +356,8 @@ int rkdg_batch_advance(rkdg_batch* b, int32_t nsteps, const double* t_final, dou
             if (!b->have_state[s]) throw Error{RKDG_ERR_INVALID, "solve " + std::to_string(s) + " has no state"};
         RKDG_CUDA_TRY(cudaSetDevice(b->device));
         if (!b->wave_valid) {
-            launch_wave(b->tiles, b->ld, b->U[0], b->p.precision, b->jinv, b->p.gamma, b->ctl, b->S, b->stream);
+            launch_wave(b->tiles, b->ld, b->U[0], b->p.precision, b->jinv, b->p.gamma, b->ctl, b->S,
+                        b->far, b->stream);
             b->wave_valid = true;
         }
         pull(b);

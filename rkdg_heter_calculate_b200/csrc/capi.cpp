@@ -146,7 +146,7 @@ void normalise_buffers(rkdg_ctx* c) {
 void ensure_wave(rkdg_ctx* c) {
     if (c->wave_valid) return;
     launch_wave(c->tiles, c->ld, c->d.U[c->cur], c->p.precision, c->d.jinv, c->p.gamma, c->d.ctl, 1,
-                c->stream);
+                c->d.far, c->stream);
     c->wave_valid = true;
 }
 
@@ -222,6 +222,7 @@ void destroy_ctx(rkdg_ctx* c) {
     cudaFree(c->d.staging);
     cudaFree(c->d.partial);
     cudaFree(c->d.ctl);
+    cudaFree(c->d.far);
     cudaFree(c->d.tcode);
     cudaFree(c->d.tdesc);
     cudaFree(c->d.halo);
@@ -352,6 +353,9 @@ int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx*
         if (const char* v = std::getenv("RKDG_STAGE_VARIANT")) c->variant = std::atoi(v) == 0 ? 0 : 1;
         c->d.partial = (double*)dev_alloc(c, sizeof(double) * 4 * (totals_partial_count(T) + 1));
         c->d.ctl = (StepCtl*)dev_alloc(c, sizeof(StepCtl));
+        c->d.far = (double*)dev_alloc(c, sizeof(double) * 4);
+        RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.far, params->farfield, sizeof(double) * 4,
+                                      cudaMemcpyHostToDevice, c->stream));
         c->h_ctl->cfl = params->cfl;
         push_ctl(c);
         sync(c);
@@ -395,7 +399,7 @@ int rkdg_set_state(rkdg_ctx* c, const double* U, int32_t ld, int32_t basis) {
         c->old = 0;
         launch_import(c->T, c->ld, c->d.staging, c->T,
                       basis == RKDG_BASIS_REFERENCE ? c->d.conv_in : nullptr, c->d.perm, c->d.U[0],
-                      c->p.order, c->p.precision, c->stream);
+                      c->p.order, c->p.precision, c->p.farfield, c->stream);
         c->have_state = true;
         c->wave_valid = false;
         ensure_wave(c);
@@ -425,7 +429,7 @@ int rkdg_get_state(rkdg_ctx* c, double* U, int32_t ld, int32_t basis) {
         else if (basis != RKDG_BASIS_NATIVE) throw Error{RKDG_ERR_INVALID, "unknown basis"};
         launch_export(c->T, c->ld, c->d.U[c->cur], basis == RKDG_BASIS_REFERENCE ? c->d.conv_out : nullptr,
                       c->d.perm, c->d.staging, c->T, c->p.order, c->p.precision, 0, c->d.jinv,
-                      c->stream);
+                      c->p.farfield, c->stream);
         RKDG_CUDA_TRY(cudaMemcpy2DAsync(U, sizeof(double) * ld, c->d.staging, sizeof(double) * c->T,
                                         sizeof(double) * c->T, 4 * c->nb, cudaMemcpyDeviceToHost,
                                         c->stream));
@@ -453,7 +457,7 @@ int rkdg_residual(rkdg_ctx* c, double* R, int32_t ld, int32_t basis) {
         launch_residual(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->variant == 1 ? c->ctas : c->block, c->stream);
         launch_export(c->T, c->ld, c->d.U[scratch], basis == RKDG_BASIS_REFERENCE ? c->d.conv_in : nullptr,
                       c->d.perm, c->d.staging, c->T, c->p.order, c->p.precision, 1, c->d.jinv,
-                      c->stream);
+                      c->p.farfield, c->stream);
         RKDG_CUDA_TRY(cudaMemcpy2DAsync(R, sizeof(double) * ld, c->d.staging, sizeof(double) * c->T,
                                         sizeof(double) * c->T, 4 * c->nb, cudaMemcpyDeviceToHost,
                                         c->stream));
@@ -658,7 +662,7 @@ int rkdg_conservation_totals(rkdg_ctx* c, double totals[4]) {
         const int n = totals_partial_count(c->T);
         double* out4 = c->d.partial + (size_t)4 * n;
         launch_totals(c->T, c->ld, c->d.U[c->cur], c->p.order, c->p.precision, c->d.jinv,
-                      c->d.partial, out4, c->stream);
+                      c->d.partial, out4, c->p.farfield, c->stream);
         RKDG_CUDA_TRY(cudaMemcpyAsync(totals, out4, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         sync(c);
     });

@@ -124,6 +124,23 @@ __device__ __forceinline__ void load_mean(const Real* __restrict__ U, int ld, in
     m[0] = u[0][0], m[1] = u[0][1], m[2] = u[0][2], m[3] = u[0][3];
 }
 
+// FP32 states store every cell mean as its deviation from the solve's
+// reference (far-field) state, so that rounding scales with the flow's
+// deviation instead of with the state (the SSP-RK combination coefficients
+// sum to one, so stage updates apply to deviations unchanged); FP64 states
+// store the mean itself.  ref_of returns the offset to add to a stored mean.
+template <typename Real>
+__device__ __forceinline__ Real ref_of(const double* ref, int v) {
+    if constexpr (sizeof(Real) == 4) return (Real)ref[v];
+    else return Real(0);
+}
+template <typename Real>
+__host__ __device__ constexpr bool stores_deviation() { return sizeof(Real) == 4; }
+
+struct Ref4 {
+    double v[4];
+};
+
 template <typename Real, int NB>
 __device__ __forceinline__ void store_state(Real* __restrict__ U, int ld, int e,
                                             const Real u[NB][4]) {
@@ -308,6 +325,12 @@ __global__ void __launch_bounds__(128) stage_kernel(const StageArgs a) {
     const Real* __restrict__ U = static_cast<const Real*>(a.U);
     Real u[NB][4];
     load_state<Real, NB>(U, a.ld, ee, u);
+    Real dev0[4];  // stored means (deviations in FP32) for the stage update
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        dev0[v] = u[0][v];
+        u[0][v] += ref_of<Real>(a.far, v);
+    }
     const double2* jinv2 = reinterpret_cast<const double2*>(a.jinv);
     const double2 r0 = __ldg(jinv2 + ee), r1 = __ldg(jinv2 + a.ld + ee);
     const int4 cn = __ldg(a.conn + ee);
@@ -375,6 +398,8 @@ __global__ void __launch_bounds__(128) stage_kernel(const StageArgs a) {
         const bool interior = ne >= 0;
         if (interior) {
             load_state<Real, NB>(U, a.ld, ne, un);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) un[0][v] += ref_of<Real>(a.far, v);
             mR[0] = un[0][0], mR[1] = un[0][1], mR[2] = un[0][2], mR[3] = un[0][3];
         } else {
 #pragma unroll
@@ -446,10 +471,12 @@ __global__ void __launch_bounds__(128) stage_kernel(const StageArgs a) {
         return;
     }
 
-    // ---- stage update: Unew = a U0 + b (U + dt L(U))
+    // ---- stage update: Unew = a U0 + b (U + dt L(U)), on the stored values
     const double dtd = a.ctl->dt;
     const Real dt = (Real)dtd, ca = (Real)a.a, cb = (Real)a.b;
     Real u0m[4] = {Real(0), Real(0), Real(0), Real(0)};
+#pragma unroll
+    for (int v = 0; v < 4; ++v) u[0][v] = dev0[v];
     if (a.U0 != nullptr) {
         Real u0[NB][4];
         load_state<Real, NB>(static_cast<const Real*>(a.U0), a.ld, ee, u0);
@@ -472,8 +499,10 @@ __global__ void __launch_bounds__(128) stage_kernel(const StageArgs a) {
         double wv = 0.0, m0 = 0.0, m1 = 0.0;
         if (active) {
             bool bad;
-            wv = wave_measure((double)R[0][0], (double)R[0][1], (double)R[0][2], (double)R[0][3],
-                              a.gamma, r0, r1, bad);
+            wv = wave_measure((double)R[0][0] + (double)ref_of<Real>(a.far, 0),
+                              (double)R[0][1] + (double)ref_of<Real>(a.far, 1),
+                              (double)R[0][2] + (double)ref_of<Real>(a.far, 2),
+                              (double)R[0][3] + (double)ref_of<Real>(a.far, 3), a.gamma, r0, r1, bad);
             if (bad) atomicOr(&a.ctl->error, 1);
             m0 = fabs((double)R[0][0] - (double)u0m[0]);
             m1 = fabs((double)R[0][3] - (double)u0m[3]);
@@ -490,18 +519,21 @@ template <typename Real>
 __global__ void __launch_bounds__(kTile) wave_kernel(const TileArgs ta, int ld,
                                                      const Real* __restrict__ U,
                                                      const double* __restrict__ jinv, double gamma,
-                                                     StepCtl* ctl) {
+                                                     StepCtl* ctl, const double* __restrict__ refs) {
     const int4 d0 = __ldg(ta.desc + 2 * blockIdx.x);
     const int e = d0.x + threadIdx.x;
     StepCtl* c = ctl + d0.z;
+    const double* ref = refs + 4 * d0.z;
     double w = 0.0;
     if ((int)threadIdx.x < d0.y) {
         Real m[4];
         load_mean<Real, 1>(U, ld, e, m);
         const double2* j2 = reinterpret_cast<const double2*>(jinv);
         bool bad;
-        w = wave_measure((double)m[0], (double)m[1], (double)m[2], (double)m[3], gamma, j2[e],
-                         j2[ld + e], bad);
+        w = wave_measure((double)m[0] + (double)ref_of<Real>(ref, 0),
+                         (double)m[1] + (double)ref_of<Real>(ref, 1),
+                         (double)m[2] + (double)ref_of<Real>(ref, 2),
+                         (double)m[3] + (double)ref_of<Real>(ref, 3), gamma, j2[e], j2[ld + e], bad);
         if (bad) atomicOr(&c->error, 1);
     }
     block_max3_atomic(w, 0.0, 0.0, &c->wave_bits, nullptr, nullptr);
@@ -565,7 +597,13 @@ __global__ void __launch_bounds__(128) limiter_kernel(int T, int ld, Real* __res
     const int4 cn = __ldg(conn + e);
     const Real gamma = (Real)gammad;
     const Real far[4] = {(Real)f0, (Real)f1, (Real)f2, (Real)f3};
-    Real mean[4] = {u[0][0], u[0][1], u[0][2], u[0][3]};
+    const double fref[4] = {f0, f1, f2, f3};
+    Real mean[4], dev0[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        dev0[v] = u[0][v];
+        mean[v] = u[0][v] + ref_of<Real>(fref, v);
+    }
     Real nbm[3][4], tilde[3][4];
     const double* L = lim + (size_t)18 * e;
 #pragma unroll
@@ -573,6 +611,8 @@ __global__ void __launch_bounds__(128) limiter_kernel(int T, int ld, Real* __res
         int ne = k == 0 ? cn.x : (k == 1 ? cn.y : cn.z);
         if (ne >= 0) {
             load_mean<Real, 1>(U, ld, ne, nbm[k]);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) nbm[k][v] += ref_of<Real>(fref, v);
         } else {
             // ghost mean across a boundary edge, mirrored about the unit
             // normal of edge k (N_k / area = 2(r0+r1), -2 r0, -2 r1)
@@ -658,7 +698,7 @@ __global__ void __launch_bounds__(128) limiter_kernel(int T, int ld, Real* __res
     Real out[NB][4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        out[0][v] = mean[v];
+        out[0][v] = dev0[v];
         out[1][v] = tb.minv[0][0] * delta[0][v] + tb.minv[0][1] * delta[1][v] + tb.minv[0][2] * delta[2][v];
         out[2][v] = tb.minv[1][0] * delta[0][v] + tb.minv[1][1] * delta[1][v] + tb.minv[1][2] * delta[2][v];
 #pragma unroll
@@ -673,7 +713,7 @@ __global__ void __launch_bounds__(128) limiter_kernel(int T, int ld, Real* __res
 template <typename Real, int NB>
 __global__ void import_kernel(int T, int ld, const double* __restrict__ st, int ldh,
                               const double* __restrict__ conv, const int32_t* __restrict__ perm,
-                              Real* __restrict__ U) {
+                              Real* __restrict__ U, Ref4 ref) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= T) return;
     const int c = perm ? perm[e] : e;
@@ -700,6 +740,20 @@ __global__ void import_kernel(int T, int ld, const double* __restrict__ st, int 
 #pragma unroll
             for (int v = 0; v < 4; ++v) b[i][v] = (Real)a[i][v];
     }
+    if (stores_deviation<Real>()) {  // mean row = basis 0 (basis-invariant)
+        const double* Cm = conv ? conv + (size_t)36 * e : nullptr;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            double m = 0;
+            if (Cm) {
+#pragma unroll
+                for (int i = 0; i < NB; ++i) m += a[i][v] * Cm[6 * i];
+            } else {
+                m = a[0][v];
+            }
+            b[0][v] = (Real)(m - ref.v[v]);
+        }
+    }
     store_state<Real, NB>(U, ld, e, b);
 }
 
@@ -707,12 +761,20 @@ template <typename Real, int NB>
 __global__ void export_kernel(int T, int ld, const Real* __restrict__ U,
                               const double* __restrict__ conv, const int32_t* __restrict__ perm,
                               double* __restrict__ st, int ldh, int residual_scale,
-                              const double* __restrict__ jinv) {
+                              const double* __restrict__ jinv, Ref4 ref) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= T) return;
     const int c = perm ? perm[e] : e;
-    Real b[NB][4];
-    load_state<Real, NB>(U, ld, e, b);
+    Real bl[NB][4];
+    load_state<Real, NB>(U, ld, e, bl);
+    double b[NB][4];
+#pragma unroll
+    for (int i = 0; i < NB; ++i)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) b[i][v] = (double)bl[i][v];
+    if (stores_deviation<Real>() && !residual_scale)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) b[0][v] += ref.v[v];
     double scale = 1.0;
     if (residual_scale) {  // area = 1 / (2 det J^-1)
         const double2* j2 = reinterpret_cast<const double2*>(jinv);
@@ -728,9 +790,9 @@ __global__ void export_kernel(int T, int ld, const Real* __restrict__ U,
                 const double* M = conv + (size_t)36 * e + 6 * i;
                 s = 0;
 #pragma unroll
-                for (int j = 0; j < NB; ++j) s += M[j] * (double)b[j][v];
+                for (int j = 0; j < NB; ++j) s += M[j] * b[j][v];
             } else {
-                s = (double)b[i][v];
+                s = b[i][v];
             }
             st[((size_t)v * NB + i) * ldh + c] = scale * s;
         }
@@ -744,7 +806,8 @@ template <typename Real>
 __global__ void __launch_bounds__(kTotBlock) totals_partial_kernel(int T, int ld,
                                                                    const Real* __restrict__ U,
                                                                    const double* __restrict__ jinv,
-                                                                   double* __restrict__ partial) {
+                                                                   double* __restrict__ partial,
+                                                                   Ref4 ref) {
     __shared__ double s[4][kTotBlock];
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     double v4[4] = {0, 0, 0, 0};
@@ -754,7 +817,8 @@ __global__ void __launch_bounds__(kTotBlock) totals_partial_kernel(int T, int ld
         const double2* j2 = reinterpret_cast<const double2*>(jinv);
         double2 r0 = j2[e], r1 = j2[ld + e];
         double area = 0.5 / (r0.x * r1.y - r0.y * r1.x);
-        for (int v = 0; v < 4; ++v) v4[v] = area * (double)m[v];
+        for (int v = 0; v < 4; ++v)
+            v4[v] = area * ((double)m[v] + (stores_deviation<Real>() ? ref.v[v] : 0.0));
     }
     for (int v = 0; v < 4; ++v) s[v][threadIdx.x] = v4[v];
     __syncthreads();
@@ -870,13 +934,13 @@ void launch_residual(const StageArgs& a, const TileArgs& t, int variant, int ord
 }
 
 void launch_wave(const TileArgs& t, int ld, const void* U, int prec, const double* jinv,
-                 double gamma, StepCtl* ctl, int nsolves, cudaStream_t stream) {
+                 double gamma, StepCtl* ctl, int nsolves, const double* refs, cudaStream_t stream) {
     reset_wave_kernel<<<(nsolves + 127) / 128, 128, 0, stream>>>(ctl, nsolves);
     if (t.ntiles > 0) {
         if (prec == RKDG_FP32)
-            wave_kernel<float><<<t.ntiles, kTile, 0, stream>>>(t, ld, static_cast<const float*>(U), jinv, gamma, ctl);
+            wave_kernel<float><<<t.ntiles, kTile, 0, stream>>>(t, ld, static_cast<const float*>(U), jinv, gamma, ctl, refs);
         else
-            wave_kernel<double><<<t.ntiles, kTile, 0, stream>>>(t, ld, static_cast<const double*>(U), jinv, gamma, ctl);
+            wave_kernel<double><<<t.ntiles, kTile, 0, stream>>>(t, ld, static_cast<const double*>(U), jinv, gamma, ctl, refs);
     }
     RKDG_CUDA_TRY(cudaGetLastError());
 }
@@ -911,40 +975,44 @@ void launch_limiter(int T, int ld, void* U, const int4* conn, const double* lim,
 }
 
 void launch_import(int T, int ld, const double* staging, int ldh, const double* conv,
-                   const int32_t* perm, void* U, int order, int prec, cudaStream_t stream) {
+                   const int32_t* perm, void* U, int order, int prec, const double* ref,
+                   cudaStream_t stream) {
+    Ref4 r{{ref[0], ref[1], ref[2], ref[3]}};
     const int grid = (T + 127) / 128;
     if (prec == RKDG_FP32) {
-        if (order == 1) import_kernel<float, 3><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<float*>(U));
-        else import_kernel<float, 6><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<float*>(U));
+        if (order == 1) import_kernel<float, 3><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<float*>(U), r);
+        else import_kernel<float, 6><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<float*>(U), r);
     } else {
-        if (order == 1) import_kernel<double, 3><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<double*>(U));
-        else import_kernel<double, 6><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<double*>(U));
+        if (order == 1) import_kernel<double, 3><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<double*>(U), r);
+        else import_kernel<double, 6><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<double*>(U), r);
     }
     RKDG_CUDA_TRY(cudaGetLastError());
 }
 
 void launch_export(int T, int ld, const void* U, const double* conv, const int32_t* perm,
                    double* staging, int ldh, int order, int prec, int residual_scale,
-                   const double* jinv, cudaStream_t stream) {
+                   const double* jinv, const double* ref, cudaStream_t stream) {
+    Ref4 r{{ref[0], ref[1], ref[2], ref[3]}};
     const int grid = (T + 127) / 128;
     if (prec == RKDG_FP32) {
-        if (order == 1) export_kernel<float, 3><<<grid, 128, 0, stream>>>(T, ld, static_cast<const float*>(U), conv, perm, staging, ldh, residual_scale, jinv);
-        else export_kernel<float, 6><<<grid, 128, 0, stream>>>(T, ld, static_cast<const float*>(U), conv, perm, staging, ldh, residual_scale, jinv);
+        if (order == 1) export_kernel<float, 3><<<grid, 128, 0, stream>>>(T, ld, static_cast<const float*>(U), conv, perm, staging, ldh, residual_scale, jinv, r);
+        else export_kernel<float, 6><<<grid, 128, 0, stream>>>(T, ld, static_cast<const float*>(U), conv, perm, staging, ldh, residual_scale, jinv, r);
     } else {
-        if (order == 1) export_kernel<double, 3><<<grid, 128, 0, stream>>>(T, ld, static_cast<const double*>(U), conv, perm, staging, ldh, residual_scale, jinv);
-        else export_kernel<double, 6><<<grid, 128, 0, stream>>>(T, ld, static_cast<const double*>(U), conv, perm, staging, ldh, residual_scale, jinv);
+        if (order == 1) export_kernel<double, 3><<<grid, 128, 0, stream>>>(T, ld, static_cast<const double*>(U), conv, perm, staging, ldh, residual_scale, jinv, r);
+        else export_kernel<double, 6><<<grid, 128, 0, stream>>>(T, ld, static_cast<const double*>(U), conv, perm, staging, ldh, residual_scale, jinv, r);
     }
     RKDG_CUDA_TRY(cudaGetLastError());
 }
 
 void launch_totals(int T, int ld, const void* U, int order, int prec, const double* jinv,
-                   double* partial, double* out4, cudaStream_t stream) {
+                   double* partial, double* out4, const double* ref, cudaStream_t stream) {
+    Ref4 r{{ref[0], ref[1], ref[2], ref[3]}};
     (void)order;
     const int n = totals_partial_count(T);
     if (prec == RKDG_FP32)
-        totals_partial_kernel<float><<<n, kTotBlock, 0, stream>>>(T, ld, static_cast<const float*>(U), jinv, partial);
+        totals_partial_kernel<float><<<n, kTotBlock, 0, stream>>>(T, ld, static_cast<const float*>(U), jinv, partial, r);
     else
-        totals_partial_kernel<double><<<n, kTotBlock, 0, stream>>>(T, ld, static_cast<const double*>(U), jinv, partial);
+        totals_partial_kernel<double><<<n, kTotBlock, 0, stream>>>(T, ld, static_cast<const double*>(U), jinv, partial, r);
     totals_final_kernel<<<1, kTotBlock, 0, stream>>>(n, partial, out4);
     RKDG_CUDA_TRY(cudaGetLastError());
 }

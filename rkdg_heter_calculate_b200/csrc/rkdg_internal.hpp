@@ -144,6 +144,7 @@ struct DeviceArrays {
     double* staging = nullptr;  // [4][6][T] dense FP64 host-layout staging
     double* partial = nullptr;  // block partial sums for deterministic totals
     StepCtl* ctl = nullptr;
+    double* far = nullptr;      // [4] far-field / reference state (device copy)
     // tile tables
     int4* tcode = nullptr;
     int4* tdesc = nullptr;
@@ -188,20 +189,23 @@ void launch_stage(const StageArgs& a, const TileArgs& t, int variant, int order,
 void launch_residual(const StageArgs& a, const TileArgs& t, int variant, int order, int nq,
                      int ng, int flux, int prec, int block, cudaStream_t stream);
 // CFL measure per solve, one CTA per tile (resets the solves' wave slots first)
+// FP32 states store cell means as deviations from a per-solve reference
+// state (the far field); `refs` ([solves][4], device) / `ref` (4, host) give it.
 void launch_wave(const TileArgs& t, int ld, const void* U, int prec, const double* jinv,
-                 double gamma, StepCtl* ctl, int nsolves, cudaStream_t stream);
+                 double gamma, StepCtl* ctl, int nsolves, const double* refs, cudaStream_t stream);
 void launch_step_begin(StepCtl* ctl, int nsolves, cudaStream_t stream);
 int tiled_max_ctas_per_sm(int prec, int order);
 void launch_limiter(int T, int ld, void* U, const int4* conn, const double* lim,
                     const double* jinv, int order, int nq, int ng, int prec, double gamma,
                     const double* far, double tvb_m, cudaStream_t stream);
 void launch_import(int T, int ld, const double* staging, int ldh, const double* conv,
-                   const int32_t* perm, void* U, int order, int prec, cudaStream_t stream);
+                   const int32_t* perm, void* U, int order, int prec, const double* ref,
+                   cudaStream_t stream);
 void launch_export(int T, int ld, const void* U, const double* conv, const int32_t* perm,
                    double* staging, int ldh, int order, int prec, int residual_scale,
-                   const double* jinv, cudaStream_t stream);
+                   const double* jinv, const double* ref, cudaStream_t stream);
 void launch_totals(int T, int ld, const void* U, int order, int prec, const double* jinv,
-                   double* partial, double* out4, cudaStream_t stream);
+                   double* partial, double* out4, const double* ref, cudaStream_t stream);
 int totals_partial_count(int T);
 
 }  // namespace rkdg

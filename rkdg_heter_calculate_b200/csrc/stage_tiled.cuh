@@ -84,7 +84,10 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
         Real u[NB][4];
         load_state<Real, NB>(U, a.ld, ee, u);
 #pragma unroll
-        for (int v = 0; v < 4; ++v) s_mean[v * BT + tid] = u[0][v];
+        for (int v = 0; v < 4; ++v) {
+            u[0][v] += ref_of<Real>(fs, v);  // stored deviation -> state (FP32)
+            s_mean[v * BT + tid] = u[0][v];
+        }
 #pragma unroll
         for (int i = 0; i < NB; ++i)
 #pragma unroll
@@ -133,7 +136,10 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
             Real un[NB][4];
             load_state<Real, NB>(U, a.ld, hh.x, un);
 #pragma unroll
-            for (int v = 0; v < 4; ++v) s_hmean[v * HM + h] = un[0][v];
+            for (int v = 0; v < 4; ++v) {
+                un[0][v] += ref_of<Real>(fs, v);
+                s_hmean[v * HM + h] = un[0][v];
+            }
 #pragma unroll
             for (int g = 0; g < NG; ++g)
 #pragma unroll
@@ -273,7 +279,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     Real u0m[4] = {Real(0), Real(0), Real(0), Real(0)};
     {
         Real u[NB][4];
-        load_state<Real, NB>(U, a.ld, ee, u);  // L1/L2 hit: read in phase A
+        load_state<Real, NB>(U, a.ld, ee, u);  // stored values (L1/L2 hit: read in phase A)
         if (a.U0 != nullptr) {
             Real u0[NB][4];
             load_state<Real, NB>(static_cast<const Real*>(a.U0), a.ld, ee, u0);
@@ -295,8 +301,10 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
         double wv = 0.0, m0 = 0.0, m1 = 0.0;
         if (active) {
             bool bad;
-            wv = wave_measure((double)R[0][0], (double)R[0][1], (double)R[0][2], (double)R[0][3],
-                              a.gamma, r0, r1, bad);
+            wv = wave_measure((double)R[0][0] + (double)ref_of<Real>(fs, 0),
+                              (double)R[0][1] + (double)ref_of<Real>(fs, 1),
+                              (double)R[0][2] + (double)ref_of<Real>(fs, 2),
+                              (double)R[0][3] + (double)ref_of<Real>(fs, 3), a.gamma, r0, r1, bad);
             if (bad) atomicOr(&ctl->error, 1);
             m0 = fabs((double)R[0][0] - (double)u0m[0]);
             m1 = fabs((double)R[0][3] - (double)u0m[3]);
