@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "vortex"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "vortex", "serving"])
     ap.add_argument("--nsolves", type=int, default=64)
     ap.add_argument("--lattice", type=int, default=700)
     ap.add_argument("--plain-steps", type=int, default=50)
@@ -67,6 +67,10 @@ def parse():
     ap.add_argument("--precision", default="both", choices=["both", "fp32", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI run")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving sweep")
+    ap.add_argument("--serve-requests", type=int, default=16, help="requests per arrival-rate point")
+    ap.add_argument("--serve-loads", default="0.5,0.9",
+                    help="arrival rates as fractions of the measured saturated request rate")
     return ap.parse_args()
 
 
@@ -398,6 +402,136 @@ def run_plain(args, dist, peak, peak_kind, K):
     return out, T
 
 
+# ------------------------------------------------------------ serving (C5) --
+SERVE_LEVELS = 8   # mesh sizes per request kind, log-spaced over [2k, 500k] triangles
+
+
+def serving_catalogue(seed=5):
+    """Meshes and initial states the serving requests draw from: per kind
+    (isentropic vortex on a periodic Delaunay mesh, Mach-3 wind-tunnel step)
+    SERVE_LEVELS meshes with triangle counts log-spaced over [2k, 500k]."""
+    from rkdg_heter_calculate_b200 import meshgen, vortex
+
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(np.linspace(math.log(2e3), math.log(5e5), SERVE_LEVELS))
+    cat = {"vortex": [], "step": []}
+    for k, T in enumerate(sizes):
+        lat = max(8, int(round(math.sqrt(T / 2.0))))
+        m = meshgen.periodic_delaunay(lat, L=10.0, jitter=0.3, seed=int(rng.integers(0, 2 ** 31)))
+        b, th = float(rng.uniform(1.0, 5.0)), float(rng.uniform(0.0, 2 * math.pi))
+        ui, vi = math.sqrt(2) * math.cos(th), math.sqrt(2) * math.sin(th)
+        U2 = vortex.project_native(m, lambda X, Y: vortex.exact(X, Y, 0.0, b, GAMMA, ui, vi), 6, n=4)
+        # the native basis is orthonormal and hierarchical: the P1 projection
+        # is the first three coefficients of the P2 one
+        cat["vortex"].append((m, U2, np.ascontiguousarray(U2[:, :3]), conservative(1.0, ui, vi, 1.0)))
+        k = max(10, 5 * int(round(math.sqrt(T / 5.04) / 5)))  # 1/h: the step corner on the lattice
+        st = meshgen.forward_step(h=1.0 / k, seed=int(rng.integers(0, 2 ** 31)))
+        far = conservative(1.4, 3.0, 0.0, 1.0)
+        U1 = np.zeros((4, 3, st.ntri))
+        U1[:, 0, :] = np.array(far)[:, None]
+        cat["step"].append((st, U1, far))
+    return cat, sizes
+
+
+def serving_requests(cat, sizes, n, rng):
+    """n requests: kind 50/50, triangle count log-uniform in [2k, 500k]
+    (snapped to the nearest catalogue size), vortex P1/P2 50/50 without
+    limiter, step P1 with the TVB limiter, final time U[0.1, 1.0]."""
+    out = []
+    lo, hi = math.log(sizes[0]), math.log(sizes[-1])
+    for _ in range(n):
+        kind = "vortex" if rng.random() < 0.5 else "step"
+        lvl = int(round((rng.uniform(lo, hi) - lo) / (hi - lo) * (SERVE_LEVELS - 1)))
+        tf = float(rng.uniform(0.1, 1.0))
+        if kind == "vortex":
+            m, U2, U1, far = cat["vortex"][lvl]
+            order = 2 if rng.random() < 0.5 else 1
+            out.append((m, order, U2 if order == 2 else U1, tf, far, False))
+        else:
+            m, U1, far = cat["step"][lvl]
+            out.append((m, 1, U1, tf, far, True))
+    return out
+
+
+def serve_point(srv, reqs, rate):
+    """Submits reqs with Poisson arrivals at `rate` requests/s (inf: all at
+    once) from a pool of submitter threads; returns per-request latencies
+    (completion - arrival, seconds), DOF-stage/s over the point and counts."""
+    import concurrent.futures as cf
+
+    from rkdg_heter_calculate_b200 import capi
+    from rkdg_heter_calculate_b200.serve import clock
+
+    rng = np.random.default_rng(6)
+    gaps = rng.exponential(1.0 / rate, len(reqs)) if math.isfinite(rate) else np.zeros(len(reqs))
+    gaps[0] = 0.0
+    arrive = np.cumsum(gaps)
+    st0 = srv.stats()
+    pool = cf.ThreadPoolExecutor(8)
+    t0 = clock()
+    futs = []
+    for (m, order, U, tf, far, lim), at in zip(reqs, arrive):
+        d = t0 + at - clock()
+        if d > 0:
+            time.sleep(d)
+        futs.append(pool.submit(srv.submit, m, order, U, tf, far, lim))
+    lat, failed, t_end = [], 0, t0
+    for f, at in zip(futs, arrive):
+        try:
+            r = srv.wait(f.result())
+            lat.append(r.completed - (t0 + at))
+            t_end = max(t_end, r.completed)
+        except capi.RkdgError:
+            failed += 1
+    pool.shutdown()
+    st1 = srv.stats()
+    wall = t_end - t0
+    return {"latency": np.array(lat), "dof_per_s": (st1["dof_stage_updates"] - st0["dof_stage_updates"]) / wall,
+            "wall_s": wall, "failed": failed, "busy_frac": (st1["busy_seconds"] - st0["busy_seconds"]) / wall,
+            "peak_in_flight": st1["peak_in_flight"]}
+
+
+def run_serving(args, dist):
+    from rkdg_heter_calculate_b200.serve import Server
+
+    cat, sizes = serving_catalogue()
+    rng = np.random.default_rng(5 + dist.rank)
+    n = args.serve_requests
+    with Server(8 << 30, max_slots=64, precision="fp32", flux="llf", rk=3, gamma=GAMMA, cfl=0.2,
+                tvb_m=50.0) as srv:
+        # warm-up: one small request of each kind
+        for r in (serving_requests(cat, sizes, 4, np.random.default_rng(99))):
+            m, order, U, tf, far, lim = r
+            try:
+                srv.wait(srv.submit(m, order, U, min(tf, 0.05), far, lim))
+            except Exception:
+                pass
+        # one request set, offered all at once and then at Poisson rates that
+        # are fractions of the saturated completion rate
+        reqs = serving_requests(cat, sizes, n, rng)
+        sat = serve_point(srv, reqs, math.inf)
+        cap_rate = n / sat["wall_s"]
+        points = [("saturated", math.inf, sat)]
+        for f in [float(x) for x in args.serve_loads.split(",") if x]:
+            points.append((f, f * cap_rate, serve_point(srv, reqs, f * cap_rate)))
+    out = []
+    for f, rate, p in points:
+        lat = p["latency"]
+        out.append({"load": f, "lambda_req_per_s": None if not math.isfinite(rate) else round(rate, 3),
+                    "p50_s": dist.max(float(np.percentile(lat, 50))) if len(lat) else None,
+                    "p99_s": dist.max(float(np.percentile(lat, 99))) if len(lat) else None,
+                    "dof_stage_per_s": dist.sum(p["dof_per_s"]), "wall_s": round(p["wall_s"], 3),
+                    "completed": int(len(lat)), "failed": p["failed"],
+                    "busy_frac": round(p["busy_frac"], 3), "peak_in_flight": p["peak_in_flight"]})
+    return {"workload": f"Poisson arrivals (default_rng(5)) of isentropic-vortex and Mach-3-step requests "
+                        f"50/50, triangles log-uniform in [2k, 500k] snapped to {SERVE_LEVELS} mesh sizes "
+                        "per kind, vortex P1/P2 50/50, step P1 with TVB (M=50), final time U[0.1, 1.0]; "
+                        "FP32, LLF, SSP-RK3, CFL 0.2; 8 GiB pool, 64 slots",
+            "requests_per_point": n, "saturated_req_per_s": round(cap_rate, 3),
+            "latency": "completion - arrival, host preprocessing and result read-back included",
+            "points": out}
+
+
 # --------------------------------------------------------- CPU baselines --
 def cpu_reference_sample(seconds: float, threads: int | None = None):
     """The reference's own code (oracle/_ref) when built, else the oracle
@@ -484,6 +618,7 @@ def main():
             plain, T2 = run_plain(args, dist, peak, peak_kind, args.plain_steps)
         head = "fp32" if "fp32" in res else "fp64"
         r = res[head]
+        serving = None if args.no_serving else run_serving(args, dist)
         cpu = None
         if dist.rank == 0 and not args.no_cpu:
             _, cpu = cpu_reference_sample(args.cpu_seconds)
@@ -523,8 +658,12 @@ def main():
                 "plain": ({p: {k: v for k, v in plain[p].items() if k != "l2"} for p in plain}
                           if plain else None),
                 "cpu_baseline": cpu, "clocks": r["clocks"], "gpu_launches": 4 * args.steps,
-                "l2": l2,
+                "l2": l2, "serving": serving,
             }
+    elif args.workload == "serving":
+        serving = run_serving(args, dist)
+        if dist.rank == 0:
+            print(json.dumps({"workload": "serving", "n_gpus": dist.world, "serving": serving}), flush=True)
     else:
         res, T = run_plain(args, dist, peak, peak_kind, args.steps)
         head = "fp32" if "fp32" in res else "fp64"

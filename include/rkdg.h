@@ -243,6 +243,47 @@ int rkdg_batch_time_stage(rkdg_batch* b, int32_t s, int32_t reps, double* ms_per
 int rkdg_batch_get_sizes(const rkdg_batch* b, int64_t* elements, int32_t* ntiles, size_t* device_bytes);
 int rkdg_batch_get_stream(const rkdg_batch* b, void** stream);
 
+/* ---- serving: continuous batching of solve requests --------------------- */
+/* A request loop on its own host thread.  It admits solve requests into a
+ * device pool sized by an HBM budget (elements, halo and flux-task entries,
+ * solve slots), keeps every admitted solve's state resident in HBM, and
+ * advances all in-flight solves together: one launch per RK stage over the
+ * packed tiles (CUDA graph; the set of tiles changes without recapture).
+ * Requests that arrive while others run are admitted as soon as a slot and
+ * memory are free; each solve runs to its own final time and is retired
+ * (state copied back, memory freed) by the loop.  A solve's arithmetic is
+ * independent of what else is in flight: its result equals the same solve
+ * run alone.  No reference counterpart (the reference runs one solve per
+ * process). */
+typedef struct rkdg_server rkdg_server;
+
+/* params: precision, flux, rk, gamma, cfl, tvb_m and nq (P2 rule, 6) shared
+ * by all requests; hbm_budget_bytes bounds the pool; max_slots bounds the
+ * number of solves in flight. */
+int rkdg_server_create(const rkdg_params* params, size_t hbm_budget_bytes, int32_t max_slots,
+                       rkdg_server** out);
+/* Stops the loop (in-flight solves are abandoned) and frees everything. */
+int rkdg_server_destroy(rkdg_server* s);
+/* Queues a solve: mesh, order (1 or 2), native-basis initial state
+ * [4][nbasis][ntri] (caller triangle order), final time, far-field /
+ * inflow state, limiter flag.  Host preprocessing (connectivity, geometry,
+ * tiles) runs in the calling thread.  Returns the request id. */
+int rkdg_server_submit(rkdg_server* s, const rkdg_mesh_desc* mesh, int32_t order, const double* U0,
+                       double t_final, const double* farfield, int32_t limiter, int64_t* id);
+/* Waits up to timeout_s (< 0: forever) for request id; status 0 queued,
+ * 1 running, 2 done, 3 failed.  On done, U (may be NULL) receives the final
+ * state [4][nbasis][ntri], and times[3] (may be NULL) the submit, admit and
+ * completion times in seconds on the loop's steady clock; steps the number
+ * of time steps taken.  A fetched request is released. */
+int rkdg_server_wait(rkdg_server* s, int64_t id, double timeout_s, int32_t* status, double* U,
+                     double* times, int32_t* steps);
+/* Aggregate counters: DOF-stage updates done, seconds with work in flight,
+ * requests completed, peak solves in flight, pool capacity in elements. */
+int rkdg_server_stats(rkdg_server* s, double* dof_stage_updates, double* busy_seconds,
+                      int64_t* completed, int32_t* peak_in_flight, int64_t* capacity_elements);
+/* Seconds on the loop's steady clock (the clock of rkdg_server_wait's times). */
+double rkdg_server_clock(void);
+
 /* ---- mesh files -------------------------------------------------------- */
 /* Reads the reference's mesh set: the mesh configuration file
  * (trianglenum, verticenum, edgenum and the five file names) and the five

@@ -15,6 +15,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "librkdg.so")
 
 RKDG_OK = 0
+RKDG_ERR_INVALID, RKDG_ERR_CUDA, RKDG_ERR_NOMEM, RKDG_ERR_STATE = 1, 2, 3, 4
+RKDG_ERR_NODEVICE, RKDG_ERR_IO, RKDG_ERR_BUSY = 5, 6, 7
 ERRORS = {1: "INVALID", 2: "CUDA", 3: "NOMEM", 4: "STATE", 5: "NODEVICE", 6: "IO", 7: "BUSY"}
 FLUX_LLF, FLUX_HLLC = 0, 1
 LIMITER_NONE, LIMITER_TVB = 0, 1
@@ -97,6 +99,15 @@ def lib():
             "rkdg_batch_get_sizes": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32),
                                                C.POINTER(C.c_size_t)]),
             "rkdg_batch_get_stream": (C.c_int, [vp, C.POINTER(vp)]),
+            "rkdg_server_create": (C.c_int, [C.POINTER(Params), C.c_size_t, C.c_int32, C.POINTER(vp)]),
+            "rkdg_server_destroy": (C.c_int, [vp]),
+            "rkdg_server_submit": (C.c_int, [vp, C.POINTER(MeshDesc), C.c_int32, _dp, C.c_double, _dp,
+                                             C.c_int32, C.POINTER(C.c_int64)]),
+            "rkdg_server_wait": (C.c_int, [vp, C.c_int64, C.c_double, C.POINTER(C.c_int32), _dp, _dp,
+                                           C.POINTER(C.c_int32)]),
+            "rkdg_server_stats": (C.c_int, [vp, _dp, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                                            C.POINTER(C.c_int64)]),
+            "rkdg_server_clock": (C.c_double, []),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

@@ -183,9 +183,9 @@ void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out) {
     a.last_stage = s == c->p.rk - 1;
     launch_stage(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->variant == 1 ? c->ctas : c->block, c->stream);
     if (c->p.limiter == RKDG_LIMITER_TVB)
-        launch_limiter(c->T, c->ld, c->d.U[out], c->d.conn, c->d.lim, c->d.jinv, c->p.order,
-                       c->p.nq, c->p.ng, c->p.precision, c->p.gamma, c->p.farfield, c->p.tvb_m,
-                       c->stream);
+        launch_tiled_limiter(c->tiles, 0, c->ld, c->d.U[out], c->d.conn, c->d.lim, c->d.jinv, nullptr,
+                             c->d.far, c->p.precision, c->p.nq, c->p.gamma, c->p.tvb_m, c->d.ctl,
+                             c->stream);
 }
 
 // one full step on the stream with the state in buffer 0 (graph-capturable)
@@ -519,9 +519,9 @@ int rkdg_limit(rkdg_ctx* c) {
         require_state(c);
         if (c->p.limiter != RKDG_LIMITER_TVB) throw Error{RKDG_ERR_INVALID, "context created without limiter"};
         RKDG_CUDA_TRY(cudaSetDevice(c->device));
-        launch_limiter(c->T, c->ld, c->d.U[c->cur], c->d.conn, c->d.lim, c->d.jinv, c->p.order,
-                       c->p.nq, c->p.ng, c->p.precision, c->p.gamma, c->p.farfield, c->p.tvb_m,
-                       c->stream);
+        launch_tiled_limiter(c->tiles, 0, c->ld, c->d.U[c->cur], c->d.conn, c->d.lim, c->d.jinv,
+                             nullptr, c->d.far, c->p.precision, c->p.nq, c->p.gamma, c->p.tvb_m,
+                             nullptr, c->stream);
         sync(c);
     });
 }

@@ -20,6 +20,7 @@
 // from J^-1: the scaled normals N_k/area are 2(r0+r1), -2 r0, -2 r1.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "rkdg_internal.hpp"
@@ -520,6 +521,8 @@ __global__ void __launch_bounds__(kTile) wave_kernel(const TileArgs ta, int ld,
                                                      const Real* __restrict__ U,
                                                      const double* __restrict__ jinv, double gamma,
                                                      StepCtl* ctl, const double* __restrict__ refs) {
+    const int ntiles = ta.ntiles_dev ? *ta.ntiles_dev : ta.ntiles;
+    if ((int)blockIdx.x >= ntiles) return;
     const int4 d0 = __ldg(ta.desc + 2 * blockIdx.x);
     const int e = d0.x + threadIdx.x;
     StepCtl* c = ctl + d0.z;
@@ -581,15 +584,12 @@ __global__ void step_begin_kernel(StepCtl* ctls, int n) {
 // J. Comput. Phys. 141 (1998) 199-224, sec. 2.4/3.3).  In place: only
 // modes >= 1 change, and neighbours read only cell means.
 template <typename Real, int NB>
-__global__ void __launch_bounds__(128) limiter_kernel(int T, int ld, Real* __restrict__ U,
-                                                      const int4* __restrict__ conn,
-                                                      const double* __restrict__ lim,
-                                                      const double* __restrict__ jinv,
-                                                      double gammad, double f0, double f1,
-                                                      double f2, double f3, double tvb_m, int cfg) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= T) return;
-    const Tab<Real>& tb = tab<Real>(cfg);
+__device__ __forceinline__ void limit_element(int e, int ld, Real* __restrict__ U,
+                                              const int4* __restrict__ conn,
+                                              const double* __restrict__ lim,
+                                              const double* __restrict__ jinv, double gammad,
+                                              double f0, double f1, double f2, double f3,
+                                              double tvb_m, const Tab<Real>& tb) {
     const double2* j2 = reinterpret_cast<const double2*>(jinv);
     const double2 r0 = __ldg(j2 + e), r1 = __ldg(j2 + ld + e);
     Real u[3][4];
@@ -705,6 +705,35 @@ __global__ void __launch_bounds__(128) limiter_kernel(int T, int ld, Real* __res
         for (int i = 3; i < NB; ++i) out[i][v] = Real(0);
     }
     store_state<Real, NB>(U, ld, e, out);
+}
+
+// The limiter over tiles (one solve, a pack of solves or the serving pool):
+// tiles of solves whose flag is 0 (when flags is set) or whose control
+// block says done are skipped; P1 and P2 tiles limit their P1 part (P2
+// tiles drop their quadratic modes where limited).  Every path runs this one
+// kernel, so a solve limits to the same bits wherever it runs.
+template <typename Real>
+__global__ void __launch_bounds__(kTile) tiled_limiter_kernel(const TileArgs ta, int ld,
+                                                              Real* __restrict__ U,
+                                                              const int4* __restrict__ conn,
+                                                              const double* __restrict__ lim,
+                                                              const double* __restrict__ jinv,
+                                                              const int* __restrict__ flags,
+                                                              const double* __restrict__ refs,
+                                                              double gamma, double tvb_m,
+                                                              int cfg1, int cfg2,
+                                                              const StepCtl* __restrict__ ctl) {
+    const int ntiles = ta.ntiles_dev ? *ta.ntiles_dev : ta.ntiles;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int4 d0 = __ldg(ta.desc + 2 * tile);
+        if ((flags && !flags[d0.z]) || (ctl && ctl[d0.z].done) || (int)threadIdx.x >= d0.y) continue;
+        const double* f = refs + 4 * d0.z;
+        const int e = d0.x + threadIdx.x;
+        if (d0.w == 2)
+            limit_element<Real, 6>(e, ld, U, conn, lim, jinv, gamma, f[0], f[1], f[2], f[3], tvb_m, tab<Real>(cfg2));
+        else
+            limit_element<Real, 3>(e, ld, U, conn, lim, jinv, gamma, f[0], f[1], f[2], f[3], tvb_m, tab<Real>(cfg1));
+    }
 }
 
 // ---------------------------------------------------- basis conversion --
@@ -935,7 +964,7 @@ void launch_residual(const StageArgs& a, const TileArgs& t, int variant, int ord
 
 void launch_wave(const TileArgs& t, int ld, const void* U, int prec, const double* jinv,
                  double gamma, StepCtl* ctl, int nsolves, const double* refs, cudaStream_t stream) {
-    reset_wave_kernel<<<(nsolves + 127) / 128, 128, 0, stream>>>(ctl, nsolves);
+    if (nsolves > 0) reset_wave_kernel<<<(nsolves + 127) / 128, 128, 0, stream>>>(ctl, nsolves);
     if (t.ntiles > 0) {
         if (prec == RKDG_FP32)
             wave_kernel<float><<<t.ntiles, kTile, 0, stream>>>(t, ld, static_cast<const float*>(U), jinv, gamma, ctl, refs);
@@ -955,22 +984,16 @@ int tiled_max_ctas_per_sm(int prec, int order) {
     return order == 1 ? TiledOccupancy<double, 1>::value : TiledOccupancy<double, 2>::value;
 }
 
-void launch_limiter(int T, int ld, void* U, const int4* conn, const double* lim,
-                    const double* jinv, int order, int nq, int ng, int prec, double gamma,
-                    const double* far, double tvb_m, cudaStream_t stream) {
-    const int grid = (T + 127) / 128;
-    const int cfg = cfg_index(nq, ng);  // midpoint tables are in every uploaded configuration
-    if (prec == RKDG_FP32) {
-        if (order == 1)
-            limiter_kernel<float, 3><<<grid, 128, 0, stream>>>(T, ld, static_cast<float*>(U), conn, lim, jinv, gamma, far[0], far[1], far[2], far[3], tvb_m, cfg);
-        else
-            limiter_kernel<float, 6><<<grid, 128, 0, stream>>>(T, ld, static_cast<float*>(U), conn, lim, jinv, gamma, far[0], far[1], far[2], far[3], tvb_m, cfg);
-    } else {
-        if (order == 1)
-            limiter_kernel<double, 3><<<grid, 128, 0, stream>>>(T, ld, static_cast<double*>(U), conn, lim, jinv, gamma, far[0], far[1], far[2], far[3], tvb_m, cfg);
-        else
-            limiter_kernel<double, 6><<<grid, 128, 0, stream>>>(T, ld, static_cast<double*>(U), conn, lim, jinv, gamma, far[0], far[1], far[2], far[3], tvb_m, cfg);
-    }
+void launch_tiled_limiter(const TileArgs& t, int ctas, int ld, void* U, const int4* conn,
+                          const double* lim, const double* jinv, const int* flags,
+                          const double* refs, int prec, int nq2, double gamma, double tvb_m,
+                          const StepCtl* ctl, cudaStream_t stream) {
+    const int cfg1 = cfg_index(3, 2), cfg2 = cfg_index(nq2, 3);
+    const int grid = ctas > 0 ? ctas : std::max(1, t.ntiles);
+    if (prec == RKDG_FP32)
+        tiled_limiter_kernel<float><<<grid, kTile, 0, stream>>>(t, ld, static_cast<float*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl);
+    else
+        tiled_limiter_kernel<double><<<grid, kTile, 0, stream>>>(t, ld, static_cast<double*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl);
     RKDG_CUDA_TRY(cudaGetLastError());
 }
 

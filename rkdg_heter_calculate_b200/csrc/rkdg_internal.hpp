@@ -160,6 +160,7 @@ struct TileArgs {
     const uint16_t* task;  // task pool
     int max_halo;
     int ntiles;
+    const int* ntiles_dev;  // when set, kernels read the tile count here (graph-stable)
 };
 
 struct StageArgs {
@@ -188,16 +189,21 @@ void launch_stage(const StageArgs& a, const TileArgs& t, int variant, int order,
                   int flux, int prec, int block, cudaStream_t stream);
 void launch_residual(const StageArgs& a, const TileArgs& t, int variant, int order, int nq,
                      int ng, int flux, int prec, int block, cudaStream_t stream);
-// CFL measure per solve, one CTA per tile (resets the solves' wave slots first)
+// CFL measure per solve, one CTA per tile (resets the wave slots of solves
+// 0..nsolves-1 first; nsolves 0 leaves them as they are)
 // FP32 states store cell means as deviations from a per-solve reference
 // state (the far field); `refs` ([solves][4], device) / `ref` (4, host) give it.
 void launch_wave(const TileArgs& t, int ld, const void* U, int prec, const double* jinv,
                  double gamma, StepCtl* ctl, int nsolves, const double* refs, cudaStream_t stream);
 void launch_step_begin(StepCtl* ctl, int nsolves, cudaStream_t stream);
 int tiled_max_ctas_per_sm(int prec, int order);
-void launch_limiter(int T, int ld, void* U, const int4* conn, const double* lim,
-                    const double* jinv, int order, int nq, int ng, int prec, double gamma,
-                    const double* far, double tvb_m, cudaStream_t stream);
+// TVB limiter over tiles; flags[solve] (may be null: all on) enables it per
+// solve, solves whose control block (ctl may be null) says done are skipped;
+// ctas 0 = one CTA per tile
+void launch_tiled_limiter(const TileArgs& t, int ctas, int ld, void* U, const int4* conn,
+                          const double* lim, const double* jinv, const int* flags,
+                          const double* refs, int prec, int nq2, double gamma, double tvb_m,
+                          const StepCtl* ctl, cudaStream_t stream);
 void launch_import(int T, int ld, const double* staging, int ldh, const double* conv,
                    const int32_t* perm, void* U, int order, int prec, const double* ref,
                    cudaStream_t stream);

@@ -319,7 +319,8 @@ template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
 __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
     tiled_stage_kernel(const StageArgs a, const TileArgs ta) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    for (int tile = blockIdx.x; tile < ta.ntiles; tile += gridDim.x) {
+    const int ntiles = ta.ntiles_dev ? *ta.ntiles_dev : ta.ntiles;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int4 d0 = __ldg(ta.desc + 2 * tile), d1 = __ldg(ta.desc + 2 * tile + 1);
         if (ORD == 2 || (ORD == 3 && d0.w == 2))
             tile_stage<Real, 6, NQ2, 3, FLUX, MODE>(a, ta, d0, d1, smem_raw);
