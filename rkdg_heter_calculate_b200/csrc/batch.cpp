@@ -272,9 +272,9 @@ int rkdg_batch_create(int32_t nsolves, const rkdg_mesh_desc* meshes, const int32
         h2d(b, reinterpret_cast<int32_t*>(b->tcode), code);
         b->tdesc = (int4*)balloc(b, sizeof(int32_t) * b->desc_solve.size());
         upload_desc(b);
-        b->halo = (int2*)balloc(b, sizeof(int32_t) * std::max<size_t>(2, halo.size()));
+        b->halo = (int2*)balloc(b, sizeof(int32_t) * std::max<size_t>(2, halo.size()) + kTablePad);
         h2d(b, reinterpret_cast<int32_t*>(b->halo), halo);
-        b->task = (uint16_t*)balloc(b, sizeof(uint16_t) * std::max<size_t>(1, task.size()));
+        b->task = (uint16_t*)balloc(b, sizeof(uint16_t) * std::max<size_t>(1, task.size()) + kTablePad);
         h2d(b, b->task, task);
         b->perm = (int32_t*)balloc(b, sizeof(int32_t) * perm.size());
         h2d(b, b->perm, perm);
@@ -402,9 +402,7 @@ int rkdg_batch_advance(rkdg_batch* b, int32_t nsteps, const double* t_final, dou
             if (t) t[s] = b->h_ctl[s].t;
             if (steps) steps[s] = b->h_ctl[s].step - step0[s];
         }
-        for (int s = 0; s < b->S; ++s)
-            if (b->h_ctl[s].error)
-                throw Error{RKDG_ERR_STATE, "non-physical state in solve " + std::to_string(s)};
+        for (int s = 0; s < b->S; ++s) throw_ctl_error(b->h_ctl[s].error, "solve " + std::to_string(s));
     });
 }
 
@@ -465,7 +463,8 @@ int rkdg_batch_autotune(rkdg_batch* b, int32_t* ctas_out, int32_t* order_out) {
         RKDG_CUDA_TRY(cudaSetDevice(b->device));
         cudaDeviceProp prop;
         RKDG_CUDA_TRY(cudaGetDeviceProperties(&prop, b->device));
-        const int per_sm = tiled_max_ctas_per_sm(b->p.precision, b->ord == 1 ? 1 : 2);
+        const int per_sm = std::max(1, tiled_max_ctas_per_sm(b->p.precision, b->ord, b->p.nq, b->p.flux,
+                                                              b->tiles.max_halo));
         const int wave = prop.multiProcessorCount * per_sm;
         std::vector<int> cand_ctas = {0, wave, 2 * wave, 4 * wave};
         std::vector<int> cand_order = {0};

@@ -202,7 +202,7 @@ void enqueue_step(rkdg_ctx* c) {
 }
 
 void check_error_flag(rkdg_ctx* c) {
-    if (c->h_ctl->error) throw Error{RKDG_ERR_STATE, "non-physical state (NaN or non-positive density/pressure)"};
+    throw_ctl_error(c->h_ctl->error, "solve");
 }
 
 void destroy_ctx(rkdg_ctx* c) {
@@ -331,8 +331,8 @@ int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx*
             TileTables tt = build_tiles(c->mesh, 0, 0, params->order, 0, 0);
             c->d.tcode = (int4*)dev_alloc(c, sizeof(int32_t) * tt.code.size());
             c->d.tdesc = (int4*)dev_alloc(c, sizeof(int32_t) * tt.desc.size());
-            c->d.halo = (int2*)dev_alloc(c, sizeof(int32_t) * std::max<size_t>(2, tt.halo.size()));
-            c->d.task = (uint16_t*)dev_alloc(c, sizeof(uint16_t) * std::max<size_t>(1, tt.task.size()));
+            c->d.halo = (int2*)dev_alloc(c, sizeof(int32_t) * std::max<size_t>(2, tt.halo.size()) + kTablePad);
+            c->d.task = (uint16_t*)dev_alloc(c, sizeof(uint16_t) * std::max<size_t>(1, tt.task.size()) + kTablePad);
             RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.tcode, tt.code.data(), sizeof(int32_t) * tt.code.size(),
                                           cudaMemcpyHostToDevice, c->stream));
             RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.tdesc, tt.desc.data(), sizeof(int32_t) * tt.desc.size(),

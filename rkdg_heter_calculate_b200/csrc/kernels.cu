@@ -206,8 +206,11 @@ __device__ __forceinline__ void normal_flux(const Real u[4], Real Nx, Real Ny, R
 // Methods for Fluid Dynamics, 3rd ed., sec. 10.4): Davis wave-speed bounds
 // (eq. 10.48), contact speed S_M (eq. 10.37), star flux in its pressure form
 // F*_K = (S_M (S_K U_K - F_K) + S_K p* (0, nx, ny, S_M)) / (S_K - S_M),
-// p* = p_K + rho_K (S_K - q_K)(S_M - q_K): four reciprocals/quotients and two
-// square roots per point.
+// p* = p_K + rho_K (S_K - q_K)(S_M - q_K).  Branch-free: both physical
+// fluxes and the star flux are formed and the result selected (F_L when
+// S_L >= 0, F_R when S_R <= 0), so a warp whose points fall in different
+// wave regions runs one path; a star value formed where it is not selected
+// (even inf or NaN) is discarded.
 template <typename Real>
 __device__ __forceinline__ void hllc(const Real uL[4], const Real uR[4], Real nx, Real ny,
                                      Real gamma, Real f[4]) {
@@ -220,32 +223,22 @@ __device__ __forceinline__ void hllc(const Real uL[4], const Real uR[4], Real nx
     Real qL = vxL * nx + vyL * ny, qR = vxR * nx + vyR * ny;
     Real cL = sqrt_(gamma * pL * iL), cR = sqrt_(gamma * pR * iR);
     Real SL = fmin(qL - cL, qR - cR), SR = fmax(qL + cL, qR + cR);
-    if (SL >= Real(0)) {
-        f[0] = rL * qL;
-        f[1] = uL[1] * qL + pL * nx;
-        f[2] = uL[2] * qL + pL * ny;
-        f[3] = (uL[3] + pL) * qL;
-        return;
-    }
-    if (SR <= Real(0)) {
-        f[0] = rR * qR;
-        f[1] = uR[1] * qR + pR * nx;
-        f[2] = uR[2] * qR + pR * ny;
-        f[3] = (uR[3] + pR) * qR;
-        return;
-    }
+    const Real FL[4] = {rL * qL, uL[1] * qL + pL * nx, uL[2] * qL + pL * ny, (uL[3] + pL) * qL};
+    const Real FR[4] = {rR * qR, uR[1] * qR + pR * nx, uR[2] * qR + pR * ny, (uR[3] + pR) * qR};
     Real dL = rL * (SL - qL), dR = rR * (SR - qR);
     Real SM = div_(pR - pL + dL * qL - dR * qR, dL - dR);
     const bool left = SM >= Real(0);
-    const Real* u = left ? uL : uR;
     Real d = left ? dL : dR, p = left ? pL : pR, q = left ? qL : qR, S = left ? SL : SR;
     Real ps = p + d * (SM - q);
     Real k = rcp_(S - SM);
-    Real F0 = u[0] * q, F1 = u[1] * q + p * nx, F2 = u[2] * q + p * ny, F3 = (u[3] + p) * q;
-    f[0] = SM * (S * u[0] - F0) * k;
-    f[1] = (SM * (S * u[1] - F1) + S * ps * nx) * k;
-    f[2] = (SM * (S * u[2] - F2) + S * ps * ny) * k;
-    f[3] = (SM * (S * u[3] - F3) + S * ps * SM) * k;
+    const bool sl = SL >= Real(0), sr = SR <= Real(0);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const Real uK = left ? uL[v] : uR[v], FK = left ? FL[v] : FR[v];
+        const Real pn = v == 0 ? Real(0) : (v == 1 ? nx : (v == 2 ? ny : SM));
+        const Real fs = (SM * (S * uK - FK) + S * ps * pn) * k;
+        f[v] = sl ? FL[v] : (sr ? FR[v] : fs);
+    }
 }
 
 // ---------------------------------------------------------- reductions --
@@ -880,14 +873,15 @@ __global__ void __launch_bounds__(kTotBlock) totals_final_kernel(int n, const do
 // ----------------------------------------------------------- launchers --
 namespace {
 
+// Shared-memory attributes of one instantiation for a halo size; returns the
+// dynamic shared memory per CTA.
 template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
-void launch_tiled(const StageArgs& a, const TileArgs& t, int ctas, cudaStream_t s) {
-    const size_t smem = TiledSmem<Real, NQ2>::bytes(t.max_halo);
-    // dynamic + static shared memory above 48 KB needs the opt-in; the
-    // static part (tables, block reduction) is ~1.2 KB, so opt in early.
-    // Per instantiation; raised when a context with a larger halo appears.
+size_t prepare_tiled(int max_halo) {
+    const size_t smem = TiledSmem<Real, ORD>::bytes(max_halo);
+    // dynamic + static shared memory above 48 KB needs the opt-in.  Per
+    // instantiation; raised when a context with a larger halo appears.
     static size_t configured = 0;
-    if (configured == 0)  // residency is register-limited: give shared memory the carveout
+    if (configured == 0)  // give shared memory the whole carveout
         RKDG_CUDA_TRY(cudaFuncSetAttribute(tiled_stage_kernel<Real, NQ2, FLUX, MODE, ORD>,
                                            cudaFuncAttributePreferredSharedMemoryCarveout,
                                            (int)cudaSharedmemCarveoutMaxShared));
@@ -896,6 +890,21 @@ void launch_tiled(const StageArgs& a, const TileArgs& t, int ctas, cudaStream_t 
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         configured = smem;
     }
+    return smem;
+}
+
+template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
+int occupancy_tiled(int max_halo) {
+    const size_t smem = prepare_tiled<Real, NQ2, FLUX, MODE, ORD>(max_halo);
+    int n = 0;
+    RKDG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &n, tiled_stage_kernel<Real, NQ2, FLUX, MODE, ORD>, kTile, smem));
+    return n;
+}
+
+template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
+void launch_tiled(const StageArgs& a, const TileArgs& t, int ctas, cudaStream_t s) {
+    const size_t smem = prepare_tiled<Real, NQ2, FLUX, MODE, ORD>(t.max_halo);
     const int grid = (ctas > 0 && ctas < t.ntiles) ? ctas : t.ntiles;
     if (grid > 0) tiled_stage_kernel<Real, NQ2, FLUX, MODE, ORD><<<grid, kTile, smem, s>>>(a, t);
 }
@@ -979,9 +988,26 @@ void launch_step_begin(StepCtl* ctl, int nsolves, cudaStream_t stream) {
     RKDG_CUDA_TRY(cudaGetLastError());
 }
 
-int tiled_max_ctas_per_sm(int prec, int order) {
-    if (prec == RKDG_FP32) return order == 1 ? TiledOccupancy<float, 1>::value : TiledOccupancy<float, 2>::value;
-    return order == 1 ? TiledOccupancy<double, 1>::value : TiledOccupancy<double, 2>::value;
+int tiled_max_ctas_per_sm(int prec, int order, int nq, int flux, int max_halo) {
+    const bool h = flux == RKDG_FLUX_HLLC;
+    if (prec == RKDG_FP32) {
+        if (order == 1) return h ? occupancy_tiled<float, 6, RKDG_FLUX_HLLC, MODE_STAGE, 1>(max_halo)
+                                 : occupancy_tiled<float, 6, RKDG_FLUX_LLF, MODE_STAGE, 1>(max_halo);
+        if (order == 3) return h ? occupancy_tiled<float, 6, RKDG_FLUX_HLLC, MODE_STAGE, 3>(max_halo)
+                                 : occupancy_tiled<float, 6, RKDG_FLUX_LLF, MODE_STAGE, 3>(max_halo);
+        if (nq == 7) return h ? occupancy_tiled<float, 7, RKDG_FLUX_HLLC, MODE_STAGE, 2>(max_halo)
+                              : occupancy_tiled<float, 7, RKDG_FLUX_LLF, MODE_STAGE, 2>(max_halo);
+        return h ? occupancy_tiled<float, 6, RKDG_FLUX_HLLC, MODE_STAGE, 2>(max_halo)
+                 : occupancy_tiled<float, 6, RKDG_FLUX_LLF, MODE_STAGE, 2>(max_halo);
+    }
+    if (order == 1) return h ? occupancy_tiled<double, 6, RKDG_FLUX_HLLC, MODE_STAGE, 1>(max_halo)
+                             : occupancy_tiled<double, 6, RKDG_FLUX_LLF, MODE_STAGE, 1>(max_halo);
+    if (order == 3) return h ? occupancy_tiled<double, 6, RKDG_FLUX_HLLC, MODE_STAGE, 3>(max_halo)
+                             : occupancy_tiled<double, 6, RKDG_FLUX_LLF, MODE_STAGE, 3>(max_halo);
+    if (nq == 7) return h ? occupancy_tiled<double, 7, RKDG_FLUX_HLLC, MODE_STAGE, 2>(max_halo)
+                          : occupancy_tiled<double, 7, RKDG_FLUX_LLF, MODE_STAGE, 2>(max_halo);
+    return h ? occupancy_tiled<double, 6, RKDG_FLUX_HLLC, MODE_STAGE, 2>(max_halo)
+             : occupancy_tiled<double, 6, RKDG_FLUX_LLF, MODE_STAGE, 2>(max_halo);
 }
 
 void launch_tiled_limiter(const TileArgs& t, int ctas, int ld, void* U, const int4* conn,

@@ -100,6 +100,9 @@ uint32_t pack_info(const int8_t* shared3, const int8_t* bc3);
 //   bits 2-3 neighbour-local edge (kinds 0-2) or boundary tag (kind 3)
 //   bits 4.. local index of the in-tile neighbour, or the halo slot
 constexpr int kTile = 128;
+// Bytes added to the halo and task tables so that the stage kernel's L2
+// prefetch of a tile's list, rounded out to 16-byte boundaries, stays inside.
+constexpr size_t kTablePad = 64;
 enum { EDGE_IN_OWNER = 0, EDGE_IN_OTHER = 1, EDGE_HALO = 2, EDGE_BOUNDARY = 3 };
 
 // Tiles of one solve.  Element indices are global in the packed element
@@ -129,9 +132,15 @@ struct StepCtl {
     unsigned long long mon_bits[2]; // residual monitor, as bits
     int step;
     int done;
-    int error;                 // bit 0: non-physical state seen
+    int error;                 // bit 0: non-physical state seen; bit 1: a device wait timed out
     int pad;
 };
+
+// Throws the error a solve's control word reports (no-op when clean).
+inline void throw_ctl_error(int error, const std::string& who) {
+    if (error & 2) throw Error{RKDG_ERR_CUDA, who + ": a device-side wait on staged data timed out"};
+    if (error) throw Error{RKDG_ERR_STATE, who + ": non-physical state (NaN or non-positive density/pressure)"};
+}
 
 struct DeviceArrays {
     void* U[3] = {nullptr, nullptr, nullptr};  // state buffers (A holds U^n)
@@ -196,7 +205,8 @@ void launch_residual(const StageArgs& a, const TileArgs& t, int variant, int ord
 void launch_wave(const TileArgs& t, int ld, const void* U, int prec, const double* jinv,
                  double gamma, StepCtl* ctl, int nsolves, const double* refs, cudaStream_t stream);
 void launch_step_begin(StepCtl* ctl, int nsolves, cudaStream_t stream);
-int tiled_max_ctas_per_sm(int prec, int order);
+// resident CTAs per SM of the tiled stage kernel (order 3: mixed pack)
+int tiled_max_ctas_per_sm(int prec, int order, int nq, int flux, int max_halo);
 // TVB limiter over tiles; flags[solve] (may be null: all on) enables it per
 // solve, solves whose control block (ctl may be null) says done are skipped;
 // ctas 0 = one CTA per tile

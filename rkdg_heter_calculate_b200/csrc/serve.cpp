@@ -104,6 +104,7 @@ struct Request {
     int slot = -1;
     int64_t e_off = -1, h_off = -1, k_off = -1;
     std::string error;
+    int error_code = RKDG_ERR_STATE;
 };
 
 }  // namespace
@@ -328,7 +329,14 @@ void retire(rkdg_server* s, Request& r, bool failed) {
     s->active[r.slot].reset();
     r.t_done = now_s();
     r.status = failed ? REQ_FAILED : REQ_DONE;
-    if (failed) r.error = "non-physical state (NaN, rho <= 0 or p <= 0) in request " + std::to_string(r.id);
+    if (failed) {
+        try {
+            throw_ctl_error(s->h_ctl[r.slot].error, "request " + std::to_string(r.id));
+        } catch (const Error& e) {
+            r.error = e.msg;
+            r.error_code = e.code;
+        }
+    }
     r.tiles = TileTables();
     r.jinv.clear();
     r.lim.clear();
@@ -427,8 +435,8 @@ void engine_loop(rkdg_server* s) {
         std::lock_guard<std::mutex> lk(s->mu);
         s->fatal = e.msg;
         for (auto& r : s->active)
-            if (r) r->status = REQ_FAILED, r->error = e.msg;
-        for (auto& r : s->queue) r->status = REQ_FAILED, r->error = e.msg;
+            if (r) r->status = REQ_FAILED, r->error = e.msg, r->error_code = e.code;
+        for (auto& r : s->queue) r->status = REQ_FAILED, r->error = e.msg, r->error_code = e.code;
         s->queue.clear();
         s->cv_done.notify_all();
     }
@@ -516,8 +524,8 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
         s->conn = (int4*)salloc(s, sizeof(int4) * (size_t)s->cap);
         s->lim = (double*)salloc(s, sizeof(double) * 18 * (size_t)s->cap);
         s->perm = (int32_t*)salloc(s, sizeof(int32_t) * (size_t)s->cap);
-        s->halo = (int2*)salloc(s, sizeof(int2) * (size_t)s->hcap);
-        s->task = (uint16_t*)salloc(s, sizeof(uint16_t) * (size_t)s->kcap);
+        s->halo = (int2*)salloc(s, sizeof(int2) * (size_t)s->hcap + kTablePad);
+        s->task = (uint16_t*)salloc(s, sizeof(uint16_t) * (size_t)s->kcap + kTablePad);
         s->desc = (int4*)salloc(s, sizeof(int32_t) * 16 * (size_t)s->tcap);  // list + admission scratch
         s->ntiles_dev = (int*)salloc(s, sizeof(int));
         RKDG_CUDA_TRY(cudaMemsetAsync(s->ntiles_dev, 0, sizeof(int), s->stream));
@@ -544,8 +552,8 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
         for (int i = max_slots - 1; i >= 0; --i) s->free_slots.push_back(i);
         s->active.assign(max_slots, nullptr);
         // persistent grid, and a graph of one step whose tile count is read on the device
-        const int per_sm = tiled_max_ctas_per_sm(p.precision, 2);
-        s->ctas = 2 * prop.multiProcessorCount * per_sm;
+        const int per_sm = std::max(1, tiled_max_ctas_per_sm(p.precision, 3, p.nq, p.flux, kPoolHalo));
+        s->ctas = prop.multiProcessorCount * per_sm;
         s->tiles.code = s->tcode;
         s->tiles.desc = s->desc;
         s->tiles.halo = s->halo;
@@ -643,8 +651,9 @@ int rkdg_server_wait(rkdg_server* s, int64_t id, double timeout_s, int32_t* stat
             if (steps) *steps = r->steps;
             const bool failed = r->status == REQ_FAILED;
             std::string err = r->error;
+            const int code = r->error_code;
             s->reqs.erase(it);
-            if (failed) throw Error{RKDG_ERR_STATE, err.empty() ? "request failed" : err};
+            if (failed) throw Error{code, err.empty() ? "request failed" : err};
         }
     });
 }

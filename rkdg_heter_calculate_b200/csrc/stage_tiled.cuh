@@ -21,34 +21,180 @@
 // its own dt, CFL measure and monitor.  A tile's arithmetic depends only on
 // its own solve's data: results are deterministic and identical whether a
 // solve runs alone or in a batch.
+//
+// Staging pipeline: a tile's own state rows, J^-1 rows and edge codes are
+// contiguous 16-byte rows in HBM (pack p of element e at (p ld + e) 16), so
+// one thread moves them into shared memory with bulk asynchronous copies
+// (cp.async.bulk, completion counted in bytes on an mbarrier).  The copies
+// for the CTA's next tile are issued as soon as phase A has read the current
+// tile's rows, and run under the current tile's halo, flux and update work;
+// the next tile's U^n rows are prefetched into L2 at the same time.
 
-template <typename Real, int NQ2>
+// ------------------------------------------------------------- staging --
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+// 16-byte asynchronous gather into shared memory (completion per thread).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// Orders this thread's earlier generic-proxy shared-memory accesses before
+// later asynchronous-proxy (bulk copy) accesses.
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Waits for the barrier phase of the given parity; gives up after about two
+// seconds (or 2^26 polls), returning false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 1; it < (1u << 26); ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 255u) == 0 && global_ns() - t0 > 2000000000ull) return false;
+    }
+    return false;
+}
+
+// Shared memory of one CTA: the work area (J^-1, 2 area, edge codes, flux
+// tasks, own traces and means, halo traces and means), sized for the largest
+// tile layout the kernel dispatches (P1 tiles of a mixed pack use a prefix),
+// then the staging area.  The staging area first receives the tile's own
+// rows by bulk copy -- the state (SROWS rows of 16 bytes per element), the
+// two J^-1 rows and the edge-code row -- and, once phase A has read them,
+// the halo neighbours' states by 16-byte gathers ([SROWS][hm] rows).
+template <typename Real, int ORD>
 struct TiledSmem {
-    // sized for the larger (P2, 3 edge points) layout; P1 tiles use a prefix
-    static constexpr size_t bytes(int hm) {
-        constexpr int NG = 3;
-        return sizeof(double) * 5 * kTile +
+    static constexpr int NG = ORD == 1 ? 2 : 3;
+    static constexpr int SROWS = (ORD == 1 ? 3 : 6) * (int)(sizeof(Real) / 4);
+    static constexpr int MAX_TASKS = 3 * kTile;
+    __host__ __device__ static constexpr size_t work(int hm) {
+        return sizeof(double) * 5 * kTile + sizeof(int4) * kTile + sizeof(uint16_t) * MAX_TASKS +
                sizeof(Real) * ((size_t)3 * NG * 4 * kTile + 4 * kTile + (size_t)NG * 4 * hm + 4 * hm);
     }
+    __host__ __device__ static constexpr size_t stage_offset(int hm) { return (work(hm) + 127) / 128 * 128; }
+    __host__ __device__ static constexpr size_t stage_rows(int hm) {
+        return (size_t)(SROWS + 3) * kTile > (size_t)SROWS * hm ? (size_t)(SROWS + 3) * kTile : (size_t)SROWS * hm;
+    }
+    __host__ __device__ static constexpr size_t bytes(int hm) { return stage_offset(hm) + stage_rows(hm) * 16; }
 };
 
-// Resident CTAs per SM the register allocation is held to (FP64 P2 would
-// otherwise take ~218 registers and leave 8 warps per SM).
+// Resident CTAs per SM the register allocation is held to.
 template <typename Real, int ORD>
 struct TiledOccupancy {
-    static constexpr int value = sizeof(Real) == 8 ? (ORD == 1 ? 4 : 3) : (ORD == 1 ? 8 : 5);
+    static constexpr int value = sizeof(Real) == 8 ? (ORD == 1 ? 3 : 2) : (ORD == 1 ? 5 : 4);
 };
 
-template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE>
+// Issues the bulk copies of tile d's rows into the staging area (one thread),
+// and L2 prefetches of its U^n rows and of its halo and task lists (the
+// tables are padded so that the 16-byte rounding stays inside them).
+template <typename Real, int SROWS>
+__device__ __forceinline__ void stage_issue(const StageArgs& a, const TileArgs& ta, const int4 d,
+                                            const int4 dd, unsigned char* stg, uint64_t* bar) {
+    const int rows = (d.w == 2 ? 6 : 3) * (int)(sizeof(Real) / 4);
+    const uint32_t rb = (uint32_t)d.y * 16u;
+    mbar_expect_tx(bar, rb * (uint32_t)(rows + 3));
+    const char* U = static_cast<const char*>(a.U);
+    for (int r = 0; r < rows; ++r)
+        bulk_g2s(stg + (size_t)r * kTile * 16, U + ((size_t)r * a.ld + d.x) * 16, rb, bar);
+    const char* J = reinterpret_cast<const char*>(a.jinv);
+    bulk_g2s(stg + (size_t)SROWS * kTile * 16, J + (size_t)d.x * 16, rb, bar);
+    bulk_g2s(stg + (size_t)(SROWS + 1) * kTile * 16, J + ((size_t)a.ld + d.x) * 16, rb, bar);
+    bulk_g2s(stg + (size_t)(SROWS + 2) * kTile * 16, ta.code + d.x, rb, bar);
+    if (a.U0 != nullptr) {
+        const char* U0 = static_cast<const char*>(a.U0);
+        for (int r = 0; r < rows; ++r) bulk_prefetch_l2(U0 + ((size_t)r * a.ld + d.x) * 16, rb);
+    }
+    if (dd.y > 0) {
+        const uintptr_t b = reinterpret_cast<uintptr_t>(ta.halo + dd.x) & ~uintptr_t(15);
+        const uintptr_t e = (reinterpret_cast<uintptr_t>(ta.halo + dd.x + dd.y) + 15) & ~uintptr_t(15);
+        bulk_prefetch_l2(reinterpret_cast<const void*>(b), (uint32_t)(e - b));
+    }
+    if (dd.w > 0) {
+        const uintptr_t b = reinterpret_cast<uintptr_t>(ta.task + dd.z) & ~uintptr_t(15);
+        const uintptr_t e = (reinterpret_cast<uintptr_t>(ta.task + dd.z + dd.w) + 15) & ~uintptr_t(15);
+        bulk_prefetch_l2(reinterpret_cast<const void*>(b), (uint32_t)(e - b));
+    }
+}
+
+// Element x's state from the staging rows.
+template <typename Real, int NB>
+__device__ __forceinline__ void load_staged(const unsigned char* stg, int x, Real u[NB][4]) {
+    if constexpr (sizeof(Real) == 8) {
+        const double2* p = reinterpret_cast<const double2*>(stg);
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+            const double2 a = p[(2 * i) * kTile + x], b = p[(2 * i + 1) * kTile + x];
+            u[i][0] = a.x;
+            u[i][1] = a.y;
+            u[i][2] = b.x;
+            u[i][3] = b.y;
+        }
+    } else {
+        const float4* p = reinterpret_cast<const float4*>(stg);
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+            const float4 a = p[i * kTile + x];
+            u[i][0] = a.x;
+            u[i][1] = a.y;
+            u[i][2] = a.z;
+            u[i][3] = a.w;
+        }
+    }
+}
+
+// FP32 tiles keep the stage input in registers from phase A to the update;
+// FP64 tiles, short of registers, read it again (an L2 hit).
+#ifndef RKDG_HOLD_STATE
+#define RKDG_HOLD_STATE 1
+#endif
+
+template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE, int SROWS>
 __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& ta, const int4 d0,
-                                           const int4 d1, unsigned char* smem_raw) {
+                                           const int4 d1, unsigned char* smem_raw, unsigned char* stg,
+                                           const int4 dn, const int4 dn1, uint64_t* bar) {
     constexpr int CFG = cfg_index(NQ, NG);
     constexpr int BT = kTile;
+    constexpr bool HOLD = RKDG_HOLD_STATE && sizeof(Real) == 4;
     const Tab<Real>& tb = tab<Real>(CFG);
     const int HM = ta.max_halo;
     double* s_jinv = reinterpret_cast<double*>(smem_raw);  // [4][BT]
     double* s_area2 = s_jinv + 4 * BT;                     // [BT] twice the area
-    Real* s_tr = reinterpret_cast<Real*>(s_area2 + BT);    // [3][NG][4][BT]
+    int4* s_code = reinterpret_cast<int4*>(s_area2 + BT);  // [BT] edge codes
+    uint16_t* s_task = reinterpret_cast<uint16_t*>(s_code + BT);  // [3 BT] flux tasks
+    Real* s_tr = reinterpret_cast<Real*>(s_task + 3 * BT);  // [3][NG][4][BT]
     Real* s_mean = s_tr + 3 * NG * 4 * BT;                 // [4][BT]
     Real* s_htr = s_mean + 4 * BT;                         // [NG][4][HM]
     Real* s_hmean = s_htr + NG * 4 * HM;                   // [4][HM]
@@ -59,32 +205,66 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     }
     const int sid = d0.z;
     StepCtl* ctl = a.ctl + sid;
-    if (MODE == MODE_STAGE && ctl->done) return;  // uniform over the CTA
 
     const int tid = threadIdx.x;
     const int e0 = d0.x;
     const int e = e0 + tid;
     const bool active = tid < d0.y;
     const int ee = active ? e : e0;
+    const int sx = active ? tid : 0;  // staging row index
     const Real* __restrict__ U = static_cast<const Real*>(a.U);
     const Real gamma = (Real)a.gamma, gm1 = gamma - Real(1);
     const double* fs = a.far_sid ? a.far_sid + 4 * sid : a.far;
     Real far[4] = {(Real)fs[0], (Real)fs[1], (Real)fs[2], (Real)fs[3]};
 
     // ------------------------------------------------------------ phase A
+    // the halo and task lists first (L2 hits: prefetched with the tile's
+    // rows); their latency runs under the staged reads
+    constexpr int SR = NB * (int)(sizeof(Real) / 4);  // 16-byte rows of a state
+    const int h0 = d1.x, nh = d1.y, t0 = d1.z, nt = d1.w;
+    int2 hh[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const int h = tid + r * BT;
+        hh[r] = h < nh ? __ldg(ta.halo + h0 + h) : make_int2(0, 0);
+    }
+    uint16_t tk[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const int j = tid + r * BT;
+        tk[r] = j < nt ? __ldg(ta.task + t0 + j) : (uint16_t)0;
+    }
     Real R[NB][4];
-    const double2* jinv2 = reinterpret_cast<const double2*>(a.jinv);
-    const double2 r0 = __ldg(jinv2 + ee), r1 = __ldg(jinv2 + a.ld + ee);
+    Real u[NB][4];
+    const double2* sj = reinterpret_cast<const double2*>(stg + (size_t)SROWS * BT * 16);
+    const double2 r0 = sj[sx], r1 = sj[BT + sx];
+    s_code[tid] = reinterpret_cast<const int4*>(stg + (size_t)(SROWS + 2) * BT * 16)[sx];
     s_jinv[0 * BT + tid] = r0.x;
     s_jinv[1 * BT + tid] = r0.y;
     s_jinv[2 * BT + tid] = r1.x;
     s_jinv[3 * BT + tid] = r1.y;
     s_area2[tid] = 1.0 / (r0.x * r1.y - r0.y * r1.x);  // 2 * area
+    Real m_st[4];  // the stored cell mean (a deviation in FP32)
     {
-        Real u[NB][4];
-        load_state<Real, NB>(U, a.ld, ee, u);
+        load_staged<Real, NB>(stg, sx, u);
+        __syncthreads();  // staged rows consumed: the area takes the halo states
+        {
+            const char* Ub = static_cast<const char*>(a.U);
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const int h = tid + r * BT;
+                if (h < nh) {
+#pragma unroll
+                    for (int q = 0; q < SR; ++q)
+                        cp_async16(stg + ((size_t)q * HM + h) * 16, Ub + ((size_t)q * a.ld + hh[r].x) * 16);
+                }
+                const int j = tid + r * BT;
+                if (j < nt) s_task[j] = tk[r];
+            }
+        }
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
+            m_st[v] = u[0][v];
             u[0][v] += ref_of<Real>(fs, v);  // stored deviation -> state (FP32)
             s_mean[v * BT + tid] = u[0][v];
         }
@@ -127,39 +307,63 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                     for (int i = 0; i < NB; ++i) s += tb.ephi[k][g][i] * u[i][v];
                     s_tr[((k * NG + g) * 4 + v) * BT + tid] = s;
                 }
+        if constexpr (HOLD) {
+#pragma unroll
+            for (int v = 0; v < 4; ++v) u[0][v] = m_st[v];  // the stored values for the update
+        }
     }
-    __syncthreads();  // s_ephi visible below; own traces complete
+    cp_async_wait_all();
+    __syncthreads();  // s_ephi visible below; own traces complete; halo states landed
     {
-        const int h0 = d1.x, nh = d1.y;
-        for (int h = tid; h < nh; h += BT) {
-            const int2 hh = __ldg(ta.halo + h0 + h);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            const int h = tid + r * BT;
+            if (h >= nh) break;
             Real un[NB][4];
-            load_state<Real, NB>(U, a.ld, hh.x, un);
+            if constexpr (sizeof(Real) == 8) {
+                const double2* p = reinterpret_cast<const double2*>(stg);
+#pragma unroll
+                for (int i = 0; i < NB; ++i) {
+                    const double2 x = p[(2 * i) * HM + h], y = p[(2 * i + 1) * HM + h];
+                    un[i][0] = x.x, un[i][1] = x.y, un[i][2] = y.x, un[i][3] = y.y;
+                }
+            } else {
+                const float4* p = reinterpret_cast<const float4*>(stg);
+#pragma unroll
+                for (int i = 0; i < NB; ++i) {
+                    const float4 x = p[i * HM + h];
+                    un[i][0] = x.x, un[i][1] = x.y, un[i][2] = x.z, un[i][3] = x.w;
+                }
+            }
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
                 un[0][v] += ref_of<Real>(fs, v);
                 s_hmean[v * HM + h] = un[0][v];
             }
+            const int he = hh[r].y;
 #pragma unroll
             for (int g = 0; g < NG; ++g)
 #pragma unroll
                 for (int v = 0; v < 4; ++v) {
                     Real s = Real(0);
 #pragma unroll
-                    for (int i = 0; i < NB; ++i) s += s_ephi[hh.y][g][i] * un[i][v];
+                    for (int i = 0; i < NB; ++i) s += s_ephi[he][g][i] * un[i][v];
                     s_htr[(g * 4 + v) * HM + h] = s;
                 }
         }
     }
-    __syncthreads();
+    __syncthreads();  // halo traces complete; halo states read
+    if (tid == 0 && dn.y > 0) {
+        fence_proxy_async();
+        stage_issue<Real, SROWS>(a, ta, dn, dn1, stg, bar);
+    }
 
     // ------------------------------------------------------------ phase B
     {
-        const int t0 = d1.z, nt = d1.w;
         for (int j = tid; j < nt; j += BT) {
-            const int tk = __ldg(ta.task + t0 + j);
-            const int le = tk >> 2, k = tk & 3;
-            const int c = __ldg(&ta.code[e0 + le].x + k);
+            const int tkj = s_task[j];
+            const int le = tkj >> 2, k = tkj & 3;
+            const int c = reinterpret_cast<const int*>(s_code + le)[k];
             const int kind = c & 3, se = (c >> 2) & 3, idx = c >> 4;
             // physical normal N = n * length of edge k of element le from the
             // FP64 J^-1 and area (N_k / area = 2(r0 + r1), -2 r0, -2 r1);
@@ -243,7 +447,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     __syncthreads();
 
     // ------------------------------------------------------------ phase C
-    const int4 cd = __ldg(ta.code + ee);
+    const int4 cd = s_code[tid];
     const Real inv_area = (Real)(2.0 / s_area2[tid]);  // 1 / area
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -278,8 +482,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     const Real dt = (Real)dtd, ca = (Real)a.a, cb = (Real)a.b;
     Real u0m[4] = {Real(0), Real(0), Real(0), Real(0)};
     {
-        Real u[NB][4];
-        load_state<Real, NB>(U, a.ld, ee, u);  // stored values (L1/L2 hit: read in phase A)
+        if constexpr (!HOLD) load_state<Real, NB>(U, a.ld, ee, u);  // stored values (L2 hit)
         if (a.U0 != nullptr) {
             Real u0[NB][4];
             load_state<Real, NB>(static_cast<const Real*>(a.U0), a.ld, ee, u0);
@@ -315,17 +518,43 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 
 // ORD: 1 = P1 tiles only, 2 = P2 tiles only, 3 = both (dispatch per tile;
 // P2 tiles use the NQ2-point volume rule, P1 tiles the 3/2-point rules).
+// A barrier wait that times out sets bit 1 of the solve's error word and
+// ends the CTA (all threads together).
 template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
 __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
     tiled_stage_kernel(const StageArgs a, const TileArgs ta) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using SM = TiledSmem<Real, ORD>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t s_bar;
+    unsigned char* stg = smem_raw + SM::stage_offset(ta.max_halo);
     const int ntiles = ta.ntiles_dev ? *ta.ntiles_dev : ta.ntiles;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    int tile = blockIdx.x;
+    if (tile >= ntiles) return;
+    if (threadIdx.x == 0) mbar_init(&s_bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0)
+        stage_issue<Real, SM::SROWS>(a, ta, __ldg(ta.desc + 2 * tile), __ldg(ta.desc + 2 * tile + 1), stg,
+                                     &s_bar);
+    uint32_t parity = 0;
+    for (; tile < ntiles; tile += gridDim.x) {
         const int4 d0 = __ldg(ta.desc + 2 * tile), d1 = __ldg(ta.desc + 2 * tile + 1);
+        const int nxt = tile + gridDim.x;
+        const int4 dn = nxt < ntiles ? __ldg(ta.desc + 2 * nxt) : make_int4(0, 0, 0, 0);
+        const int4 dn1 = nxt < ntiles ? __ldg(ta.desc + 2 * nxt + 1) : make_int4(0, 0, 0, 0);
+        const bool ok = mbar_wait(&s_bar, parity);
+        if (__syncthreads_or(!ok)) {  // also: every thread has seen this phase complete
+            if (threadIdx.x == 0) atomicOr(&a.ctl[d0.z].error, 2);
+            return;
+        }
+        parity ^= 1u;
+        if (MODE == MODE_STAGE && a.ctl[d0.z].done) {  // finished solve: pass the tile on
+            if (threadIdx.x == 0 && dn.y > 0) stage_issue<Real, SM::SROWS>(a, ta, dn, dn1, stg, &s_bar);
+            continue;
+        }
         if (ORD == 2 || (ORD == 3 && d0.w == 2))
-            tile_stage<Real, 6, NQ2, 3, FLUX, MODE>(a, ta, d0, d1, smem_raw);
+            tile_stage<Real, 6, NQ2, 3, FLUX, MODE, SM::SROWS>(a, ta, d0, d1, smem_raw, stg, dn, dn1, &s_bar);
         else
-            tile_stage<Real, 3, 3, 2, FLUX, MODE>(a, ta, d0, d1, smem_raw);
+            tile_stage<Real, 3, 3, 2, FLUX, MODE, SM::SROWS>(a, ta, d0, d1, smem_raw, stg, dn, dn1, &s_bar);
         __syncthreads();  // shared memory is reused by the next tile
     }
 }
