@@ -214,8 +214,16 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     const int sx = active ? tid : 0;  // staging row index
     const Real* __restrict__ U = static_cast<const Real*>(a.U);
     const Real gamma = (Real)a.gamma, gm1 = gamma - Real(1);
-    const double* fs = a.far_sid ? a.far_sid + 4 * sid : a.far;
-    Real far[4] = {(Real)fs[0], (Real)fs[1], (Real)fs[2], (Real)fs[3]};
+    // far-field / reference state by value (a pointer into the parameter
+    // block would put the parameter array in local memory)
+    double fs[4];
+    if (a.far_sid) {
+        const double* p = a.far_sid + 4 * sid;
+        fs[0] = p[0], fs[1] = p[1], fs[2] = p[2], fs[3] = p[3];
+    } else {
+        fs[0] = a.far[0], fs[1] = a.far[1], fs[2] = a.far[2], fs[3] = a.far[3];
+    }
+    const Real far[4] = {(Real)fs[0], (Real)fs[1], (Real)fs[2], (Real)fs[3]};
 
     // ------------------------------------------------------------ phase A
     // the halo and task lists first (L2 hits: prefetched with the tile's
@@ -318,7 +326,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
             const int h = tid + r * BT;
-            if (h >= nh) break;
+            if (h < nh) {
             Real un[NB][4];
             if constexpr (sizeof(Real) == 8) {
                 const double2* p = reinterpret_cast<const double2*>(stg);
@@ -350,6 +358,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                     for (int i = 0; i < NB; ++i) s += s_ephi[he][g][i] * un[i][v];
                     s_htr[(g * 4 + v) * HM + h] = s;
                 }
+            }
         }
     }
     __syncthreads();  // halo traces complete; halo states read
@@ -539,8 +548,11 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
     for (; tile < ntiles; tile += gridDim.x) {
         const int4 d0 = __ldg(ta.desc + 2 * tile), d1 = __ldg(ta.desc + 2 * tile + 1);
         const int nxt = tile + gridDim.x;
-        const int4 dn = nxt < ntiles ? __ldg(ta.desc + 2 * nxt) : make_int4(0, 0, 0, 0);
-        const int4 dn1 = nxt < ntiles ? __ldg(ta.desc + 2 * nxt + 1) : make_int4(0, 0, 0, 0);
+        int4 dn = make_int4(0, 0, 0, 0), dn1 = dn;
+        if (nxt < ntiles) {
+            dn = __ldg(ta.desc + 2 * nxt);
+            dn1 = __ldg(ta.desc + 2 * nxt + 1);
+        }
         const bool ok = mbar_wait(&s_bar, parity);
         if (__syncthreads_or(!ok)) {  // also: every thread has seen this phase complete
             if (threadIdx.x == 0) atomicOr(&a.ctl[d0.z].error, 2);
