@@ -282,19 +282,40 @@ __device__ __forceinline__ void block_max3_atomic(double a, double b, double c,
     }
 }
 
-// (|u| + c) * perimeter / area of a cell mean (src/kernelfunctions.cu:19-25),
-// with perimeter / area = sum_k |N_k / area|; FP64.
-__device__ __forceinline__ double wave_measure(double rho, double mu, double mv, double E,
-                                               double gamma, double2 r0, double2 r1, bool& bad) {
-    double u = mu / rho, v = mv / rho;
-    double p = (gamma - 1) * (E - 0.5 * rho * (u * u + v * v));
-    double a = sqrt(gamma * p / rho);
-    double l0 = 2.0 * hypot(r0.x + r1.x, r0.y + r1.y);
-    double l1 = 2.0 * hypot(r0.x, r0.y);
-    double l2 = 2.0 * hypot(r1.x, r1.y);
-    bad = !(rho > 0.0) || !(p > 0.0);
-    double w = (sqrt(u * u + v * v) + a) * (l0 + l1 + l2);
-    return bad ? __longlong_as_double(0x7ff8000000000000LL) : w;
+// sqrt that returns 0 at 0 (the FP32 form uses the reciprocal square root).
+__device__ __forceinline__ double sqrt0_(double x) { return sqrt(x); }
+__device__ __forceinline__ float sqrt0_(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+
+// Edge lengths |N_k| and 1 / area of an element from its FP64 J^-1 rows:
+// N_k = 2 area (r0 + r1, -r0, -r1) in FP64, cast to the working precision,
+// its length there; 1 / area = 2 det J^-1.  The tile kernel forms the same
+// values in phase A.
+template <typename Real>
+__device__ __forceinline__ void elem_lengths(double2 r0, double2 r1, Real len[3], Real& inv_area) {
+    const double det = r0.x * r1.y - r0.y * r1.x;
+    inv_area = (Real)(2.0 * det);
+    const double area2 = 1.0 / det;
+    const double cx[3] = {r0.x + r1.x, -r0.x, -r1.x}, cy[3] = {r0.y + r1.y, -r0.y, -r1.y};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const Real Nx = (Real)(cx[k] * area2), Ny = (Real)(cy[k] * area2);
+        len[k] = sqrt_(Nx * Nx + Ny * Ny);
+    }
+}
+
+// (|u| + c) * perimeter / area of a cell mean (src/kernelfunctions.cu:19-25)
+// in the working precision; the max over cells and dt = CFL / max are FP64.
+// A non-physical mean (rho <= 0, p <= 0, NaN) sets bad and returns NaN.
+template <typename Real>
+__device__ __forceinline__ double wave_of(const Real m[4], Real gamma, const Real len[3], Real inv_area,
+                                          bool& bad) {
+    const Real ri = rcp_(m[0]);
+    const Real u = m[1] * ri, v = m[2] * ri;
+    const Real p = (gamma - Real(1)) * (m[3] - Real(0.5) * (m[1] * u + m[2] * v));
+    bad = !(m[0] > Real(0)) || !(p > Real(0));
+    const Real c = sqrt0_(gamma * p * ri);
+    const Real w = (sqrt0_(u * u + v * v) + c) * ((len[0] + len[1] + len[2]) * inv_area);
+    return bad ? __longlong_as_double(0x7ff8000000000000LL) : (double)w;
 }
 
 // ------------------------------------------------------------ the stage --
@@ -493,10 +514,11 @@ __global__ void __launch_bounds__(128) stage_kernel(const StageArgs a) {
         double wv = 0.0, m0 = 0.0, m1 = 0.0;
         if (active) {
             bool bad;
-            wv = wave_measure((double)R[0][0] + (double)ref_of<Real>(a.far, 0),
-                              (double)R[0][1] + (double)ref_of<Real>(a.far, 1),
-                              (double)R[0][2] + (double)ref_of<Real>(a.far, 2),
-                              (double)R[0][3] + (double)ref_of<Real>(a.far, 3), a.gamma, r0, r1, bad);
+            Real m[4], len[3], ia;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) m[v] = R[0][v] + ref_of<Real>(a.far, v);
+            elem_lengths<Real>(r0, r1, len, ia);
+            wv = wave_of<Real>(m, gamma, len, ia, bad);
             if (bad) atomicOr(&a.ctl->error, 1);
             m0 = fabs((double)R[0][0] - (double)u0m[0]);
             m1 = fabs((double)R[0][3] - (double)u0m[3]);
@@ -526,10 +548,11 @@ __global__ void __launch_bounds__(kTile) wave_kernel(const TileArgs ta, int ld,
         load_mean<Real, 1>(U, ld, e, m);
         const double2* j2 = reinterpret_cast<const double2*>(jinv);
         bool bad;
-        w = wave_measure((double)m[0] + (double)ref_of<Real>(ref, 0),
-                         (double)m[1] + (double)ref_of<Real>(ref, 1),
-                         (double)m[2] + (double)ref_of<Real>(ref, 2),
-                         (double)m[3] + (double)ref_of<Real>(ref, 3), gamma, j2[e], j2[ld + e], bad);
+        Real mm[4], len[3], ia;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) mm[v] = m[v] + ref_of<Real>(ref, v);
+        elem_lengths<Real>(j2[e], j2[ld + e], len, ia);
+        w = wave_of<Real>(mm, (Real)gamma, len, ia, bad);
         if (bad) atomicOr(&c->error, 1);
     }
     block_max3_atomic(w, 0.0, 0.0, &c->wave_bits, nullptr, nullptr);

@@ -88,21 +88,41 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     return false;
 }
 
-// Shared memory of one CTA: the work area (J^-1, 2 area, edge codes, flux
-// tasks, own traces and means, halo traces and means), sized for the largest
-// tile layout the kernel dispatches (P1 tiles of a mixed pack use a prefix),
-// then the staging area.  The staging area first receives the tile's own
-// rows by bulk copy -- the state (SROWS rows of 16 bytes per element), the
-// two J^-1 rows and the edge-code row -- and, once phase A has read them,
-// the halo neighbours' states by 16-byte gathers ([SROWS][hm] rows).
+// Shared memory of one CTA: the work area (edge normals, edge codes, flux
+// tasks, own traces and means, halo traces and means as 4-vectors), sized
+// for the largest tile layout the kernel dispatches (P1 tiles of a mixed
+// pack use a prefix), then the staging area.  The staging area first
+// receives the tile's own rows by bulk copy -- the state (SROWS rows of 16
+// bytes per element), the two J^-1 rows and the edge-code row -- and, once
+// phase A has read them, the halo neighbours' states by 16-byte gathers
+// ([SROWS][hm] rows).
+template <typename Real>
+struct alignas(16) Vec4 {
+    Real x, y, z, w;
+};
+template <typename Real>
+__device__ __forceinline__ void put4(Vec4<Real>* p, const Real a[4]) {
+    Vec4<Real> t;
+    t.x = a[0], t.y = a[1], t.z = a[2], t.w = a[3];
+    *p = t;
+}
+template <typename Real>
+__device__ __forceinline__ void get4(const Vec4<Real>* p, Real a[4]) {
+    const Vec4<Real> t = *p;
+    a[0] = t.x, a[1] = t.y, a[2] = t.z, a[3] = t.w;
+}
+template <typename Real>
+struct TiledLayout {
+    static constexpr size_t code_off = (sizeof(Real) * 9 * kTile + 15) / 16 * 16;
+};
+
 template <typename Real, int ORD>
 struct TiledSmem {
     static constexpr int NG = ORD == 1 ? 2 : 3;
     static constexpr int SROWS = (ORD == 1 ? 3 : 6) * (int)(sizeof(Real) / 4);
-    static constexpr int MAX_TASKS = 3 * kTile;
     __host__ __device__ static constexpr size_t work(int hm) {
-        return sizeof(double) * 5 * kTile + sizeof(int4) * kTile + sizeof(uint16_t) * MAX_TASKS +
-               sizeof(Real) * ((size_t)3 * NG * 4 * kTile + 4 * kTile + (size_t)NG * 4 * hm + 4 * hm);
+        return TiledLayout<Real>::code_off + sizeof(int4) * kTile + sizeof(uint16_t) * 3 * kTile +
+               sizeof(Vec4<Real>) * ((size_t)3 * NG * kTile + kTile + (size_t)NG * hm + hm);
     }
     __host__ __device__ static constexpr size_t stage_offset(int hm) { return (work(hm) + 127) / 128 * 128; }
     __host__ __device__ static constexpr size_t stage_rows(int hm) {
@@ -188,16 +208,16 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     constexpr int CFG = cfg_index(NQ, NG);
     constexpr int BT = kTile;
     constexpr bool HOLD = RKDG_HOLD_STATE && sizeof(Real) == 4;
+    using V4 = Vec4<Real>;
     const Tab<Real>& tb = tab<Real>(CFG);
     const int HM = ta.max_halo;
-    double* s_jinv = reinterpret_cast<double*>(smem_raw);  // [4][BT]
-    double* s_area2 = s_jinv + 4 * BT;                     // [BT] twice the area
-    int4* s_code = reinterpret_cast<int4*>(s_area2 + BT);  // [BT] edge codes
-    uint16_t* s_task = reinterpret_cast<uint16_t*>(s_code + BT);  // [3 BT] flux tasks
-    Real* s_tr = reinterpret_cast<Real*>(s_task + 3 * BT);  // [3][NG][4][BT]
-    Real* s_mean = s_tr + 3 * NG * 4 * BT;                 // [4][BT]
-    Real* s_htr = s_mean + 4 * BT;                         // [NG][4][HM]
-    Real* s_hmean = s_htr + NG * 4 * HM;                   // [4][HM]
+    Real* s_nrm = reinterpret_cast<Real*>(smem_raw);                       // [3][3][BT] Nx, Ny, len
+    int4* s_code = reinterpret_cast<int4*>(smem_raw + TiledLayout<Real>::code_off);  // [BT]
+    uint16_t* s_task = reinterpret_cast<uint16_t*>(s_code + BT);           // [3 BT] flux tasks
+    V4* s_tr = reinterpret_cast<V4*>(s_task + 3 * BT);                     // [3][NG][BT] own traces
+    V4* s_mean = s_tr + 3 * NG * BT;                                       // [BT]
+    V4* s_htr = s_mean + BT;                                               // [NG][HM] halo traces
+    V4* s_hmean = s_htr + NG * HM;                                         // [HM]
     __shared__ Real s_ephi[3][NG][NB];
     for (int x = threadIdx.x; x < 3 * NG * NB; x += BT) {
         int k = x / (NG * NB), g = (x / NB) % NG, i = x % NB;
@@ -247,11 +267,21 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     const double2* sj = reinterpret_cast<const double2*>(stg + (size_t)SROWS * BT * 16);
     const double2 r0 = sj[sx], r1 = sj[BT + sx];
     s_code[tid] = reinterpret_cast<const int4*>(stg + (size_t)(SROWS + 2) * BT * 16)[sx];
-    s_jinv[0 * BT + tid] = r0.x;
-    s_jinv[1 * BT + tid] = r0.y;
-    s_jinv[2 * BT + tid] = r1.x;
-    s_jinv[3 * BT + tid] = r1.y;
-    s_area2[tid] = 1.0 / (r0.x * r1.y - r0.y * r1.x);  // 2 * area
+    // edge normals N_k (length = edge length; N_k / area = 2(r0 + r1), -2 r0,
+    // -2 r1) from the FP64 J^-1 rows, kept in the working precision
+    const double det = r0.x * r1.y - r0.y * r1.x;  // 1 / (2 area)
+    const Real inv_area = (Real)(2.0 * det);
+    {
+        const double area2 = 1.0 / det;
+        const double cx[3] = {r0.x + r1.x, -r0.x, -r1.x}, cy[3] = {r0.y + r1.y, -r0.y, -r1.y};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const Real Nx = (Real)(cx[k] * area2), Ny = (Real)(cy[k] * area2);
+            s_nrm[(3 * k + 0) * BT + tid] = Nx;
+            s_nrm[(3 * k + 1) * BT + tid] = Ny;
+            s_nrm[(3 * k + 2) * BT + tid] = sqrt_(Nx * Nx + Ny * Ny);
+        }
+    }
     Real m_st[4];  // the stored cell mean (a deviation in FP32)
     {
         load_staged<Real, NB>(stg, sx, u);
@@ -274,8 +304,8 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
         for (int v = 0; v < 4; ++v) {
             m_st[v] = u[0][v];
             u[0][v] += ref_of<Real>(fs, v);  // stored deviation -> state (FP32)
-            s_mean[v * BT + tid] = u[0][v];
         }
+        put4(s_mean + tid, u[0]);
 #pragma unroll
         for (int i = 0; i < NB; ++i)
 #pragma unroll
@@ -307,14 +337,17 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
-            for (int g = 0; g < NG; ++g)
+            for (int g = 0; g < NG; ++g) {
+                Real t[4];
 #pragma unroll
                 for (int v = 0; v < 4; ++v) {
                     Real s = Real(0);
 #pragma unroll
                     for (int i = 0; i < NB; ++i) s += tb.ephi[k][g][i] * u[i][v];
-                    s_tr[((k * NG + g) * 4 + v) * BT + tid] = s;
+                    t[v] = s;
                 }
+                put4(s_tr + (k * NG + g) * BT + tid, t);
+            }
         if constexpr (HOLD) {
 #pragma unroll
             for (int v = 0; v < 4; ++v) u[0][v] = m_st[v];  // the stored values for the update
@@ -327,36 +360,37 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
         for (int r = 0; r < 3; ++r) {
             const int h = tid + r * BT;
             if (h < nh) {
-            Real un[NB][4];
-            if constexpr (sizeof(Real) == 8) {
-                const double2* p = reinterpret_cast<const double2*>(stg);
+                Real un[NB][4];
+                if constexpr (sizeof(Real) == 8) {
+                    const double2* p = reinterpret_cast<const double2*>(stg);
 #pragma unroll
-                for (int i = 0; i < NB; ++i) {
-                    const double2 x = p[(2 * i) * HM + h], y = p[(2 * i + 1) * HM + h];
-                    un[i][0] = x.x, un[i][1] = x.y, un[i][2] = y.x, un[i][3] = y.y;
+                    for (int i = 0; i < NB; ++i) {
+                        const double2 x = p[(2 * i) * HM + h], y = p[(2 * i + 1) * HM + h];
+                        un[i][0] = x.x, un[i][1] = x.y, un[i][2] = y.x, un[i][3] = y.y;
+                    }
+                } else {
+                    const float4* p = reinterpret_cast<const float4*>(stg);
+#pragma unroll
+                    for (int i = 0; i < NB; ++i) {
+                        const float4 x = p[i * HM + h];
+                        un[i][0] = x.x, un[i][1] = x.y, un[i][2] = x.z, un[i][3] = x.w;
+                    }
                 }
-            } else {
-                const float4* p = reinterpret_cast<const float4*>(stg);
 #pragma unroll
-                for (int i = 0; i < NB; ++i) {
-                    const float4 x = p[i * HM + h];
-                    un[i][0] = x.x, un[i][1] = x.y, un[i][2] = x.z, un[i][3] = x.w;
-                }
-            }
+                for (int v = 0; v < 4; ++v) un[0][v] += ref_of<Real>(fs, v);
+                put4(s_hmean + h, un[0]);
+                const int he = hh[r].y;
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                un[0][v] += ref_of<Real>(fs, v);
-                s_hmean[v * HM + h] = un[0][v];
-            }
-            const int he = hh[r].y;
+                for (int g = 0; g < NG; ++g) {
+                    Real t[4];
 #pragma unroll
-            for (int g = 0; g < NG; ++g)
+                    for (int v = 0; v < 4; ++v) {
+                        Real s = Real(0);
 #pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    Real s = Real(0);
-#pragma unroll
-                    for (int i = 0; i < NB; ++i) s += s_ephi[he][g][i] * un[i][v];
-                    s_htr[(g * 4 + v) * HM + h] = s;
+                        for (int i = 0; i < NB; ++i) s += s_ephi[he][g][i] * un[i][v];
+                        t[v] = s;
+                    }
+                    put4(s_htr + g * HM + h, t);
                 }
             }
         }
@@ -374,39 +408,15 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
             const int le = tkj >> 2, k = tkj & 3;
             const int c = reinterpret_cast<const int*>(s_code + le)[k];
             const int kind = c & 3, se = (c >> 2) & 3, idx = c >> 4;
-            // physical normal N = n * length of edge k of element le from the
-            // FP64 J^-1 and area (N_k / area = 2(r0 + r1), -2 r0, -2 r1);
-            // its length and direction in the working precision
-            const double a0 = s_jinv[0 * BT + le], a1 = s_jinv[1 * BT + le];
-            const double b0 = s_jinv[2 * BT + le], b1 = s_jinv[3 * BT + le];
-            const double area2 = s_area2[le];
-            double Nxd, Nyd;
-            if (k == 0) {
-                Nxd = (a0 + b0) * area2;
-                Nyd = (a1 + b1) * area2;
-            } else if (k == 1) {
-                Nxd = -a0 * area2;
-                Nyd = -a1 * area2;
-            } else {
-                Nxd = -b0 * area2;
-                Nyd = -b1 * area2;
-            }
-            const Real Nx = (Real)Nxd, Ny = (Real)Nyd;
-            const Real len = sqrt_(Nx * Nx + Ny * Ny);
+            // physical normal N (|N| = edge length) and unit normal of edge k
+            const Real Nx = s_nrm[(3 * k + 0) * BT + le], Ny = s_nrm[(3 * k + 1) * BT + le];
+            const Real len = s_nrm[(3 * k + 2) * BT + le];
             const Real il = rcp_(len);
             const Real nx = Nx * il, ny = Ny * il;
             Real mL[4], mR[4];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) mL[v] = s_mean[v * BT + le];
-            if (kind == EDGE_IN_OWNER) {
-#pragma unroll
-                for (int v = 0; v < 4; ++v) mR[v] = s_mean[v * BT + idx];
-            } else if (kind == EDGE_HALO) {
-#pragma unroll
-                for (int v = 0; v < 4; ++v) mR[v] = s_hmean[v * HM + idx];
-            } else {
-                ghost<Real>(se, mL, far, nx, ny, mR);
-            }
+            get4(s_mean + le, mL);
+            if (kind == EDGE_BOUNDARY) ghost<Real>(se, mL, far, nx, ny, mR);
+            else get4(kind == EDGE_HALO ? s_hmean + idx : s_mean + idx, mR);
             Real alpha = Real(0);
             if (FLUX == RKDG_FLUX_LLF) {
                 // LLF coefficient from the average of the two cell means
@@ -422,20 +432,13 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 #pragma unroll
             for (int g = 0; g < NG; ++g) {
                 Real uL[4], uR[4];
-                Real* slot = s_tr + (k * NG + g) * 4 * BT + le;
-#pragma unroll
-                for (int v = 0; v < 4; ++v) uL[v] = slot[v * BT];
+                V4* slot = s_tr + (k * NG + g) * BT + le;
+                get4(slot, uL);
                 // the neighbour's point NG-1-g on its edge se pairs with ours
                 // (src/kernelfunctions.cu:545-549)
-                if (kind == EDGE_IN_OWNER) {
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) uR[v] = s_tr[((se * NG + NG - 1 - g) * 4 + v) * BT + idx];
-                } else if (kind == EDGE_HALO) {
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) uR[v] = s_htr[((NG - 1 - g) * 4 + v) * HM + idx];
-                } else {
-                    ghost<Real>(se, uL, far, nx, ny, uR);
-                }
+                if (kind == EDGE_BOUNDARY) ghost<Real>(se, uL, far, nx, ny, uR);
+                else get4(kind == EDGE_HALO ? s_htr + (NG - 1 - g) * HM + idx
+                                            : s_tr + (se * NG + NG - 1 - g) * BT + idx, uR);
                 Real fh[4];
                 if (FLUX == RKDG_FLUX_LLF) {
                     Real fL[4], fR[4], pL, pR;
@@ -448,8 +451,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 #pragma unroll
                     for (int v = 0; v < 4; ++v) fh[v] *= len;
                 }
-#pragma unroll
-                for (int v = 0; v < 4; ++v) slot[v * BT] = fh[v];
+                put4(slot, fh);
             }
         }
     }
@@ -457,22 +459,16 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 
     // ------------------------------------------------------------ phase C
     const int4 cd = s_code[tid];
-    const Real inv_area = (Real)(2.0 / s_area2[tid]);  // 1 / area
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const int c = k == 0 ? cd.x : (k == 1 ? cd.y : cd.z);
         const int kind = c & 3, se = (c >> 2) & 3, idx = c >> 4;
+        const bool other = kind == EDGE_IN_OTHER;
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
             Real f[4];
-            if (kind == EDGE_IN_OTHER) {
-#pragma unroll
-                for (int v = 0; v < 4; ++v) f[v] = -s_tr[((se * NG + NG - 1 - g) * 4 + v) * BT + idx];
-            } else {
-#pragma unroll
-                for (int v = 0; v < 4; ++v) f[v] = s_tr[((k * NG + g) * 4 + v) * BT + tid];
-            }
-            const Real wg = tb.ew[g] * inv_area;
+            get4(other ? s_tr + (se * NG + NG - 1 - g) * BT + idx : s_tr + (k * NG + g) * BT + tid, f);
+            const Real wg = other ? -(tb.ew[g] * inv_area) : tb.ew[g] * inv_area;
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
                 Real cw = wg * f[v];
@@ -513,10 +509,12 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
         double wv = 0.0, m0 = 0.0, m1 = 0.0;
         if (active) {
             bool bad;
-            wv = wave_measure((double)R[0][0] + (double)ref_of<Real>(fs, 0),
-                              (double)R[0][1] + (double)ref_of<Real>(fs, 1),
-                              (double)R[0][2] + (double)ref_of<Real>(fs, 2),
-                              (double)R[0][3] + (double)ref_of<Real>(fs, 3), a.gamma, r0, r1, bad);
+            Real m[4], len[3];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) m[v] = R[0][v] + ref_of<Real>(fs, v);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) len[k] = s_nrm[(3 * k + 2) * BT + tid];
+            wv = wave_of<Real>(m, gamma, len, inv_area, bad);
             if (bad) atomicOr(&ctl->error, 1);
             m0 = fabs((double)R[0][0] - (double)u0m[0]);
             m1 = fabs((double)R[0][3] - (double)u0m[3]);
