@@ -252,11 +252,23 @@ def event_time(stream_ptr, fn, dist):
     return dist.max(e0.elapsed_time(e1))
 
 
-def roofline(t0, t1, alg_bytes, peak, peak_kind, kernel):
+def measured_traffic(profile):
+    """DRAM bytes per launch (mean over an SSP-RK3 step) that an ncu capture
+    of the same workload recorded in profiles/<profile> (None if absent)."""
+    p = os.path.join(ROOT, "profiles", profile)
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch_mean:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def roofline(t0, t1, alg_bytes, peak, peak_kind, kernel, traffic=None):
     t_avg = (t0 + 2 * t1) / 3.0  # SSP-RK3: one stage without U^n, two with
     achieved = alg_bytes / (t_avg * 1e-3) / 1e9
     return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "traffic": None, "kernel": kernel,
+            "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": kernel,
             "peak_kind": peak_kind,
             "ms_per_launch": {"stage_without_U0": round(t0, 5), "stage_with_U0": round(t1, 5)},
             "algorithmic_bytes_per_launch": alg_bytes}
@@ -303,7 +315,9 @@ def run_batched(args, dist, peak, peak_kind):
         value = dist.sum(dofs * 3 * K) / (ms * 1e-3)
         alg = sum(m.ntri * bytes_per_elem_stage(nb, word) for m, nb in zip(meshes, nbs))
         roof = roofline(b.time_stage(0, 10), b.time_stage(1, 10), alg, peak, peak_kind,
-                        "tiled_stage_kernel (P1+P2 tiles, one launch per stage)")
+                        "tiled_stage_kernel (P1+P2 tiles, one launch per stage)",
+                        measured_traffic("tiled_stage_kernel_batched_fp32.md")
+                        if prec == "fp32" and args.nsolves == 64 else None)
         e2e = None
         if not args.no_e2e:
             hosts = [pinned_like(U) for U in states]
