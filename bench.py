@@ -56,7 +56,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "vortex", "serving"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "vortex", "serving", "step"])
+    ap.add_argument("--no-step", action="store_true", help="skip the Mach-3 step FP32/FP64 comparison")
+    ap.add_argument("--step-h", type=int, default=400, help="1/h of the Mach-3 step lattice")
+    ap.add_argument("--step-sensitivity", action="store_true",
+                    help="also run FP64 from an initial state perturbed at FP32 rounding level")
     ap.add_argument("--nsolves", type=int, default=64)
     ap.add_argument("--lattice", type=int, default=700)
     ap.add_argument("--plain-steps", type=int, default=50)
@@ -416,6 +420,61 @@ def run_plain(args, dist, peak, peak_kind, K):
     return out, T
 
 
+# ------------------------------------------------------ Mach-3 step (C3) --
+def run_step(args, dist):
+    """Mach-3 wind-tunnel step: jittered Delaunay mesh, h = 1/400 (seed 3),
+    P1, LLF, TVB limiter M = 50 on characteristic variables, SSP-RK3, CFL 0.3,
+    uniform inflow (1.4, 3, 0, 1) to t = 0.5; FP32 (FP64 geometry and dt)
+    against FP64.  Reports the relative L1 difference of the cell-mean
+    density, sum_e A_e |rho32 - rho64| / sum_e A_e |rho64|, at t = 0.05 and
+    t = 0.5, and each precision's DOF-stage/s over the run (CUDA events)."""
+    from rkdg_heter_calculate_b200 import CUDARkdgSolver, meshgen
+
+    m = meshgen.forward_step(h=1.0 / args.step_h, seed=3)
+    far = np.array(conservative(1.4, 3.0, 0.0, 1.0))
+    U = np.zeros((4, 3, m.ntri))
+    U[:, 0, :] = far[:, None]
+    a = m.areas()
+    kw = dict(order=1, nq=3, ng=2, flux="llf", rk=3, limiter="tvb", tvb_m=50.0, cfl=0.3, farfield=far)
+    runs = [("fp64", U), ("fp32", U)]
+    if args.step_sensitivity:
+        rng = np.random.default_rng(7)
+        Up = U.copy()
+        Up[:, 0, :] *= 1.0 + 6e-8 * rng.uniform(-1.0, 1.0, (4, m.ntri))
+        runs.append(("fp64_perturbed", Up))
+    res = {}
+    for name, U0 in runs:
+        s = CUDARkdgSolver(m, precision="fp32" if name == "fp32" else "fp64", **kw)
+        s.setFreedom(U0, basis="native")
+        out = {}
+        steps = 0
+        ms = 0.0
+        for tt in (0.05, 0.5):
+            box = {}
+            ms += event_time(s.stream(), lambda: box.update(r=s.advance(10 ** 8, t_final=tt)), dist)
+            steps += box["r"][1]
+            out[tt] = s.copyFreedomToHost(basis="native")[0, 0]
+        s.close()
+        res[name] = {"rho": out, "steps": steps, "ms": ms}
+
+    def rel(x, y):
+        return float(np.sum(a * np.abs(x - y)) / np.sum(a * np.abs(y)))
+
+    line = {"workload": "Mach-3 step, jittered Delaunay h = 1/%d (seed 3), %d triangles, P1, LLF, TVB M = 50, "
+                        "SSP-RK3, CFL 0.3, to t = 0.5" % (args.step_h, m.ntri),
+            "triangles": int(m.ntri),
+            "rel_L1_rho_fp32_vs_fp64": {str(t): rel(res["fp32"]["rho"][t], res["fp64"]["rho"][t]) for t in (0.05, 0.5)},
+            "definition": "sum_e A_e |rho32 - rho64| / sum_e A_e |rho64| over cell means"}
+    for name in res:
+        r = res[name]
+        line[name] = {"steps": r["steps"], "ms": round(r["ms"], 1),
+                      "dof_stage_per_s": dist.sum(r["steps"] * 3 * 12 * m.ntri / (r["ms"] * 1e-3))}
+    if "fp64_perturbed" in res:
+        line["rel_L1_rho_fp64_perturbed_vs_fp64"] = {
+            str(t): rel(res["fp64_perturbed"]["rho"][t], res["fp64"]["rho"][t]) for t in (0.05, 0.5)}
+    return line
+
+
 # ------------------------------------------------------------ serving (C5) --
 SERVE_LEVELS = 8   # mesh sizes per request kind, log-spaced over [2k, 500k] triangles
 
@@ -547,6 +606,16 @@ def run_serving(args, dist):
 
 
 # --------------------------------------------------------- CPU baselines --
+def host_cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip() + f" ({os.cpu_count()} logical CPUs)"
+    except OSError:
+        pass
+    return f"{os.cpu_count()} logical CPUs"
+
+
 def cpu_reference_sample(seconds: float, threads: int | None = None):
     """The reference's own code (oracle/_ref) when built, else the oracle
     port, on a 20,000-triangle periodic Delaunay vortex mesh; returns
@@ -633,9 +702,13 @@ def main():
         head = "fp32" if "fp32" in res else "fp64"
         r = res[head]
         serving = None if args.no_serving else run_serving(args, dist)
+        step = None if (args.no_step or args.no_accuracy) else run_step(args, dist)
         cpu = None
         if dist.rank == 0 and not args.no_cpu:
             _, cpu = cpu_reference_sample(args.cpu_seconds)
+            v1, d1 = cpu_reference_sample(args.cpu_seconds / 3.0, threads=1)
+            cpu["single_core"] = {"value": v1, "sample": d1["sample"]}
+            cpu["host_cpu"] = host_cpu_model()
         if dist.rank == 0:
             l2 = None
             if r.get("l2") is not None and "fp64" in res and res["fp64"].get("l2") is not None:
@@ -672,8 +745,12 @@ def main():
                 "plain": ({p: {k: v for k, v in plain[p].items() if k != "l2"} for p in plain}
                           if plain else None),
                 "cpu_baseline": cpu, "clocks": r["clocks"], "gpu_launches": 4 * args.steps,
-                "l2": l2, "serving": serving,
+                "l2": l2, "serving": serving, "step_fp32_vs_fp64": step,
             }
+    elif args.workload == "step":
+        step = run_step(args, dist)
+        if dist.rank == 0:
+            print(json.dumps({"workload": "step", "n_gpus": dist.world, "step_fp32_vs_fp64": step}), flush=True)
     elif args.workload == "serving":
         serving = run_serving(args, dist)
         if dist.rank == 0:
