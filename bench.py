@@ -80,25 +80,30 @@ def parse():
 
 # ------------------------------------------------------------ distributed --
 class Dist:
-    def __init__(self):
+    """One process per GPU (torchrun env vars); NCCL on GPUs, gloo when the
+    process has no GPU (the CPU tests of the multi-rank path)."""
+
+    def __init__(self, backend: str | None = None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
         self.pg = False
 
     def init(self):
         import torch
 
+        if self.backend is None:
+            self.backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if self.backend == "nccl":
+            torch.cuda.set_device(self.local if self.world > 1 else 0)
         if self.world > 1:
             import datetime
 
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            dist.init_process_group(self.backend, timeout=datetime.timedelta(seconds=600))
             self.pg = True
-        else:
-            torch.cuda.set_device(0)
 
     def barrier(self):
         if self.pg:
@@ -112,7 +117,7 @@ class Dist:
         import torch
         import torch.distributed as dist
 
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device="cuda" if self.backend == "nccl" else "cpu")
         dist.all_reduce(t, op=op)
         return float(t.item())
 
