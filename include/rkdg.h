@@ -205,6 +205,20 @@ int rkdg_conservation_totals_noalloc(int32_t ntri, const double* d_means, int32_
  * (CCUDARkdgSolver::outputSolution, src/cudarkdgsolver.cu:860-1001). */
 int rkdg_write_solution(rkdg_ctx* ctx, const char* path);
 
+/* ---- checkpoint / resume ----------------------------------------------- */
+/* No reference counterpart (the reference writes no restart files).
+ * rkdg_checkpoint_save writes the context's full state to path: a header
+ * (format tag, triangle count, order, precision, a hash of the mesh in its
+ * internal order, time, step count, the CFL wave maximum and monitor, the
+ * far-field state) followed by the state rows exactly as held on the device.
+ * A run restored from it continues bit for bit as if never stopped.
+ * rkdg_checkpoint_load restores such a file into a context built on the
+ * same mesh, order and precision (RKDG_ERR_INVALID otherwise; an FP32 file
+ * also needs the same far-field state, its cell means being stored relative
+ * to it); RKDG_ERR_IO when the file cannot be read or written. */
+int rkdg_checkpoint_save(rkdg_ctx* ctx, const char* path);
+int rkdg_checkpoint_load(rkdg_ctx* ctx, const char* path);
+
 /* ---- batched independent solves ----------------------------------------- */
 /* Many independent solves on meshes of uneven size and mixed order (P1
  * and P2) packed into one element space: every RK stage of all solves is

@@ -108,6 +108,8 @@ def lib():
             "rkdg_server_stats": (C.c_int, [vp, _dp, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_int32),
                                             C.POINTER(C.c_int64)]),
             "rkdg_server_clock": (C.c_double, []),
+            "rkdg_checkpoint_save": (C.c_int, [vp, C.c_char_p]),
+            "rkdg_checkpoint_load": (C.c_int, [vp, C.c_char_p]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

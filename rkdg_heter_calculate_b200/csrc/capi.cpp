@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -733,3 +734,109 @@ int rkdg_write_solution(rkdg_ctx* c, const char* path) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------ checkpoint / resume
+namespace {
+
+struct CheckpointHeader {
+    char magic[8];
+    uint32_t version;
+    int32_t ntri, order, nbasis, precision, packs;
+    uint64_t mesh_hash;
+    double t;
+    int32_t step, pad;
+    unsigned long long wave_bits, mon_bits[2];
+    double farfield[4];
+};
+constexpr char kCkptMagic[8] = {'R', 'K', 'D', 'G', 'C', 'K', 'P', '1'};
+
+// FNV-1a over the internal-order vertex coordinates of every triangle: the
+// same caller mesh and ordering setting give the same value.
+uint64_t mesh_hash(const HostMesh& m) {
+    uint64_t h = 1469598103934665603ull;
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(m.xy.data());
+    for (size_t i = 0; i < m.xy.size() * sizeof(double); ++i) h = (h ^ b[i]) * 1099511628211ull;
+    return h;
+}
+
+// 16-byte packs per element in the state layout
+int state_packs(const rkdg_ctx* c) { return c->nb * (c->p.precision == RKDG_FP32 ? 1 : 2); }
+
+}  // namespace
+
+int rkdg_checkpoint_save(rkdg_ctx* c, const char* path) {
+    return guarded([&] {
+        if (!c || !path) throw Error{RKDG_ERR_INVALID, "rkdg_checkpoint_save: bad arguments"};
+        require_state(c);
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        ensure_wave(c);
+        pull_ctl(c);
+        const int packs = state_packs(c);
+        std::vector<unsigned char> rows((size_t)packs * c->T * 16);
+        RKDG_CUDA_TRY(cudaMemcpy2DAsync(rows.data(), (size_t)c->T * 16, c->d.U[c->cur], (size_t)c->ld * 16,
+                                        (size_t)c->T * 16, packs, cudaMemcpyDeviceToHost, c->stream));
+        sync(c);
+        CheckpointHeader h{};
+        std::memcpy(h.magic, kCkptMagic, 8);
+        h.version = 1;
+        h.ntri = c->T;
+        h.order = c->p.order;
+        h.nbasis = c->nb;
+        h.precision = c->p.precision;
+        h.packs = packs;
+        h.mesh_hash = mesh_hash(c->mesh);
+        h.t = c->h_ctl->t;
+        h.step = c->h_ctl->step;
+        h.wave_bits = c->h_ctl->wave_bits;
+        h.mon_bits[0] = c->h_ctl->mon_bits[0];
+        h.mon_bits[1] = c->h_ctl->mon_bits[1];
+        for (int v = 0; v < 4; ++v) h.farfield[v] = c->p.farfield[v];
+        std::ofstream f(path, std::ios::binary);
+        if (!f) throw Error{RKDG_ERR_IO, std::string("cannot open ") + path + " for writing"};
+        f.write(reinterpret_cast<const char*>(&h), sizeof(h));
+        f.write(reinterpret_cast<const char*>(rows.data()), (std::streamsize)rows.size());
+        if (!f) throw Error{RKDG_ERR_IO, std::string("write to ") + path + " failed"};
+    });
+}
+
+int rkdg_checkpoint_load(rkdg_ctx* c, const char* path) {
+    return guarded([&] {
+        if (!c || !path) throw Error{RKDG_ERR_INVALID, "rkdg_checkpoint_load: bad arguments"};
+        std::ifstream f(path, std::ios::binary);
+        if (!f) throw Error{RKDG_ERR_IO, std::string("cannot open ") + path};
+        CheckpointHeader h{};
+        f.read(reinterpret_cast<char*>(&h), sizeof(h));
+        if (!f) throw Error{RKDG_ERR_IO, std::string("short read from ") + path};
+        if (std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != 1)
+            throw Error{RKDG_ERR_INVALID, std::string(path) + " is not a checkpoint of this format"};
+        const int packs = state_packs(c);
+        if (h.ntri != c->T || h.order != c->p.order || h.precision != c->p.precision || h.packs != packs)
+            throw Error{RKDG_ERR_INVALID, "checkpoint was written for another triangle count, order or precision"};
+        if (h.mesh_hash != mesh_hash(c->mesh))
+            throw Error{RKDG_ERR_INVALID, "checkpoint was written for another mesh (or triangle ordering)"};
+        if (c->p.precision == RKDG_FP32)
+            for (int v = 0; v < 4; ++v)
+                if (h.farfield[v] != c->p.farfield[v])
+                    throw Error{RKDG_ERR_INVALID, "FP32 checkpoint was written with another far-field state"};
+        std::vector<unsigned char> rows((size_t)packs * c->T * 16);
+        f.read(reinterpret_cast<char*>(rows.data()), (std::streamsize)rows.size());
+        if (!f) throw Error{RKDG_ERR_IO, std::string("short read from ") + path};
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        RKDG_CUDA_TRY(cudaMemcpy2DAsync(c->d.U[0], (size_t)c->ld * 16, rows.data(), (size_t)c->T * 16,
+                                        (size_t)c->T * 16, packs, cudaMemcpyHostToDevice, c->stream));
+        c->cur = 0;
+        c->old = 0;
+        pull_ctl(c);
+        c->h_ctl->t = h.t;
+        c->h_ctl->step = h.step;
+        c->h_ctl->wave_bits = h.wave_bits;
+        c->h_ctl->mon_bits[0] = h.mon_bits[0];
+        c->h_ctl->mon_bits[1] = h.mon_bits[1];
+        c->h_ctl->done = 0;
+        c->h_ctl->error = 0;
+        push_ctl(c);
+        sync(c);
+        c->wave_valid = true;
+        c->have_state = true;
+    });
+}

@@ -23,6 +23,7 @@ Errors raise ``capi.RkdgError`` (the reference threw CMyException).
 from __future__ import annotations
 
 import ctypes as C
+import os
 import math
 
 import numpy as np
@@ -183,6 +184,14 @@ class CUDARkdgSolver:
         out = np.zeros(4)
         capi.check(capi.lib().rkdg_conservation_totals(self.h, capi.dptr(out)))
         return out
+
+    def checkpoint(self, path: str):
+        """Writes the full state, time and step count (bitwise restart)."""
+        capi.check(capi.lib().rkdg_checkpoint_save(self.h, os.fsencode(path)))
+
+    def restore(self, path: str):
+        """Restores a checkpoint written on the same mesh, order and precision."""
+        capi.check(capi.lib().rkdg_checkpoint_load(self.h, os.fsencode(path)))
 
     def outputSolution(self, path: str):
         capi.check(capi.lib().rkdg_write_solution(self.h, path.encode()))
