@@ -180,7 +180,7 @@ struct StageArgs {
     const double* jinv;
     const int4* conn;
     StepCtl* ctl;
-    double a, b;         // Unew = a U0 + b (U + dt L(U))
+    double a, b;         // Unew = a U0 + b (U + dt L(U)), formed as U0 + b ((U - U0) + dt L); a = 1 - b
     double gamma;
     double far[4];
     const double* far_sid;  // per-solve far-field states [solves][4], or nullptr

@@ -244,6 +244,9 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
         fs[0] = a.far[0], fs[1] = a.far[1], fs[2] = a.far[2], fs[3] = a.far[3];
     }
     const Real far[4] = {(Real)fs[0], (Real)fs[1], (Real)fs[2], (Real)fs[3]};
+    // FP32: traces and fluxes in deviation form about the reference state
+    constexpr bool DEV = stores_deviation<Real>();
+    const RefState<Real> rs = ref_state<Real>(fs, a.gamma);
 
     // ------------------------------------------------------------ phase A
     // the halo and task lists first (L2 hits: prefetched with the tile's
@@ -300,12 +303,16 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                 if (j < nt) s_task[j] = tk[r];
             }
         }
+        {
+            Real mfull[4];
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            m_st[v] = u[0][v];
-            u[0][v] += ref_of<Real>(fs, v);  // stored deviation -> state (FP32)
+            for (int v = 0; v < 4; ++v) {
+                m_st[v] = u[0][v];
+                mfull[v] = u[0][v] + ref_of<Real>(fs, v);  // the cell mean itself
+                if constexpr (!DEV) u[0][v] = mfull[v];
+            }
+            put4(s_mean + tid, mfull);
         }
-        put4(s_mean + tid, u[0]);
 #pragma unroll
         for (int i = 0; i < NB; ++i)
 #pragma unroll
@@ -321,17 +328,29 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                 for (int i = 0; i < NB; ++i) s += tb.vphi[q][i] * u[i][v];
                 w[v] = s;
             }
-            Real ri = rcp_(w[0]);
-            Real vx = w[1] * ri, vy = w[2] * ri;
-            Real p = gm1 * (w[3] - Real(0.5) * (w[1] * vx + w[2] * vy));
-            Real F[4] = {w[1], w[1] * vx + p, w[2] * vx, (w[3] + p) * vx};
-            Real G[4] = {w[2], w[1] * vy, w[2] * vy + p, (w[3] + p) * vy};
+            if constexpr (DEV) {
+                // flux deviations through the rows of J^-1: (j00 F + j01 G) - ref
+                const DevPrims<Real> pw = dev_prims(w, rs, gm1);
+                Real fx[4], fy[4];
+                dev_flux(w, pw, rs, j00, j01, fx);
+                dev_flux(w, pw, rs, j10, j11, fy);
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                Real fx = j00 * F[v] + j01 * G[v];
-                Real fy = j10 * F[v] + j11 * G[v];
+                for (int v = 0; v < 4; ++v)
 #pragma unroll
-                for (int i = 1; i < NB; ++i) R[i][v] += fx * tb.vdxi[q][i] + fy * tb.veta[q][i];
+                    for (int i = 1; i < NB; ++i) R[i][v] += fx[v] * tb.vdxi[q][i] + fy[v] * tb.veta[q][i];
+            } else {
+                Real ri = rcp_(w[0]);
+                Real vx = w[1] * ri, vy = w[2] * ri;
+                Real p = gm1 * (w[3] - Real(0.5) * (w[1] * vx + w[2] * vy));
+                Real F[4] = {w[1], w[1] * vx + p, w[2] * vx, (w[3] + p) * vx};
+                Real G[4] = {w[2], w[1] * vy, w[2] * vy + p, (w[3] + p) * vy};
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    Real fx = j00 * F[v] + j01 * G[v];
+                    Real fy = j10 * F[v] + j11 * G[v];
+#pragma unroll
+                    for (int i = 1; i < NB; ++i) R[i][v] += fx * tb.vdxi[q][i] + fy * tb.veta[q][i];
+                }
             }
         }
 #pragma unroll
@@ -348,7 +367,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                 }
                 put4(s_tr + (k * NG + g) * BT + tid, t);
             }
-        if constexpr (HOLD) {
+        if constexpr (HOLD && !DEV) {
 #pragma unroll
             for (int v = 0; v < 4; ++v) u[0][v] = m_st[v];  // the stored values for the update
         }
@@ -376,9 +395,15 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                         un[i][0] = x.x, un[i][1] = x.y, un[i][2] = x.z, un[i][3] = x.w;
                     }
                 }
+                {
+                    Real mfull[4];
 #pragma unroll
-                for (int v = 0; v < 4; ++v) un[0][v] += ref_of<Real>(fs, v);
-                put4(s_hmean + h, un[0]);
+                    for (int v = 0; v < 4; ++v) {
+                        mfull[v] = un[0][v] + ref_of<Real>(fs, v);
+                        if constexpr (!DEV) un[0][v] = mfull[v];
+                    }
+                    put4(s_hmean + h, mfull);
+                }
                 const int he = hh[r].y;
 #pragma unroll
                 for (int g = 0; g < NG; ++g) {
@@ -436,18 +461,28 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                 get4(slot, uL);
                 // the neighbour's point NG-1-g on its edge se pairs with ours
                 // (src/kernelfunctions.cu:545-549)
-                if (kind == EDGE_BOUNDARY) ghost<Real>(se, uL, far, nx, ny, uR);
+                if (kind == EDGE_BOUNDARY) {
+                    if constexpr (DEV) ghost_dev<Real>(se, uL, rs, nx, ny, uR);
+                    else ghost<Real>(se, uL, far, nx, ny, uR);
+                }
                 else get4(kind == EDGE_HALO ? s_htr + (NG - 1 - g) * HM + idx
                                             : s_tr + (se * NG + NG - 1 - g) * BT + idx, uR);
                 Real fh[4];
                 if (FLUX == RKDG_FLUX_LLF) {
-                    Real fL[4], fR[4], pL, pR;
-                    normal_flux<Real>(uL, Nx, Ny, gm1, fL, pL);
-                    normal_flux<Real>(uR, Nx, Ny, gm1, fR, pR);
+                    Real fL[4], fR[4];
+                    if constexpr (DEV) {
+                        dev_flux(uL, dev_prims(uL, rs, gm1), rs, Nx, Ny, fL);
+                        dev_flux(uR, dev_prims(uR, rs, gm1), rs, Nx, Ny, fR);
+                    } else {
+                        Real pL, pR;
+                        normal_flux<Real>(uL, Nx, Ny, gm1, fL, pL);
+                        normal_flux<Real>(uR, Nx, Ny, gm1, fR, pR);
+                    }
 #pragma unroll
                     for (int v = 0; v < 4; ++v) fh[v] = Real(0.5) * (fL[v] + fR[v] - alpha * (uR[v] - uL[v]));
                 } else {
-                    hllc<Real>(uL, uR, nx, ny, gamma, fh);
+                    if constexpr (DEV) hllc_dev<Real>(uL, uR, nx, ny, gamma, rs, fh);
+                    else hllc<Real>(uL, uR, nx, ny, gamma, fh);
 #pragma unroll
                     for (int v = 0; v < 4; ++v) fh[v] *= len;
                 }
@@ -484,7 +519,10 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
         return;
     }
     const double dtd = ctl->dt;
-    const Real dt = (Real)dtd, ca = (Real)a.a, cb = (Real)a.b;
+    // a U^n + b (U + dt L) as U^n + b ((U - U^n) + dt L): a + b = 1 holds
+    // exactly (1/3 and 2/3 both round up in FP32, and a scale of 1 + 3e-8
+    // per step would accumulate into the state)
+    const Real dt = (Real)dtd, cb = (Real)a.b;
     Real u0m[4] = {Real(0), Real(0), Real(0), Real(0)};
     {
         if constexpr (!HOLD) load_state<Real, NB>(U, a.ld, ee, u);  // stored values (L2 hit)
@@ -494,7 +532,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 #pragma unroll
             for (int i = 0; i < NB; ++i)
 #pragma unroll
-                for (int v = 0; v < 4; ++v) R[i][v] = ca * u0[i][v] + cb * (u[i][v] + dt * R[i][v]);
+                for (int v = 0; v < 4; ++v) R[i][v] = u0[i][v] + cb * ((u[i][v] - u0[i][v]) + dt * R[i][v]);
 #pragma unroll
             for (int v = 0; v < 4; ++v) u0m[v] = u0[0][v];
         } else {
