@@ -204,6 +204,14 @@ int rkdg_conservation_totals_noalloc(int32_t ntri, const double* d_means, int32_
 /* Writes the cell means as the reference's Tecplot solution.plt
  * (CCUDARkdgSolver::outputSolution, src/cudarkdgsolver.cu:860-1001). */
 int rkdg_write_solution(rkdg_ctx* ctx, const char* path);
+/* Residual history, as the reference's residual file (RkdgAdvance::advance,
+ * src/rkdgadvance.cpp:10-17,201-211): the file starts with the line
+ * "N, rho" and then takes one line per step taken by rkdg_step or
+ * rkdg_advance, "<step>   <log10(max |change of a cell-mean density| /
+ * far-field density)>" (the reference labels step k's value k+1 and omits
+ * the last step).  While a history file is open, rkdg_advance launches one
+ * step at a time.  NULL closes it. */
+int rkdg_set_residual_log(rkdg_ctx* ctx, const char* path);
 
 /* ---- checkpoint / resume ----------------------------------------------- */
 /* No reference counterpart (the reference writes no restart files).

@@ -110,6 +110,7 @@ def lib():
             "rkdg_server_clock": (C.c_double, []),
             "rkdg_checkpoint_save": (C.c_int, [vp, C.c_char_p]),
             "rkdg_checkpoint_load": (C.c_int, [vp, C.c_char_p]),
+            "rkdg_set_residual_log": (C.c_int, [vp, C.c_char_p]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

@@ -45,6 +45,7 @@ struct rkdg_ctx {
     TileArgs tiles{};
     int variant = 1;  // 1 tile-staged (default), 0 owner-computes
     int ctas = 0;     // tiled grid size (0: one CTA per tile)
+    std::unique_ptr<std::ofstream> reslog;  // residual history file (rkdg_set_residual_log)
 };
 
 namespace {
@@ -204,6 +205,16 @@ void enqueue_step(rkdg_ctx* c) {
 
 void check_error_flag(rkdg_ctx* c) {
     throw_ctl_error(c->h_ctl->error, "solve");
+}
+
+// One line of the residual history for the step just taken (the control
+// block on the host is current): the step number and log10 of the largest
+// cell-mean density change over the step relative to the far-field density.
+void log_residual(rkdg_ctx* c) {
+    if (!c->reslog) return;
+    double m0;
+    std::memcpy(&m0, &c->h_ctl->mon_bits[0], sizeof(double));
+    *c->reslog << c->h_ctl->step << "   " << std::log10(m0 / c->p.farfield[0]) << "\n";
 }
 
 void destroy_ctx(rkdg_ctx* c) {
@@ -543,6 +554,7 @@ int rkdg_step(rkdg_ctx* c, double dt, double* dt_used, double* monitor) {
         c->wave_valid = true;
         pull_ctl(c);
         check_error_flag(c);
+        log_residual(c);
         if (dt_used) *dt_used = c->h_ctl->dt;
         if (monitor) {
             std::memcpy(&monitor[0], &c->h_ctl->mon_bits[0], sizeof(double));
@@ -576,6 +588,17 @@ int rkdg_advance(rkdg_ctx* c, int32_t nsteps, double t_final, double* t, int32_t
             RKDG_CUDA_TRY(cudaStreamEndCapture(c->stream, &g));
             RKDG_CUDA_TRY(cudaGraphInstantiate(&c->graph, g, 0));
             cudaGraphDestroy(g);
+        }
+        if (c->reslog) {  // the history needs every step's monitor: one step per launch
+            for (int i = 0; i < nsteps; ++i) {
+                const int before = c->h_ctl->step;
+                RKDG_CUDA_TRY(cudaGraphLaunch(c->graph, c->stream));
+                pull_ctl(c);
+                if (c->h_ctl->step == before || c->h_ctl->error) break;  // done or failed
+                log_residual(c);
+            }
+            c->reslog->flush();
+            nsteps = 0;
         }
         // launch in chunks; with a final time, stop once the device says done
         int left = nsteps;
@@ -838,5 +861,18 @@ int rkdg_checkpoint_load(rkdg_ctx* c, const char* path) {
         sync(c);
         c->wave_valid = true;
         c->have_state = true;
+    });
+}
+
+int rkdg_set_residual_log(rkdg_ctx* c, const char* path) {
+    return guarded([&] {
+        if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        c->reslog.reset();
+        if (!path) return;
+        auto f = std::make_unique<std::ofstream>(path);
+        if (!*f) throw Error{RKDG_ERR_IO, std::string("cannot open ") + path};
+        *f << "N, rho" << std::endl;  // src/rkdgadvance.cpp:10-17
+        f->precision(10);
+        c->reslog = std::move(f);
     });
 }

@@ -185,6 +185,10 @@ class CUDARkdgSolver:
         capi.check(capi.lib().rkdg_conservation_totals(self.h, capi.dptr(out)))
         return out
 
+    def setResidualLog(self, path):
+        """Residual history file as the reference writes it (None closes it)."""
+        capi.check(capi.lib().rkdg_set_residual_log(self.h, None if path is None else os.fsencode(path)))
+
     def checkpoint(self, path: str):
         """Writes the full state, time and step count (bitwise restart)."""
         capi.check(capi.lib().rkdg_checkpoint_save(self.h, os.fsencode(path)))

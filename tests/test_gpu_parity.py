@@ -243,6 +243,33 @@ def test_nonphysical_state_is_reported():
         s.advance(3)
 
 
+def test_residual_history_file(tmp_path):
+    """The reference's residual history: header "N, rho", then one line per
+    step with log10 of the largest cell-mean density change over the step
+    (relative to the far-field density), through rkdg_step and rkdg_advance."""
+    import math
+
+    mesh = meshgen.periodic_delaunay(10, seed=3)
+    far = primitive_to_conservative(1.2, 1.0, 1.0, 1.0)
+    o = oracle.Oracle(mesh, order=2, nq=6, ng=3, flux=oracle.HLLC, rk=3, farfield=far, cfl=0.2)
+    s = CUDARkdgSolver(mesh, order=2, nq=6, ng=3, flux="hllc", farfield=far, cfl=0.2)
+    s.setFreedom(vortex_state(mesh, o.basis()["coeff"], 6))
+    path = tmp_path / "residual.dat"
+    s.setResidualLog(str(path))
+    mons = [s.step()[1][0] for _ in range(2)]
+    t, n = s.advance(5)
+    s.setResidualLog(None)
+    s.step()  # not logged
+    lines = path.read_text().splitlines()
+    assert lines[0] == "N, rho"
+    assert len(lines) == 1 + 2 + 5
+    steps = [int(x.split()[0]) for x in lines[1:]]
+    assert steps == list(range(1, 8))
+    for line, m in zip(lines[1:3], mons):
+        assert float(line.split()[1]) == pytest.approx(math.log10(m / far[0]), rel=1e-9)
+    assert all(math.isfinite(float(x.split()[1])) for x in lines[1:])
+
+
 def test_solution_file_format(tmp_path):
     z, mesh = load_fixture("box_obstacle_12")
     s = gpu_from_fixture(z, mesh)
