@@ -1006,7 +1006,7 @@ namespace {
 // dynamic shared memory per CTA.
 template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
 size_t prepare_tiled(int max_halo) {
-    const size_t smem = TiledSmem<Real, ORD>::bytes(max_halo);
+    const size_t smem = TiledSmem<Real, ORD, FLUX>::bytes(max_halo);
     // dynamic + static shared memory above 48 KB needs the opt-in.  Per
     // instantiation; raised when a context with a larger halo appears.
     static size_t configured = 0;

@@ -22,13 +22,13 @@
 // its own solve's data: results are deterministic and identical whether a
 // solve runs alone or in a batch.
 //
-// Staging pipeline: a tile's own state rows, J^-1 rows and edge codes are
-// contiguous 16-byte rows in HBM (pack p of element e at (p ld + e) 16), so
-// one thread moves them into shared memory with bulk asynchronous copies
-// (cp.async.bulk, completion counted in bytes on an mbarrier).  The copies
-// for the CTA's next tile are issued as soon as phase A has read the current
-// tile's rows, and run under the current tile's halo, flux and update work;
-// the next tile's U^n rows are prefetched into L2 at the same time.
+// Staging pipeline: a tile's own state rows are contiguous 16-byte rows in
+// HBM (pack p of element e at (p ld + e) 16), so one thread moves them into
+// shared memory with bulk asynchronous copies (cp.async.bulk, completion
+// counted in bytes on an mbarrier).  The copies for the CTA's next tile are
+// issued once the current tile's halo traces are formed, and run under its
+// flux and update work; the next tile's J^-1, edge-code and U^n rows and its
+// halo and task lists are prefetched into L2 at the same time.
 
 // ------------------------------------------------------------- staging --
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -92,10 +92,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 // tasks, own traces and means, halo traces and means as 4-vectors), sized
 // for the largest tile layout the kernel dispatches (P1 tiles of a mixed
 // pack use a prefix), then the staging area.  The staging area first
-// receives the tile's own rows by bulk copy -- the state (SROWS rows of 16
-// bytes per element), the two J^-1 rows and the edge-code row -- and, once
-// phase A has read them, the halo neighbours' states by 16-byte gathers
-// ([SROWS][hm] rows).
+// receives the tile's own state rows by bulk copy (SROWS rows of 16 bytes
+// per element) and, once phase A has read them, the halo neighbours' states
+// by 16-byte gathers ([SROWS][hm] rows).  J^-1 and the edge codes are read
+// per thread (L2 hits, prefetched with the rows) while the rows arrive.
 template <typename Real>
 struct alignas(16) Vec4 {
     Real x, y, z, w;
@@ -116,43 +116,48 @@ struct TiledLayout {
     static constexpr size_t code_off = (sizeof(Real) * 9 * kTile + 15) / 16 * 16;
 };
 
-template <typename Real, int ORD>
+// Cell means (own and halo) are kept only where the LLF coefficient needs
+// them.
+template <typename Real, int ORD, int FLUX>
 struct TiledSmem {
     static constexpr int NG = ORD == 1 ? 2 : 3;
     static constexpr int SROWS = (ORD == 1 ? 3 : 6) * (int)(sizeof(Real) / 4);
+    static constexpr int MEANS = FLUX == RKDG_FLUX_LLF ? 1 : 0;
     __host__ __device__ static constexpr size_t work(int hm) {
         return TiledLayout<Real>::code_off + sizeof(int4) * kTile + sizeof(uint16_t) * 3 * kTile +
-               sizeof(Vec4<Real>) * ((size_t)3 * NG * kTile + kTile + (size_t)NG * hm + hm);
+               sizeof(Vec4<Real>) * ((size_t)3 * NG * kTile + MEANS * kTile + (size_t)NG * hm + MEANS * hm);
     }
     __host__ __device__ static constexpr size_t stage_offset(int hm) { return (work(hm) + 127) / 128 * 128; }
     __host__ __device__ static constexpr size_t stage_rows(int hm) {
-        return (size_t)(SROWS + 3) * kTile > (size_t)SROWS * hm ? (size_t)(SROWS + 3) * kTile : (size_t)SROWS * hm;
+        return (size_t)SROWS * (kTile > hm ? kTile : hm);
     }
     __host__ __device__ static constexpr size_t bytes(int hm) { return stage_offset(hm) + stage_rows(hm) * 16; }
 };
 
-// Resident CTAs per SM the register allocation is held to.
+// Resident CTAs per SM the register allocation is held to (FP32 P2: 96
+// registers, 20 warps per SM).
 template <typename Real, int ORD>
 struct TiledOccupancy {
-    static constexpr int value = sizeof(Real) == 8 ? (ORD == 1 ? 3 : 2) : (ORD == 1 ? 5 : 4);
+    static constexpr int value = sizeof(Real) == 8 ? (ORD == 1 ? 3 : 2) : 5;
 };
 
-// Issues the bulk copies of tile d's rows into the staging area (one thread),
-// and L2 prefetches of its U^n rows and of its halo and task lists (the
-// tables are padded so that the 16-byte rounding stays inside them).
-template <typename Real, int SROWS>
+// Issues the bulk copies of tile d's state rows into the staging area (one
+// thread), and L2 prefetches of its J^-1 and edge-code rows, its U^n rows
+// and its halo and task lists (the tables are padded so that the 16-byte
+// rounding stays inside them).
+template <typename Real>
 __device__ __forceinline__ void stage_issue(const StageArgs& a, const TileArgs& ta, const int4 d,
                                             const int4 dd, unsigned char* stg, uint64_t* bar) {
     const int rows = (d.w == 2 ? 6 : 3) * (int)(sizeof(Real) / 4);
     const uint32_t rb = (uint32_t)d.y * 16u;
-    mbar_expect_tx(bar, rb * (uint32_t)(rows + 3));
+    mbar_expect_tx(bar, rb * (uint32_t)rows);
     const char* U = static_cast<const char*>(a.U);
     for (int r = 0; r < rows; ++r)
         bulk_g2s(stg + (size_t)r * kTile * 16, U + ((size_t)r * a.ld + d.x) * 16, rb, bar);
     const char* J = reinterpret_cast<const char*>(a.jinv);
-    bulk_g2s(stg + (size_t)SROWS * kTile * 16, J + (size_t)d.x * 16, rb, bar);
-    bulk_g2s(stg + (size_t)(SROWS + 1) * kTile * 16, J + ((size_t)a.ld + d.x) * 16, rb, bar);
-    bulk_g2s(stg + (size_t)(SROWS + 2) * kTile * 16, ta.code + d.x, rb, bar);
+    bulk_prefetch_l2(J + (size_t)d.x * 16, rb);
+    bulk_prefetch_l2(J + ((size_t)a.ld + d.x) * 16, rb);
+    bulk_prefetch_l2(ta.code + d.x, rb);
     if (a.U0 != nullptr) {
         const char* U0 = static_cast<const char*>(a.U0);
         for (int r = 0; r < rows; ++r) bulk_prefetch_l2(U0 + ((size_t)r * a.ld + d.x) * 16, rb);
@@ -195,16 +200,18 @@ __device__ __forceinline__ void load_staged(const unsigned char* stg, int x, Rea
     }
 }
 
-// FP32 tiles keep the stage input in registers from phase A to the update;
-// FP64 tiles, short of registers, read it again (an L2 hit).
+// With RKDG_HOLD_STATE 1, FP32 tiles keep the stage input in registers from
+// phase A to the update; by default both precisions read it again (an L2
+// hit), which leaves FP32 P2 tiles at 96 registers.
 #ifndef RKDG_HOLD_STATE
-#define RKDG_HOLD_STATE 1
+#define RKDG_HOLD_STATE 0
 #endif
 
-template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE, int SROWS>
+template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE>
 __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& ta, const int4 d0,
                                            const int4 d1, unsigned char* smem_raw, unsigned char* stg,
-                                           const int4 dn, const int4 dn1, uint64_t* bar) {
+                                           const int nxt, const int ntiles, uint64_t* bar, const double2 r0,
+                                           const double2 r1, const int4 code) {
     constexpr int CFG = cfg_index(NQ, NG);
     constexpr int BT = kTile;
     constexpr bool HOLD = RKDG_HOLD_STATE && sizeof(Real) == 4;
@@ -215,9 +222,10 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     int4* s_code = reinterpret_cast<int4*>(smem_raw + TiledLayout<Real>::code_off);  // [BT]
     uint16_t* s_task = reinterpret_cast<uint16_t*>(s_code + BT);           // [3 BT] flux tasks
     V4* s_tr = reinterpret_cast<V4*>(s_task + 3 * BT);                     // [3][NG][BT] own traces
-    V4* s_mean = s_tr + 3 * NG * BT;                                       // [BT]
-    V4* s_htr = s_mean + BT;                                               // [NG][HM] halo traces
-    V4* s_hmean = s_htr + NG * HM;                                         // [HM]
+    constexpr int MEANS = FLUX == RKDG_FLUX_LLF ? 1 : 0;                   // LLF needs cell means
+    V4* s_mean = s_tr + 3 * NG * BT;                                       // [BT] (LLF)
+    V4* s_htr = s_mean + MEANS * BT;                                       // [NG][HM] halo traces
+    V4* s_hmean = s_htr + NG * HM;                                         // [HM] (LLF)
     __shared__ Real s_ephi[3][NG][NB];
     for (int x = threadIdx.x; x < 3 * NG * NB; x += BT) {
         int k = x / (NG * NB), g = (x / NB) % NG, i = x % NB;
@@ -267,9 +275,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     }
     Real R[NB][4];
     Real u[NB][4];
-    const double2* sj = reinterpret_cast<const double2*>(stg + (size_t)SROWS * BT * 16);
-    const double2 r0 = sj[sx], r1 = sj[BT + sx];
-    s_code[tid] = reinterpret_cast<const int4*>(stg + (size_t)(SROWS + 2) * BT * 16)[sx];
+    s_code[tid] = code;
     // edge normals N_k (length = edge length; N_k / area = 2(r0 + r1), -2 r0,
     // -2 r1) from the FP64 J^-1 rows, kept in the working precision
     const double det = r0.x * r1.y - r0.y * r1.x;  // 1 / (2 area)
@@ -311,7 +317,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                 mfull[v] = u[0][v] + ref_of<Real>(fs, v);  // the cell mean itself
                 if constexpr (!DEV) u[0][v] = mfull[v];
             }
-            put4(s_mean + tid, mfull);
+            if constexpr (MEANS) put4(s_mean + tid, mfull);
         }
 #pragma unroll
         for (int i = 0; i < NB; ++i)
@@ -402,7 +408,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                         mfull[v] = un[0][v] + ref_of<Real>(fs, v);
                         if constexpr (!DEV) un[0][v] = mfull[v];
                     }
-                    put4(s_hmean + h, mfull);
+                    if constexpr (MEANS) put4(s_hmean + h, mfull);
                 }
                 const int he = hh[r].y;
 #pragma unroll
@@ -421,9 +427,9 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
         }
     }
     __syncthreads();  // halo traces complete; halo states read
-    if (tid == 0 && dn.y > 0) {
+    if (tid == 0 && nxt < ntiles) {  // the CTA's next tile (only this thread reads its descriptor)
         fence_proxy_async();
-        stage_issue<Real, SROWS>(a, ta, dn, dn1, stg, bar);
+        stage_issue<Real>(a, ta, __ldg(ta.desc + 2 * nxt), __ldg(ta.desc + 2 * nxt + 1), stg, bar);
     }
 
     // ------------------------------------------------------------ phase B
@@ -439,9 +445,11 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
             const Real il = rcp_(len);
             const Real nx = Nx * il, ny = Ny * il;
             Real mL[4], mR[4];
-            get4(s_mean + le, mL);
-            if (kind == EDGE_BOUNDARY) ghost<Real>(se, mL, far, nx, ny, mR);
-            else get4(kind == EDGE_HALO ? s_hmean + idx : s_mean + idx, mR);
+            if constexpr (MEANS) {
+                get4(s_mean + le, mL);
+                if (kind == EDGE_BOUNDARY) ghost<Real>(se, mL, far, nx, ny, mR);
+                else get4(kind == EDGE_HALO ? s_hmean + idx : s_mean + idx, mR);
+            }
             Real alpha = Real(0);
             if (FLUX == RKDG_FLUX_LLF) {
                 // LLF coefficient from the average of the two cell means
@@ -568,7 +576,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
 __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
     tiled_stage_kernel(const StageArgs a, const TileArgs ta) {
-    using SM = TiledSmem<Real, ORD>;
+    using SM = TiledSmem<Real, ORD, FLUX>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t s_bar;
     unsigned char* stg = smem_raw + SM::stage_offset(ta.max_halo);
@@ -578,17 +586,16 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
     if (threadIdx.x == 0) mbar_init(&s_bar, 1);
     __syncthreads();
     if (threadIdx.x == 0)
-        stage_issue<Real, SM::SROWS>(a, ta, __ldg(ta.desc + 2 * tile), __ldg(ta.desc + 2 * tile + 1), stg,
-                                     &s_bar);
+        stage_issue<Real>(a, ta, __ldg(ta.desc + 2 * tile), __ldg(ta.desc + 2 * tile + 1), stg, &s_bar);
+    const double2* jinv2 = reinterpret_cast<const double2*>(a.jinv);
     uint32_t parity = 0;
     for (; tile < ntiles; tile += gridDim.x) {
         const int4 d0 = __ldg(ta.desc + 2 * tile), d1 = __ldg(ta.desc + 2 * tile + 1);
         const int nxt = tile + gridDim.x;
-        int4 dn = make_int4(0, 0, 0, 0), dn1 = dn;
-        if (nxt < ntiles) {
-            dn = __ldg(ta.desc + 2 * nxt);
-            dn1 = __ldg(ta.desc + 2 * nxt + 1);
-        }
+        // this thread's J^-1 rows and edge codes (L2 hits), under the wait
+        const int ex = d0.x + ((int)threadIdx.x < d0.y ? (int)threadIdx.x : 0);
+        const double2 r0 = __ldg(jinv2 + ex), r1 = __ldg(jinv2 + a.ld + ex);
+        const int4 code = __ldg(ta.code + ex);
         const bool ok = mbar_wait(&s_bar, parity);
         if (__syncthreads_or(!ok)) {  // also: every thread has seen this phase complete
             if (threadIdx.x == 0) atomicOr(&a.ctl[d0.z].error, 2);
@@ -596,13 +603,14 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
         }
         parity ^= 1u;
         if (MODE == MODE_STAGE && a.ctl[d0.z].done) {  // finished solve: pass the tile on
-            if (threadIdx.x == 0 && dn.y > 0) stage_issue<Real, SM::SROWS>(a, ta, dn, dn1, stg, &s_bar);
+            if (threadIdx.x == 0 && nxt < ntiles)
+                stage_issue<Real>(a, ta, __ldg(ta.desc + 2 * nxt), __ldg(ta.desc + 2 * nxt + 1), stg, &s_bar);
             continue;
         }
         if (ORD == 2 || (ORD == 3 && d0.w == 2))
-            tile_stage<Real, 6, NQ2, 3, FLUX, MODE, SM::SROWS>(a, ta, d0, d1, smem_raw, stg, dn, dn1, &s_bar);
+            tile_stage<Real, 6, NQ2, 3, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, r0, r1, code);
         else
-            tile_stage<Real, 3, 3, 2, FLUX, MODE, SM::SROWS>(a, ta, d0, d1, smem_raw, stg, dn, dn1, &s_bar);
+            tile_stage<Real, 3, 3, 2, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, r0, r1, code);
         __syncthreads();  // shared memory is reused by the next tile
     }
 }
