@@ -214,6 +214,31 @@ def test_free_stream_preserved_and_conservation():
     np.testing.assert_allclose(s.conservation_totals(), tot0, rtol=1e-13)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_full_size_free_stream_and_conservation(precision):
+    """At the unstructured-vortex size (700 x 700 lattice, 980,000 triangles,
+    P2, HLLC): a uniform state stays uniform and the vortex's conserved totals
+    stay constant over 20 steps (periodic mesh, FP64 totals of the FP64 or
+    FP32 state)."""
+    from rkdg_heter_calculate_b200 import vortex
+
+    mesh = meshgen.periodic_delaunay(700, L=10.0, jitter=0.3, seed=2)
+    assert mesh.ntri == 980000
+    far = primitive_to_conservative(1.0, 1.0, 1.0, 1.0)
+    s = CUDARkdgSolver(mesh, order=2, nq=6, ng=3, flux="hllc", precision=precision, cfl=0.2,
+                       farfield=far)
+    s.initRKDG()
+    s.advance(20)
+    U = s.copyFreedomToHost(basis="native")
+    tol = 1e-13 if precision == "fp64" else 1e-6
+    assert np.abs(U[:, 0, :] - np.array(far)[:, None]).max() < tol
+    assert np.abs(U[:, 1:, :]).max() < tol
+    s.setFreedom(vortex.project_native(mesh, lambda X, Y: vortex.exact(X, Y, 0.0), 6, n=2), basis="native")
+    tot0 = s.conservation_totals()
+    s.advance(20)
+    np.testing.assert_allclose(s.conservation_totals(), tot0, rtol=1e-12 if precision == "fp64" else 1e-6)
+
+
 def test_advance_lands_on_final_time():
     mesh = meshgen.periodic_structured(10, 10)
     s = CUDARkdgSolver(mesh, order=1, nq=3, ng=2, rk=2, cfl=0.3,
