@@ -178,8 +178,9 @@ int rkdg_conservation_totals(rkdg_ctx* ctx, double totals[4]);
 
 /* Benchmark helper: launches the fused kernel of stage s (0-based) `reps`
  * times back to back on the context's stream, writing to a scratch buffer
- * (the state is not advanced), and returns the mean device time per launch
- * in milliseconds measured with CUDA events on that stream.  No reference
+ * (the state is not advanced; the last stage includes its CFL and monitor
+ * epilogue), and returns the mean device time per launch in milliseconds
+ * measured with CUDA events on that stream.  No reference
  * counterpart (the reference times nothing on the device). */
 int rkdg_time_stage(rkdg_ctx* ctx, int32_t s, int32_t reps, double* ms_per_launch);
 
@@ -260,7 +261,8 @@ int rkdg_batch_set_time(rkdg_batch* b, int32_t solve, double t);
  * tile order (0 solve order, 1 P2 tiles first). */
 int rkdg_batch_autotune(rkdg_batch* b, int32_t* ctas, int32_t* tile_order);
 int rkdg_batch_set_shape(rkdg_batch* b, int32_t ctas, int32_t tile_order);
-/* Mean device milliseconds of one launch of stage s over all solves. */
+/* Mean device milliseconds of one launch of stage s over all solves (the
+ * last stage with its CFL and monitor epilogue, as it runs in a step). */
 int rkdg_batch_time_stage(rkdg_batch* b, int32_t s, int32_t reps, double* ms_per_launch);
 int rkdg_batch_get_sizes(const rkdg_batch* b, int64_t* elements, int32_t* ntiles, size_t* device_bytes);
 int rkdg_batch_get_stream(const rkdg_batch* b, void** stream);

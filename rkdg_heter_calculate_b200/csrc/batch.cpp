@@ -422,7 +422,7 @@ int rkdg_batch_time_stage(rkdg_batch* b, int32_t s, int32_t reps, double* ms) {
         a.U = b->U[0];
         a.U0 = s == 0 ? nullptr : b->U[0];
         a.Unew = b->U[1];
-        a.last_stage = 0;
+        a.last_stage = s == (int)b->p.rk - 1;  // the last stage with its CFL/monitor epilogue
         cudaEvent_t e0, e1;
         RKDG_CUDA_TRY(cudaEventCreate(&e0));
         RKDG_CUDA_TRY(cudaEventCreate(&e1));

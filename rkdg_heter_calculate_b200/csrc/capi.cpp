@@ -46,6 +46,7 @@ struct rkdg_ctx {
     int variant = 1;  // 1 tile-staged (default), 0 owner-computes
     int ctas = 0;     // tiled grid size (0: one CTA per tile)
     std::unique_ptr<std::ofstream> reslog;  // residual history file (rkdg_set_residual_log)
+    bool graph_monitor = false;  // the captured step forms the residual monitor
 };
 
 namespace {
@@ -176,13 +177,14 @@ void stage_coeffs(int rk, int s, double& a, double& b) {
     }
 }
 
-void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out) {
+void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out, bool monitor = true) {
     StageArgs a = base_args(c);
     stage_coeffs(c->p.rk, s, a.a, a.b);
     a.U = c->d.U[in];
     a.U0 = s == 0 ? nullptr : c->d.U[u0];
     a.Unew = c->d.U[out];
     a.last_stage = s == c->p.rk - 1;
+    a.monitor = monitor ? 1 : 0;
     launch_stage(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->variant == 1 ? c->ctas : c->block, c->stream);
     if (c->p.limiter == RKDG_LIMITER_TVB)
         launch_tiled_limiter(c->tiles, 0, c->ld, c->d.U[out], c->d.conn, c->d.lim, c->d.jinv, nullptr,
@@ -190,16 +192,17 @@ void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out) {
                              c->stream);
 }
 
-// one full step on the stream with the state in buffer 0 (graph-capturable)
-void enqueue_step(rkdg_ctx* c) {
+// one full step on the stream with the state in buffer 0 (graph-capturable);
+// monitor: also form the residual monitor in the last stage
+void enqueue_step(rkdg_ctx* c, bool monitor) {
     launch_step_begin(c->d.ctl, 1, c->stream);
     if (c->p.rk == 3) {
-        launch_one_stage(c, 0, 0, 0, 1);
-        launch_one_stage(c, 1, 1, 0, 2);
-        launch_one_stage(c, 2, 2, 0, 0);
+        launch_one_stage(c, 0, 0, 0, 1, monitor);
+        launch_one_stage(c, 1, 1, 0, 2, monitor);
+        launch_one_stage(c, 2, 2, 0, 0, monitor);
     } else {
-        launch_one_stage(c, 0, 0, 0, 1);
-        launch_one_stage(c, 1, 1, 0, 0);
+        launch_one_stage(c, 0, 0, 0, 1, monitor);
+        launch_one_stage(c, 1, 1, 0, 0, monitor);
     }
 }
 
@@ -550,7 +553,7 @@ int rkdg_step(rkdg_ctx* c, double dt, double* dt_used, double* monitor) {
         c->h_ctl->t_final = 0.0;
         c->h_ctl->done = 0;
         push_ctl(c);
-        enqueue_step(c);
+        enqueue_step(c, true);
         c->wave_valid = true;
         pull_ctl(c);
         check_error_flag(c);
@@ -576,11 +579,16 @@ int rkdg_advance(rkdg_ctx* c, int32_t nsteps, double t_final, double* t, int32_t
         c->h_ctl->t_final = t_final > 0 ? t_final : 0.0;
         c->h_ctl->done = 0;
         push_ctl(c);
+        if (c->graph && c->graph_monitor != (bool)c->reslog) {  // the history needs the monitor
+            cudaGraphExecDestroy(c->graph);
+            c->graph = nullptr;
+        }
         if (!c->graph) {
+            c->graph_monitor = (bool)c->reslog;
             cudaGraph_t g;
             RKDG_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
             try {
-                enqueue_step(c);
+                enqueue_step(c, c->graph_monitor);
             } catch (...) {
                 cudaStreamEndCapture(c->stream, &g);
                 throw;
@@ -638,7 +646,7 @@ int rkdg_time_stage(rkdg_ctx* c, int32_t s, int32_t reps, double* ms) {
         a.U = c->d.U[0];
         a.U0 = s == 0 ? nullptr : c->d.U[0];
         a.Unew = c->d.U[1];
-        a.last_stage = 0;
+        a.last_stage = s == (int)c->p.rk - 1;  // the last stage with its CFL/monitor epilogue
         cudaEvent_t e0, e1;
         RKDG_CUDA_TRY(cudaEventCreate(&e0));
         RKDG_CUDA_TRY(cudaEventCreate(&e1));

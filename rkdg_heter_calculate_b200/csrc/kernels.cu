@@ -350,6 +350,11 @@ __device__ __forceinline__ double warp_max(double v) {
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
 
 // Block-wide max of up to three non-negative doubles, then one atomicMax
 // each on their bit patterns (ordered like the values for x >= 0; a NaN
@@ -626,8 +631,10 @@ __global__ void __launch_bounds__(128) stage_kernel(const StageArgs a) {
             elem_lengths<Real>(r0, r1, len, ia);
             wv = wave_of<Real>(m, gamma, len, ia, bad);
             if (bad) atomicOr(&a.ctl->error, 1);
-            m0 = fabs((double)R[0][0] - (double)u0m[0]);
-            m1 = fabs((double)R[0][3] - (double)u0m[3]);
+            if (a.monitor) {
+                m0 = fabs((double)R[0][0] - (double)u0m[0]);
+                m1 = fabs((double)R[0][3] - (double)u0m[3]);
+            }
         }
         block_max3_atomic(wv, m0, m1, &a.ctl->wave_bits, &a.ctl->mon_bits[0], &a.ctl->mon_bits[1]);
     }

@@ -184,7 +184,8 @@ struct StageArgs {
     double gamma;
     double far[4];
     const double* far_sid;  // per-solve far-field states [solves][4], or nullptr
-    int last_stage;      // compute wave max / monitor / error in the epilogue
+    int last_stage;      // compute wave max / error (and the monitor when asked) in the epilogue
+    int monitor;         // last stage: also form the residual monitor max |d mean| (rho, rhoE)
 };
 
 // Launchers (kernels.cu).  All asynchronous on `stream`.

@@ -552,7 +552,11 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     }
     if (active) store_state<Real, NB>(Uout, a.ld, e, R);
     if (a.last_stage) {
-        double wv = 0.0, m0 = 0.0, m1 = 0.0;
+        // CFL wave maximum (and the residual monitor when asked) of the new
+        // state: a max over each warp in the working precision, one atomic
+        // per warp on the solve's control block (bits of a non-negative
+        // double order like the values)
+        Real wv = Real(0), m0 = Real(0), m1 = Real(0);
         if (active) {
             bool bad;
             Real m[4], len[3];
@@ -560,12 +564,25 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
             for (int v = 0; v < 4; ++v) m[v] = R[0][v] + ref_of<Real>(fs, v);
 #pragma unroll
             for (int k = 0; k < 3; ++k) len[k] = s_nrm[(3 * k + 2) * BT + tid];
-            wv = wave_of<Real>(m, gamma, len, inv_area, bad);
+            wv = (Real)wave_of<Real>(m, gamma, len, inv_area, bad);
             if (bad) atomicOr(&ctl->error, 1);
-            m0 = fabs((double)R[0][0] - (double)u0m[0]);
-            m1 = fabs((double)R[0][3] - (double)u0m[3]);
+            if (a.monitor) {
+                m0 = fabs(R[0][0] - u0m[0]);
+                m1 = fabs(R[0][3] - u0m[3]);
+            }
         }
-        block_max3_atomic(wv, m0, m1, &ctl->wave_bits, &ctl->mon_bits[0], &ctl->mon_bits[1]);
+        wv = warp_max(wv);
+        if (a.monitor) {
+            m0 = warp_max(m0);
+            m1 = warp_max(m1);
+        }
+        if ((tid & 31) == 0) {
+            atomicMax(&ctl->wave_bits, (unsigned long long)__double_as_longlong((double)wv));
+            if (a.monitor) {
+                atomicMax(&ctl->mon_bits[0], (unsigned long long)__double_as_longlong((double)m0));
+                atomicMax(&ctl->mon_bits[1], (unsigned long long)__double_as_longlong((double)m1));
+            }
+        }
     }
 }
 
