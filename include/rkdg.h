@@ -308,6 +308,16 @@ int rkdg_server_stats(rkdg_server* s, double* dof_stage_updates, double* busy_se
 /* Seconds on the loop's steady clock (the clock of rkdg_server_wait's times). */
 double rkdg_server_clock(void);
 
+/* ---- diagnostics ------------------------------------------------------- */
+/* No reference counterpart.  The stage kernels wait on an mbarrier for each
+ * tile's staged rows, and every such wait gives up after 2 s, sets an error
+ * bit in the solve's control word (reported as RKDG_ERR_CUDA at the next host
+ * sync) and ends the CTA instead of hanging the device.  This self-test runs
+ * one such wait on data that never arrives, with limit_s (<= 10) seconds:
+ * *timed_out = 1 and *waited_s >= limit_s when the bound works; the device
+ * stays usable afterwards. */
+int rkdg_wait_selftest(double limit_s, int32_t* timed_out, double* waited_s);
+
 /* ---- mesh files -------------------------------------------------------- */
 /* Reads the reference's mesh set: the mesh configuration file
  * (trianglenum, verticenum, edgenum and the five file names) and the five

@@ -111,6 +111,7 @@ def lib():
             "rkdg_checkpoint_save": (C.c_int, [vp, C.c_char_p]),
             "rkdg_checkpoint_load": (C.c_int, [vp, C.c_char_p]),
             "rkdg_set_residual_log": (C.c_int, [vp, C.c_char_p]),
+            "rkdg_wait_selftest": (C.c_int, [C.c_double, C.POINTER(C.c_int32), _dp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

@@ -884,3 +884,19 @@ int rkdg_set_residual_log(rkdg_ctx* c, const char* path) {
         c->reslog = std::move(f);
     });
 }
+
+int rkdg_wait_selftest(double limit_s, int32_t* timed_out, double* waited_s) {
+    return guarded([&] {
+        if (!timed_out || !waited_s || !(limit_s > 0) || limit_s > 10)
+            throw Error{RKDG_ERR_INVALID, "rkdg_wait_selftest: limit must be in (0, 10] s"};
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Error{RKDG_ERR_NODEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e)};
+        }
+        int t = 0;
+        wait_selftest(limit_s, &t, waited_s);
+        *timed_out = t;
+    });
+}

@@ -1107,6 +1107,19 @@ void launch_residual(const StageArgs& a, const TileArgs& t, int variant, int ord
     dispatch<MODE_RESIDUAL>(a, t, variant, order, nq, ng, flux, prec, block, stream);
 }
 
+void wait_selftest(double limit_s, int* timed_out, double* waited_s) {
+    unsigned long long* d = nullptr;
+    RKDG_CUDA_TRY(cudaMalloc(&d, 2 * sizeof(unsigned long long)));
+    unsigned long long h[2] = {0, 0};
+    wait_selftest_kernel<<<1, 32>>>((uint64_t)(limit_s * 1e9), d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) throw Error{RKDG_ERR_CUDA, std::string("wait self-test: ") + cudaGetErrorString(e)};
+    *timed_out = (int)h[0];
+    *waited_s = (double)h[1] * 1e-9;
+}
+
 void launch_wave(const TileArgs& t, int ld, const void* U, int prec, const double* jinv,
                  double gamma, StepCtl* ctl, int nsolves, const double* refs, cudaStream_t stream) {
     if (nsolves > 0) reset_wave_kernel<<<(nsolves + 127) / 128, 128, 0, stream>>>(ctl, nsolves);

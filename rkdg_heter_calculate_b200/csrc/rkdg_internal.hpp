@@ -206,6 +206,8 @@ void launch_residual(const StageArgs& a, const TileArgs& t, int variant, int ord
 void launch_wave(const TileArgs& t, int ld, const void* U, int prec, const double* jinv,
                  double gamma, StepCtl* ctl, int nsolves, const double* refs, cudaStream_t stream);
 void launch_step_begin(StepCtl* ctl, int nsolves, cudaStream_t stream);
+// bounded device wait on data that never arrives (see rkdg_wait_selftest)
+void wait_selftest(double limit_s, int* timed_out, double* waited_s);
 // resident CTAs per SM of the tiled stage kernel (order 3: mixed pack)
 int tiled_max_ctas_per_sm(int prec, int order, int nq, int flux, int max_halo);
 // TVB limiter over tiles; flags[solve] (may be null: all on) enables it per

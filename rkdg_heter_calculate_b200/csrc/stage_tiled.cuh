@@ -76,16 +76,33 @@ __device__ __forceinline__ uint64_t global_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Waits for the barrier phase of the given parity; gives up after about two
-// seconds (or 2^26 polls), returning false.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Waits for the barrier phase of the given parity; gives up after limit_ns
+// nanoseconds (two seconds for the stage kernel's staging waits) or 2^26
+// polls, returning false.
+constexpr uint64_t kStageWaitNs = 2000000000ull;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns = kStageWaitNs) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_ns();
     for (uint32_t it = 1; it < (1u << 26); ++it) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 255u) == 0 && global_ns() - t0 > 2000000000ull) return false;
+        if ((it & 255u) == 0 && global_ns() - t0 > limit_ns) return false;
     }
     return false;
+}
+
+// Self-test of the bounded wait: one thread arms an mbarrier for 16 bytes
+// that no copy ever delivers and waits on it with the given limit; out[0] =
+// 1 if the wait gave up, out[1] = nanoseconds waited.  Nothing is in flight
+// when it returns.
+__global__ void wait_selftest_kernel(uint64_t limit_ns, unsigned long long* out) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    mbar_expect_tx(&bar, 16);
+    const uint64_t t0 = global_ns();
+    const bool ok = mbar_wait(&bar, 0, limit_ns);
+    out[0] = ok ? 0ull : 1ull;
+    out[1] = global_ns() - t0;
 }
 
 // Shared memory of one CTA: the work area (edge normals, edge codes, flux

@@ -81,3 +81,19 @@ def test_mismatched_checkpoints_are_refused(tmp_path):
     with pytest.raises(capi.RkdgError) as e:
         a.restore(str(tmp_path / "missing.ckpt"))
     assert e.value.code == capi.RKDG_ERR_IO
+
+
+def test_device_wait_gives_up_and_the_device_stays_usable():
+    """A staging wait on data that never arrives ends after its limit with a
+    status the host reads (no hang), and the next solve runs normally."""
+    import ctypes as C
+
+    t, w = C.c_int32(), C.c_double()
+    capi.check(capi.lib().rkdg_wait_selftest(0.2, C.byref(t), C.byref(w)))
+    assert t.value == 1 and 0.2 <= w.value < 5.0
+    mesh = meshgen.periodic_delaunay(8, seed=1)
+    s = solver(mesh, "fp32")
+    s.initRKDG()
+    s.advance(3)
+    U = s.copyFreedomToHost(basis="native")
+    assert np.abs(U[:, 0, :] - np.array(FAR)[:, None]).max() < 1e-6
