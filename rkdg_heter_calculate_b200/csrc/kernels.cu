@@ -34,6 +34,7 @@ struct Tab {
     Real vdxi[kMaxNQ][kMaxNB];  // weight * d psi / d xi
     Real veta[kMaxNQ][kMaxNB];  // weight * d psi / d eta
     Real ephi[3][kMaxNG][kMaxNB];
+    Real ephiw[3][kMaxNG][kMaxNB];  // 2 w_g psi_i at point g of edge k (surface projection)
     Real ew[kMaxNG];
     Real mphi[3][2];
     Real minv[2][3];
@@ -57,6 +58,16 @@ __device__ __forceinline__ const Tab<float>& tab<float>(int c) { return c_tab_f[
 
 void upload_tables(int nq, int ng) {
     RuleTables t = make_tables(nq, ng);
+    // the tile kernel forms the psi_0 term once (psi_0 is the same constant
+    // at every volume and edge point) and skips the eta-derivative of psi_1
+    // (a function of xi alone): both hold exactly for the native basis
+    for (int q = 0; q < nq; ++q)
+        if (t.vphi[q][0] != t.vphi[0][0] || t.veta_w[q][1] != 0.0)
+            throw Error{RKDG_ERR_INVALID, "basis tables: psi_0 not constant or psi_1 not a function of xi"};
+    for (int k = 0; k < 3; ++k)
+        for (int g = 0; g < ng; ++g)
+            if (t.ephi[k][g][0] != t.vphi[0][0])
+                throw Error{RKDG_ERR_INVALID, "basis tables: psi_0 not constant on the edges"};
     Tab<double> d{};
     Tab<float> f{};
     for (int q = 0; q < kMaxNQ; ++q)
@@ -73,6 +84,8 @@ void upload_tables(int nq, int ng) {
             for (int i = 0; i < kMaxNB; ++i) {
                 d.ephi[k][g][i] = t.ephi[k][g][i];
                 f.ephi[k][g][i] = (float)t.ephi[k][g][i];
+                d.ephiw[k][g][i] = 2.0 * t.ew[g] * t.ephi[k][g][i];
+                f.ephiw[k][g][i] = (float)(2.0 * t.ew[g] * t.ephi[k][g][i]);
             }
     for (int g = 0; g < kMaxNG; ++g) {
         d.ew[g] = t.ew[g];
@@ -179,14 +192,27 @@ __device__ __forceinline__ void ghost(int tag, const Real u[4], const Real far[4
 }
 
 // Reciprocal, quotient and square root: IEEE in FP64 (the parity path);
-// in FP32 the MUFU approximations (about 2 ulp), which the FP32 precision
-// form's tolerance absorbs.
+// in FP32 the PTX approximations (rcp.approx, rsqrt.approx: about 1 ulp),
+// which the FP32 precision form's tolerance absorbs, with subnormal inputs
+// and results flushed to zero (.ftz: one instruction each, no subnormal
+// range handling; the arguments are densities, pressures, edge lengths and
+// wave-speed differences, all far above the subnormal range).
+__device__ __forceinline__ float rcp_ftz(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 __device__ __forceinline__ double rcp_(double x) { return 1.0 / x; }
-__device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ float rcp_(float x) { return rcp_ftz(x); }
 __device__ __forceinline__ double div_(double a, double b) { return a / b; }
-__device__ __forceinline__ float div_(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ float div_(float a, float b) { return a * rcp_ftz(b); }
 __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
-__device__ __forceinline__ float sqrt_(float x) { return x * rsqrtf(x); }
+__device__ __forceinline__ float sqrt_(float x) { return x * rsqrt_ftz(x); }
 
 // Normal Euler flux through the scaled normal (Nx, Ny): F Nx + G Ny.
 template <typename Real>
@@ -329,19 +355,20 @@ __device__ __forceinline__ void hllc_dev(const Real dL[4], const Real dR[4], Rea
     const Real dpRL = R.dp - L.dp;
     const Real DL = (dpRL + kR * dqLR) * idk, DR = (dpRL + kL * dqLR) * idk;
     const Real SM = qL + DL;
-    const bool left = SM >= Real(0);
+    // one selection instead of hllc()'s three-way one: the result is
+    // F_K + c (U_K + ex) with K = L when S_L >= 0, R when S_R <= 0 (both
+    // with c = 0) and else the side of S_M, which equals F_L, F_R or F*_K
+    // exactly as selected there (S_M stays finite while either side has a
+    // positive sound speed)
+    const bool sl = SL >= Real(0), sr = SR <= Real(0);
+    const bool left = sl || (!sr && SM >= Real(0));
     const Real S = left ? SL : SR, D = left ? DL : DR, k = left ? kL : kR, p = left ? pL : pR;
-    const Real c = S * D * rcp_(S - SM);
+    const Real c = (sl || sr) ? Real(0) : S * D * rcp_(S - SM);
     const Real UK[4] = {r.rho + (left ? dL[0] : dR[0]), r.mx + (left ? dL[1] : dR[1]),
                         r.my + (left ? dL[2] : dR[2]), r.E + (left ? dL[3] : dR[3])};
     const Real ex[4] = {Real(0), k * nx, k * ny, k * SM + p};
-    const bool sl = SL >= Real(0), sr = SR <= Real(0);
 #pragma unroll
-    for (int v = 0; v < 4; ++v) {
-        const Real FK = left ? FL[v] : FR[v];
-        const Real fs = FK + c * (UK[v] + ex[v]);
-        f[v] = sl ? FL[v] : (sr ? FR[v] : fs);
-    }
+    for (int v = 0; v < 4; ++v) f[v] = (left ? FL[v] : FR[v]) + c * (UK[v] + ex[v]);
 }
 
 // ---------------------------------------------------------- reductions --
@@ -392,7 +419,7 @@ __device__ __forceinline__ void block_max3_atomic(double a, double b, double c,
 
 // sqrt that returns 0 at 0 (the FP32 form uses the reciprocal square root).
 __device__ __forceinline__ double sqrt0_(double x) { return sqrt(x); }
-__device__ __forceinline__ float sqrt0_(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+__device__ __forceinline__ float sqrt0_(float x) { return x > 0.0f ? x * rsqrt_ftz(x) : 0.0f; }
 
 // Edge lengths |N_k| and 1 / area of an element from its FP64 J^-1 rows:
 // N_k = 2 area (r0 + r1, -r0, -r1) in FP64, cast to the working precision,

@@ -294,21 +294,30 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     Real u[NB][4];
     s_code[tid] = code;
     // edge normals N_k (length = edge length; N_k / area = 2(r0 + r1), -2 r0,
-    // -2 r1) from the FP64 J^-1 rows, kept in the working precision
+    // -2 r1) from the FP64 J^-1 rows, kept in the working precision.  The
+    // residual is accumulated scaled by 2 area (= 1 / det J^-1): the volume
+    // term through 2 area J^-1 = (-N_1; -N_2), the surface term through the
+    // table 2 w_g psi_i, and the factor det J^-1 applied once in the update.
     const double det = r0.x * r1.y - r0.y * r1.x;  // 1 / (2 area)
     const Real inv_area = (Real)(2.0 * det);
+    Real j00, j01, j10, j11;  // rows of 2 area J^-1
     {
         const double area2 = 1.0 / det;
         const double cx[3] = {r0.x + r1.x, -r0.x, -r1.x}, cy[3] = {r0.y + r1.y, -r0.y, -r1.y};
+        Real Nx[3], Ny[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            const Real Nx = (Real)(cx[k] * area2), Ny = (Real)(cy[k] * area2);
-            s_nrm[(3 * k + 0) * BT + tid] = Nx;
-            s_nrm[(3 * k + 1) * BT + tid] = Ny;
-            s_nrm[(3 * k + 2) * BT + tid] = sqrt_(Nx * Nx + Ny * Ny);
+            Nx[k] = (Real)(cx[k] * area2), Ny[k] = (Real)(cy[k] * area2);
+            s_nrm[(3 * k + 0) * BT + tid] = Nx[k];
+            s_nrm[(3 * k + 1) * BT + tid] = Ny[k];
+            s_nrm[(3 * k + 2) * BT + tid] = sqrt_(Nx[k] * Nx[k] + Ny[k] * Ny[k]);
         }
+        j00 = -Nx[1], j01 = -Ny[1], j10 = -Nx[2], j11 = -Ny[2];
     }
     Real m_st[4];  // the stored cell mean (a deviation in FP32)
+    // psi_0 is the constant K00 at every volume and edge point: its term is
+    // formed once per state
+    const Real k00 = tb.vphi[0][0];
     {
         load_staged<Real, NB>(stg, sx, u);
         __syncthreads();  // staged rows consumed: the area takes the halo states
@@ -340,31 +349,30 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
         for (int i = 0; i < NB; ++i)
 #pragma unroll
             for (int v = 0; v < 4; ++v) R[i][v] = Real(0);
-        const Real j00 = (Real)r0.x, j01 = (Real)r0.y, j10 = (Real)r1.x, j11 = (Real)r1.y;
+        Real c0[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) c0[v] = k00 * u[0][v];
         // FP32: the quadrature loop stays rolled (a smaller body keeps the
         // instruction cache warm across the CTAs on an SM; 3 % faster);
-        // FP64 unrolls it
+        // FP64 unrolls it.  Each product is its own fused multiply-add, and
+        // psi_1 (a function of xi alone) has no eta-derivative term.
         constexpr int VOL_UNROLL = sizeof(Real) == 4 ? 1 : NQ;
 #pragma unroll VOL_UNROLL
         for (int q = 0; q < NQ; ++q) {
             Real w[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
-                Real s = Real(0);
+                Real s = c0[v];
 #pragma unroll
-                for (int i = 0; i < NB; ++i) s += tb.vphi[q][i] * u[i][v];
+                for (int i = 1; i < NB; ++i) s += tb.vphi[q][i] * u[i][v];
                 w[v] = s;
             }
+            Real fx[4], fy[4];
             if constexpr (DEV) {
-                // flux deviations through the rows of J^-1: (j00 F + j01 G) - ref
+                // flux deviations through the rows of 2 area J^-1
                 const DevPrims<Real> pw = dev_prims(w, rs, gm1);
-                Real fx[4], fy[4];
                 dev_flux(w, pw, rs, j00, j01, fx);
                 dev_flux(w, pw, rs, j10, j11, fy);
-#pragma unroll
-                for (int v = 0; v < 4; ++v)
-#pragma unroll
-                    for (int i = 1; i < NB; ++i) R[i][v] += fx[v] * tb.vdxi[q][i] + fy[v] * tb.veta[q][i];
             } else {
                 Real ri = rcp_(w[0]);
                 Real vx = w[1] * ri, vy = w[2] * ri;
@@ -373,11 +381,16 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                 Real G[4] = {w[2], w[1] * vy, w[2] * vy + p, (w[3] + p) * vy};
 #pragma unroll
                 for (int v = 0; v < 4; ++v) {
-                    Real fx = j00 * F[v] + j01 * G[v];
-                    Real fy = j10 * F[v] + j11 * G[v];
-#pragma unroll
-                    for (int i = 1; i < NB; ++i) R[i][v] += fx * tb.vdxi[q][i] + fy * tb.veta[q][i];
+                    fx[v] = j00 * F[v] + j01 * G[v];
+                    fy[v] = j10 * F[v] + j11 * G[v];
                 }
+            }
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+#pragma unroll
+                for (int i = 1; i < NB; ++i) R[i][v] += fx[v] * tb.vdxi[q][i];
+#pragma unroll
+                for (int i = 2; i < NB; ++i) R[i][v] += fy[v] * tb.veta[q][i];
             }
         }
 #pragma unroll
@@ -387,9 +400,9 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                 Real t[4];
 #pragma unroll
                 for (int v = 0; v < 4; ++v) {
-                    Real s = Real(0);
+                    Real s = c0[v];
 #pragma unroll
-                    for (int i = 0; i < NB; ++i) s += tb.ephi[k][g][i] * u[i][v];
+                    for (int i = 1; i < NB; ++i) s += tb.ephi[k][g][i] * u[i][v];
                     t[v] = s;
                 }
                 put4(s_tr + (k * NG + g) * BT + tid, t);
@@ -432,14 +445,17 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                     if constexpr (MEANS) put4(s_hmean + h, mfull);
                 }
                 const int he = hh[r].y;
+                Real c0[4];
+#pragma unroll
+                for (int v = 0; v < 4; ++v) c0[v] = k00 * un[0][v];
 #pragma unroll
                 for (int g = 0; g < NG; ++g) {
                     Real t[4];
 #pragma unroll
                     for (int v = 0; v < 4; ++v) {
-                        Real s = Real(0);
+                        Real s = c0[v];
 #pragma unroll
-                        for (int i = 0; i < NB; ++i) s += s_ephi[he][g][i] * un[i][v];
+                        for (int i = 1; i < NB; ++i) s += s_ephi[he][g][i] * un[i][v];
                         t[v] = s;
                     }
                     put4(s_htr + g * HM + h, t);
@@ -490,13 +506,14 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                 get4(slot, uL);
                 // the neighbour's point NG-1-g on its edge se pairs with ours
                 // (src/kernelfunctions.cu:545-549)
+                V4* nslot = kind == EDGE_HALO ? s_htr + (NG - 1 - g) * HM + idx
+                                              : s_tr + (se * NG + NG - 1 - g) * BT + idx;
                 if (kind == EDGE_BOUNDARY) {
                     if constexpr (DEV) ghost_dev<Real>(se, uL, rs, nx, ny, uR);
                     else ghost<Real>(se, uL, far, nx, ny, uR);
                 }
-                else get4(kind == EDGE_HALO ? s_htr + (NG - 1 - g) * HM + idx
-                                            : s_tr + (se * NG + NG - 1 - g) * BT + idx, uR);
-                Real fh[4];
+                else get4(nslot, uR);
+                Real fh[4], fn[4];  // the flux out of this side and into the neighbour
                 if (FLUX == RKDG_FLUX_LLF) {
                     Real fL[4], fR[4];
                     if constexpr (DEV) {
@@ -508,50 +525,60 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                         normal_flux<Real>(uR, Nx, Ny, gm1, fR, pR);
                     }
 #pragma unroll
-                    for (int v = 0; v < 4; ++v) fh[v] = Real(0.5) * (fL[v] + fR[v] - alpha * (uR[v] - uL[v]));
+                    for (int v = 0; v < 4; ++v) {
+                        const Real t = fL[v] + fR[v] - alpha * (uR[v] - uL[v]);
+                        fh[v] = Real(0.5) * t;
+                        fn[v] = Real(-0.5) * t;
+                    }
                 } else {
-                    if constexpr (DEV) hllc_dev<Real>(uL, uR, nx, ny, gamma, rs, fh);
-                    else hllc<Real>(uL, uR, nx, ny, gamma, fh);
+                    Real f[4];
+                    if constexpr (DEV) hllc_dev<Real>(uL, uR, nx, ny, gamma, rs, f);
+                    else hllc<Real>(uL, uR, nx, ny, gamma, f);
 #pragma unroll
-                    for (int v = 0; v < 4; ++v) fh[v] *= len;
+                    for (int v = 0; v < 4; ++v) {
+                        fh[v] = f[v] * len;
+                        fn[v] = f[v] * -len;
+                    }
                 }
+                // each slot of an edge is read by this task alone: the
+                // computing side's slot takes the flux, an in-tile
+                // neighbour's slot its negation
                 put4(slot, fh);
+                if (kind == EDGE_IN_OWNER) put4(nslot, fn);
             }
         }
     }
     __syncthreads();
 
     // ------------------------------------------------------------ phase C
-    const int4 cd = s_code[tid];
+    // every own slot now holds the outward flux of its edge point
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const int c = k == 0 ? cd.x : (k == 1 ? cd.y : cd.z);
-        const int kind = c & 3, se = (c >> 2) & 3, idx = c >> 4;
-        const bool other = kind == EDGE_IN_OTHER;
+    for (int k = 0; k < 3; ++k)
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
             Real f[4];
-            get4(other ? s_tr + (se * NG + NG - 1 - g) * BT + idx : s_tr + (k * NG + g) * BT + tid, f);
-            const Real wg = other ? -(tb.ew[g] * inv_area) : tb.ew[g] * inv_area;
+            get4(s_tr + (k * NG + g) * BT + tid, f);
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                Real cw = wg * f[v];
+            for (int v = 0; v < 4; ++v)
 #pragma unroll
-                for (int i = 0; i < NB; ++i) R[i][v] -= cw * tb.ephi[k][g][i];
-            }
+                for (int i = 0; i < NB; ++i) R[i][v] -= f[v] * tb.ephiw[k][g][i];
         }
-    }
 
     Real* __restrict__ Uout = static_cast<Real*>(a.Unew);
     if (MODE == MODE_RESIDUAL) {
+        const Real sc = (Real)det;
+#pragma unroll
+        for (int i = 0; i < NB; ++i)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) R[i][v] *= sc;
         if (active) store_state<Real, NB>(Uout, a.ld, e, R);
         return;
     }
     const double dtd = ctl->dt;
     // a U^n + b (U + dt L) as U^n + b ((U - U^n) + dt L): a + b = 1 holds
     // exactly (1/3 and 2/3 both round up in FP32, and a scale of 1 + 3e-8
-    // per step would accumulate into the state)
-    const Real dt = (Real)dtd, cb = (Real)a.b;
+    // per step would accumulate into the state); L = det J^-1 R
+    const Real dt = (Real)(dtd * det), cb = (Real)a.b;
     Real u0m[4] = {Real(0), Real(0), Real(0), Real(0)};
     {
         if constexpr (!HOLD) load_state<Real, NB>(U, a.ld, ee, u);  // stored values (L2 hit)
