@@ -422,18 +422,19 @@ __device__ __forceinline__ double sqrt0_(double x) { return sqrt(x); }
 __device__ __forceinline__ float sqrt0_(float x) { return x > 0.0f ? x * rsqrt_ftz(x) : 0.0f; }
 
 // Edge lengths |N_k| and 1 / area of an element from its FP64 J^-1 rows:
-// N_k = 2 area (r0 + r1, -r0, -r1) in FP64, cast to the working precision,
-// its length there; 1 / area = 2 det J^-1.  The tile kernel forms the same
+// N_k = 2 area (r0 + r1, -r0, -r1) formed in the working precision from
+// the rounded rows, its length there; 1 / area = 2 det J^-1.  The tile kernel forms the same
 // values in phase A.
 template <typename Real>
 __device__ __forceinline__ void elem_lengths(double2 r0, double2 r1, Real len[3], Real& inv_area) {
     const double det = r0.x * r1.y - r0.y * r1.x;
     inv_area = (Real)(2.0 * det);
-    const double area2 = 1.0 / det;
-    const double cx[3] = {r0.x + r1.x, -r0.x, -r1.x}, cy[3] = {r0.y + r1.y, -r0.y, -r1.y};
+    const Real area2 = rcp_((Real)det);
+    const Real ax = (Real)r0.x, ay = (Real)r0.y, bx = (Real)r1.x, by = (Real)r1.y;
+    const Real cx[3] = {ax + bx, -ax, -bx}, cy[3] = {ay + by, -ay, -by};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const Real Nx = (Real)(cx[k] * area2), Ny = (Real)(cy[k] * area2);
+        const Real Nx = cx[k] * area2, Ny = cy[k] * area2;
         len[k] = sqrt_(Nx * Nx + Ny * Ny);
     }
 }

@@ -106,13 +106,19 @@ __global__ void wait_selftest_kernel(uint64_t limit_ns, unsigned long long* out)
 }
 
 // Shared memory of one CTA: the work area (edge normals, edge codes, flux
-// tasks, own traces and means, halo traces and means as 4-vectors), sized
-// for the largest tile layout the kernel dispatches (P1 tiles of a mixed
-// pack use a prefix), then the staging area.  The staging area first
-// receives the tile's own state rows by bulk copy (SROWS rows of 16 bytes
-// per element) and, once phase A has read them, the halo neighbours' states
-// by 16-byte gathers ([SROWS][hm] rows).  J^-1 and the edge codes are read
-// per thread (L2 hits, prefetched with the rows) while the rows arrive.
+// tasks, own traces and means, and in FP64 the halo traces and means, as
+// 4-vectors), sized for the largest tile layout the kernel dispatches (P1
+// tiles of a mixed pack use a prefix), then the staging area.  The staging
+// area first receives the tile's own state rows by bulk copy (SROWS rows of
+// 16 bytes per element); once phase A has read them, the halo neighbours'
+// states by 16-byte gathers ([SROWS][hm] rows).  FP32 (HALO_IN_STAGING):
+// each halo thread overwrites its own neighbour's first NG (+1 with means)
+// rows with that neighbour's traces (and mean), which phase B reads, and the
+// next tile's rows are copied in after phase B; this keeps a CTA within the
+// shared memory of six per SM.  FP64 keeps the halo traces in the work area
+// and copies the next tile's rows in as soon as the halo states are read.
+// J^-1 and the edge codes are read per thread (L2 hits, prefetched with the
+// rows) while the rows arrive.
 template <typename Real>
 struct alignas(16) Vec4 {
     Real x, y, z, w;
@@ -130,7 +136,10 @@ __device__ __forceinline__ void get4(const Vec4<Real>* p, Real a[4]) {
 }
 template <typename Real>
 struct TiledLayout {
-    static constexpr size_t code_off = (sizeof(Real) * 9 * kTile + 15) / 16 * 16;
+    // edge normals per element: FP32 (Nx, Ny) per edge, the length formed
+    // where used; FP64 (Nx, Ny, length)
+    static constexpr int NC = sizeof(Real) == 4 ? 2 : 3;
+    static constexpr size_t code_off = (sizeof(Real) * 3 * NC * kTile + 15) / 16 * 16;
 };
 
 // Cell means (own and halo) are kept only where the LLF coefficient needs
@@ -140,9 +149,11 @@ struct TiledSmem {
     static constexpr int NG = ORD == 1 ? 2 : 3;
     static constexpr int SROWS = (ORD == 1 ? 3 : 6) * (int)(sizeof(Real) / 4);
     static constexpr int MEANS = FLUX == RKDG_FLUX_LLF ? 1 : 0;
+    static constexpr bool HALO_IN_STAGING = sizeof(Real) == 4;
     __host__ __device__ static constexpr size_t work(int hm) {
         return TiledLayout<Real>::code_off + sizeof(int4) * kTile + sizeof(uint16_t) * 3 * kTile +
-               sizeof(Vec4<Real>) * ((size_t)3 * NG * kTile + MEANS * kTile + (size_t)NG * hm + MEANS * hm);
+               sizeof(Vec4<Real>) * ((size_t)3 * NG * kTile + MEANS * kTile +
+                                     (HALO_IN_STAGING ? 0 : (size_t)(NG + MEANS) * hm));
     }
     __host__ __device__ static constexpr size_t stage_offset(int hm) { return (work(hm) + 127) / 128 * 128; }
     __host__ __device__ static constexpr size_t stage_rows(int hm) {
@@ -151,26 +162,36 @@ struct TiledSmem {
     __host__ __device__ static constexpr size_t bytes(int hm) { return stage_offset(hm) + stage_rows(hm) * 16; }
 };
 
-// Resident CTAs per SM the register allocation is held to (FP32 P2: 96
-// registers, 20 warps per SM).
+// Resident CTAs per SM the register allocation is held to (FP32: 80
+// registers and at most 37 KB of shared memory per CTA, 24 warps per SM).
 template <typename Real, int ORD>
 struct TiledOccupancy {
-    static constexpr int value = sizeof(Real) == 8 ? (ORD == 1 ? 3 : 2) : 5;
+    static constexpr int value = sizeof(Real) == 8 ? (ORD == 1 ? 3 : 2) : 6;
 };
 
 // Issues the bulk copies of tile d's state rows into the staging area (one
-// thread), and L2 prefetches of its J^-1 and edge-code rows, its U^n rows
-// and its halo and task lists (the tables are padded so that the 16-byte
-// rounding stays inside them).
+// thread; completion counted on bar).
 template <typename Real>
-__device__ __forceinline__ void stage_issue(const StageArgs& a, const TileArgs& ta, const int4 d,
-                                            const int4 dd, unsigned char* stg, uint64_t* bar) {
+__device__ __forceinline__ void stage_copy(const StageArgs& a, const int4 d, unsigned char* stg, uint64_t* bar) {
     const int rows = (d.w == 2 ? 6 : 3) * (int)(sizeof(Real) / 4);
     const uint32_t rb = (uint32_t)d.y * 16u;
     mbar_expect_tx(bar, rb * (uint32_t)rows);
     const char* U = static_cast<const char*>(a.U);
     for (int r = 0; r < rows; ++r)
         bulk_g2s(stg + (size_t)r * kTile * 16, U + ((size_t)r * a.ld + d.x) * 16, rb, bar);
+}
+// L2 prefetches of tile d's J^-1 and edge-code rows, U^n rows and halo and
+// task lists, and with STATE its state rows (one thread; the tables are
+// padded so that the 16-byte rounding stays inside them).
+template <typename Real, bool STATE>
+__device__ __forceinline__ void stage_prefetch(const StageArgs& a, const TileArgs& ta, const int4 d,
+                                               const int4 dd) {
+    const int rows = (d.w == 2 ? 6 : 3) * (int)(sizeof(Real) / 4);
+    const uint32_t rb = (uint32_t)d.y * 16u;
+    if constexpr (STATE) {
+        const char* U = static_cast<const char*>(a.U);
+        for (int r = 0; r < rows; ++r) bulk_prefetch_l2(U + ((size_t)r * a.ld + d.x) * 16, rb);
+    }
     const char* J = reinterpret_cast<const char*>(a.jinv);
     bulk_prefetch_l2(J + (size_t)d.x * 16, rb);
     bulk_prefetch_l2(J + ((size_t)a.ld + d.x) * 16, rb);
@@ -228,21 +249,25 @@ template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE>
 __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& ta, const int4 d0,
                                            const int4 d1, unsigned char* smem_raw, unsigned char* stg,
                                            const int nxt, const int ntiles, uint64_t* bar, const double2 r0,
-                                           const double2 r1, const int4 code) {
+                                           const double2 r1, const int4 code, Real (*s_red)[3]) {
     constexpr int CFG = cfg_index(NQ, NG);
     constexpr int BT = kTile;
     constexpr bool HOLD = RKDG_HOLD_STATE && sizeof(Real) == 4;
     using V4 = Vec4<Real>;
     const Tab<Real>& tb = tab<Real>(CFG);
     const int HM = ta.max_halo;
-    Real* s_nrm = reinterpret_cast<Real*>(smem_raw);                       // [3][3][BT] Nx, Ny, len
+    constexpr int NC = TiledLayout<Real>::NC;
+    Real* s_nrm = reinterpret_cast<Real*>(smem_raw);                       // [3][NC][BT] Nx, Ny (, len)
     int4* s_code = reinterpret_cast<int4*>(smem_raw + TiledLayout<Real>::code_off);  // [BT]
     uint16_t* s_task = reinterpret_cast<uint16_t*>(s_code + BT);           // [3 BT] flux tasks
     V4* s_tr = reinterpret_cast<V4*>(s_task + 3 * BT);                     // [3][NG][BT] own traces
     constexpr int MEANS = FLUX == RKDG_FLUX_LLF ? 1 : 0;                   // LLF needs cell means
     V4* s_mean = s_tr + 3 * NG * BT;                                       // [BT] (LLF)
-    V4* s_htr = s_mean + MEANS * BT;                                       // [NG][HM] halo traces
-    V4* s_hmean = s_htr + NG * HM;                                         // [HM] (LLF)
+    // halo traces [NG][HM] and means [HM]: FP32 in the staging rows (trace g
+    // of halo h in row g, entry h, of that neighbour's own staged state)
+    constexpr bool HALO_IN_STAGING = TiledSmem<Real, 3, FLUX>::HALO_IN_STAGING;
+    V4* s_htr = HALO_IN_STAGING ? reinterpret_cast<V4*>(stg) : s_mean + MEANS * BT;
+    V4* s_hmean = s_htr + NG * HM;
     __shared__ Real s_ephi[3][NG][NB];
     for (int x = threadIdx.x; x < 3 * NG * NB; x += BT) {
         int k = x / (NG * NB), g = (x / NB) % NG, i = x % NB;
@@ -302,15 +327,18 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     const Real inv_area = (Real)(2.0 * det);
     Real j00, j01, j10, j11;  // rows of 2 area J^-1
     {
-        const double area2 = 1.0 / det;
-        const double cx[3] = {r0.x + r1.x, -r0.x, -r1.x}, cy[3] = {r0.y + r1.y, -r0.y, -r1.y};
+        // FP64 forms them in FP64; FP32 from the rounded J^-1 rows (a few
+        // ulp, without the FP64 reciprocal)
+        const Real area2 = rcp_((Real)det);
+        const Real ax = (Real)r0.x, ay = (Real)r0.y, bx = (Real)r1.x, by = (Real)r1.y;
+        const Real cx[3] = {ax + bx, -ax, -bx}, cy[3] = {ay + by, -ay, -by};
         Real Nx[3], Ny[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            Nx[k] = (Real)(cx[k] * area2), Ny[k] = (Real)(cy[k] * area2);
-            s_nrm[(3 * k + 0) * BT + tid] = Nx[k];
-            s_nrm[(3 * k + 1) * BT + tid] = Ny[k];
-            s_nrm[(3 * k + 2) * BT + tid] = sqrt_(Nx[k] * Nx[k] + Ny[k] * Ny[k]);
+            Nx[k] = cx[k] * area2, Ny[k] = cy[k] * area2;
+            s_nrm[(NC * k + 0) * BT + tid] = Nx[k];
+            s_nrm[(NC * k + 1) * BT + tid] = Ny[k];
+            if constexpr (NC == 3) s_nrm[(NC * k + 2) * BT + tid] = sqrt_(Nx[k] * Nx[k] + Ny[k] * Ny[k]);
         }
         j00 = -Nx[1], j01 = -Ny[1], j10 = -Nx[2], j11 = -Ny[2];
     }
@@ -463,10 +491,15 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
             }
         }
     }
-    __syncthreads();  // halo traces complete; halo states read
+    __syncthreads();  // halo traces complete (FP64: halo states read)
+    int4 nd0 = make_int4(0, 0, 0, 0);
     if (tid == 0 && nxt < ntiles) {  // the CTA's next tile (only this thread reads its descriptor)
-        fence_proxy_async();
-        stage_issue<Real>(a, ta, __ldg(ta.desc + 2 * nxt), __ldg(ta.desc + 2 * nxt + 1), stg, bar);
+        nd0 = __ldg(ta.desc + 2 * nxt);
+        if constexpr (!HALO_IN_STAGING) {
+            fence_proxy_async();
+            stage_copy<Real>(a, nd0, stg, bar);
+        }
+        stage_prefetch<Real, HALO_IN_STAGING>(a, ta, nd0, __ldg(ta.desc + 2 * nxt + 1));
     }
 
     // ------------------------------------------------------------ phase B
@@ -477,8 +510,8 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
             const int c = reinterpret_cast<const int*>(s_code + le)[k];
             const int kind = c & 3, se = (c >> 2) & 3, idx = c >> 4;
             // physical normal N (|N| = edge length) and unit normal of edge k
-            const Real Nx = s_nrm[(3 * k + 0) * BT + le], Ny = s_nrm[(3 * k + 1) * BT + le];
-            const Real len = s_nrm[(3 * k + 2) * BT + le];
+            const Real Nx = s_nrm[(NC * k + 0) * BT + le], Ny = s_nrm[(NC * k + 1) * BT + le];
+            const Real len = NC == 3 ? s_nrm[(NC * k + 2) * BT + le] : sqrt_(Nx * Nx + Ny * Ny);
             const Real il = rcp_(len);
             const Real nx = Nx * il, ny = Ny * il;
             Real mL[4], mR[4];
@@ -548,7 +581,11 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
             }
         }
     }
-    __syncthreads();
+    __syncthreads();  // fluxes complete; FP32: halo traces read, the staging area takes the next tile's rows
+    if (HALO_IN_STAGING && tid == 0 && nxt < ntiles) {
+        fence_proxy_async();
+        stage_copy<Real>(a, nd0, stg, bar);
+    }
 
     // ------------------------------------------------------------ phase C
     // every own slot now holds the outward flux of its edge point
@@ -601,9 +638,11 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     if (active) store_state<Real, NB>(Uout, a.ld, e, R);
     if (a.last_stage) {
         // CFL wave maximum (and the residual monitor when asked) of the new
-        // state: a max over each warp in the working precision, one atomic
-        // per warp on the solve's control block (bits of a non-negative
-        // double order like the values)
+        // state: a max over each warp in the working precision into s_red;
+        // after the tile's closing barrier one thread takes the max over the
+        // warps and makes one atomic per tile on the solve's control block
+        // (a solve's atomics meet at one address, so their number is kept
+        // small)
         Real wv = Real(0), m0 = Real(0), m1 = Real(0);
         if (active) {
             bool bad;
@@ -611,7 +650,10 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 #pragma unroll
             for (int v = 0; v < 4; ++v) m[v] = R[0][v] + ref_of<Real>(fs, v);
 #pragma unroll
-            for (int k = 0; k < 3; ++k) len[k] = s_nrm[(3 * k + 2) * BT + tid];
+            for (int k = 0; k < 3; ++k) {
+                const Real Nx = s_nrm[(NC * k + 0) * BT + tid], Ny = s_nrm[(NC * k + 1) * BT + tid];
+                len[k] = NC == 3 ? s_nrm[(NC * k + 2) * BT + tid] : sqrt_(Nx * Nx + Ny * Ny);
+            }
             wv = (Real)wave_of<Real>(m, gamma, len, inv_area, bad);
             if (bad) atomicOr(&ctl->error, 1);
             if (a.monitor) {
@@ -625,12 +667,29 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
             m1 = warp_max(m1);
         }
         if ((tid & 31) == 0) {
-            atomicMax(&ctl->wave_bits, (unsigned long long)__double_as_longlong((double)wv));
-            if (a.monitor) {
-                atomicMax(&ctl->mon_bits[0], (unsigned long long)__double_as_longlong((double)m0));
-                atomicMax(&ctl->mon_bits[1], (unsigned long long)__double_as_longlong((double)m1));
-            }
+            s_red[tid >> 5][0] = wv;
+            s_red[tid >> 5][1] = m0;
+            s_red[tid >> 5][2] = m1;
         }
+    }
+}
+
+// The tile's maxima from s_red into its solve's control block (one thread,
+// after the barrier that closes the tile; bits of a non-negative double
+// order like the values).
+template <typename Real>
+__device__ __forceinline__ void tile_maxima_atomic(const StageArgs& a, StepCtl* ctl, const Real (*s_red)[3]) {
+    Real w = s_red[0][0], m0 = s_red[0][1], m1 = s_red[0][2];
+#pragma unroll
+    for (int k = 1; k < kTile / 32; ++k) {
+        w = fmax(w, s_red[k][0]);
+        m0 = fmax(m0, s_red[k][1]);
+        m1 = fmax(m1, s_red[k][2]);
+    }
+    atomicMax(&ctl->wave_bits, (unsigned long long)__double_as_longlong((double)w));
+    if (a.monitor) {
+        atomicMax(&ctl->mon_bits[0], (unsigned long long)__double_as_longlong((double)m0));
+        atomicMax(&ctl->mon_bits[1], (unsigned long long)__double_as_longlong((double)m1));
     }
 }
 
@@ -644,14 +703,20 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
     using SM = TiledSmem<Real, ORD, FLUX>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t s_bar;
+    __shared__ Real s_red[kTile / 32][3];  // per-warp maxima of a last stage
     unsigned char* stg = smem_raw + SM::stage_offset(ta.max_halo);
     const int ntiles = ta.ntiles_dev ? *ta.ntiles_dev : ta.ntiles;
     int tile = blockIdx.x;
     if (tile >= ntiles) return;
     if (threadIdx.x == 0) mbar_init(&s_bar, 1);
     __syncthreads();
-    if (threadIdx.x == 0)
-        stage_issue<Real>(a, ta, __ldg(ta.desc + 2 * tile), __ldg(ta.desc + 2 * tile + 1), stg, &s_bar);
+    if (threadIdx.x == 0) {
+        const int4 fd = __ldg(ta.desc + 2 * tile);
+        stage_copy<Real>(a, fd, stg, &s_bar);
+        // FP64 (two CTAs per SM) gains from the first tile's table prefetch,
+        // FP32 (six) loses
+        if constexpr (sizeof(Real) == 8) stage_prefetch<Real, false>(a, ta, fd, __ldg(ta.desc + 2 * tile + 1));
+    }
     const double2* jinv2 = reinterpret_cast<const double2*>(a.jinv);
     uint32_t parity = 0;
     for (; tile < ntiles; tile += gridDim.x) {
@@ -668,14 +733,16 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
         }
         parity ^= 1u;
         if (MODE == MODE_STAGE && a.ctl[d0.z].done) {  // finished solve: pass the tile on
-            if (threadIdx.x == 0 && nxt < ntiles)
-                stage_issue<Real>(a, ta, __ldg(ta.desc + 2 * nxt), __ldg(ta.desc + 2 * nxt + 1), stg, &s_bar);
+            if (threadIdx.x == 0 && nxt < ntiles) stage_copy<Real>(a, __ldg(ta.desc + 2 * nxt), stg, &s_bar);
             continue;
         }
         if (ORD == 2 || (ORD == 3 && d0.w == 2))
-            tile_stage<Real, 6, NQ2, 3, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, r0, r1, code);
+            tile_stage<Real, 6, NQ2, 3, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, r0, r1, code,
+                                                   s_red);
         else
-            tile_stage<Real, 3, 3, 2, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, r0, r1, code);
+            tile_stage<Real, 3, 3, 2, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, r0, r1, code,
+                                                 s_red);
         __syncthreads();  // shared memory is reused by the next tile
+        if (MODE == MODE_STAGE && a.last_stage && threadIdx.x == 0) tile_maxima_atomic<Real>(a, a.ctl + d0.z, s_red);
     }
 }
