@@ -360,7 +360,7 @@ def run_batched(args, dist, peak, peak_kind):
                 acc.append(vortex.l2_error(m, b.state(i), lambda X, Y: vortex.exact(X, Y, t_end[i], beta, GAMMA, ui, vi)))
         out[prec] = {"value": value, "ms_per_step": ms / K, "roofline": roof, "e2e": e2e,
                      "clocks": clocks, "shape": {"ctas": ctas, "tile_order": torder},
-                     "l2": acc}
+                     "l2": acc, "tris": [int(m.ntri) for m in meshes], "orders": [int(o) for o in orders]}
         b.close()
     info = {"solves": len(meshes), "triangles": int(sum(m.ntri for m in meshes)),
             "p1_solves": int((orders == 1).sum()), "p2_solves": int((orders == 2).sum()),
@@ -719,9 +719,14 @@ def main():
             l2 = None
             if r.get("l2") is not None and "fp64" in res and res["fp64"].get("l2") is not None:
                 ratio = np.array(r["l2"]) / np.array(res["fp64"]["l2"])
+                w = int(np.argmax(ratio))
                 l2 = {"batched_fp32_over_fp64_max": float(ratio.max()),
                       "batched_fp32_over_fp64_median": float(np.median(ratio)),
                       "batched_fp64_l2_rho_median": float(np.median(res["fp64"]["l2"])),
+                      "solves_over_1.05": int((ratio > 1.05).sum()),
+                      "worst": {"triangles": r["tris"][w], "order": r["orders"][w],
+                                "fp64_l2_rho": float(res["fp64"]["l2"][w]),
+                                "fp32_l2_rho": float(r["l2"][w])},
                       "steps": 200}
             if plain and plain.get("fp64", {}).get("l2"):
                 l2 = dict(l2 or {})

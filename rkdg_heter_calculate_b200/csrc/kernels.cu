@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <type_traits>
 
 #include "rkdg_internal.hpp"
 
@@ -44,6 +45,45 @@ struct Tab {
 constexpr int kNumCfg = 6;
 __constant__ Tab<double> c_tab_d[kNumCfg];
 __constant__ Tab<float> c_tab_f[kNumCfg];
+
+// FP32 tables with every value in both lanes of a pair, for the packed
+// two-lane FP32 arithmetic (f32x2) of the tile kernel; nephiw = -(2 w_g psi_i).
+struct Tab2 {
+    float2 vphi[kMaxNQ][kMaxNB];
+    float2 vdxi[kMaxNQ][kMaxNB];
+    float2 veta[kMaxNQ][kMaxNB];
+    float2 ephi[3][kMaxNG][kMaxNB];
+    float2 nephiw[3][kMaxNG][kMaxNB];
+};
+__constant__ Tab2 c_tab_f2[kNumCfg];
+
+// Two-lane FP32 arithmetic (PTX fma/mul/add/sub .f32x2, sm_100a): each lane
+// is the IEEE single-precision operation of the scalar form, rounded once
+// per lane, so the results equal the scalar code's bit for bit.
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) {
+    float2 r;
+    asm("{\n .reg .b64 a, b, c, d;\n mov.b64 a, {%2, %3};\n mov.b64 b, {%4, %5};\n mov.b64 c, {%6, %7};\n"
+        " fma.rn.f32x2 d, a, b, c;\n mov.b64 {%0, %1}, d;\n}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) {
+    float2 r;
+    asm("{\n .reg .b64 a, b, d;\n mov.b64 a, {%2, %3};\n mov.b64 b, {%4, %5};\n"
+        " mul.rn.f32x2 d, a, b;\n mov.b64 {%0, %1}, d;\n}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) {
+    float2 r;
+    asm("{\n .reg .b64 a, b, d;\n mov.b64 a, {%2, %3};\n mov.b64 b, {%4, %5};\n"
+        " sub.rn.f32x2 d, a, b;\n mov.b64 {%0, %1}, d;\n}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
 
 __host__ __device__ constexpr int cfg_index(int nq, int ng) {
     return 2 * (nq == 7 ? 0 : (nq == 6 ? 1 : 2)) + (ng == 3 ? 0 : 1);
@@ -98,9 +138,24 @@ void upload_tables(int nq, int ng) {
             d.minv[j][k] = t.minv[j][k];
             f.minv[j][k] = (float)t.minv[j][k];
         }
+    Tab2 f2{};
+    auto dup = [](double x) { return make_float2((float)x, (float)x); };
+    for (int q = 0; q < kMaxNQ; ++q)
+        for (int i = 0; i < kMaxNB; ++i) {
+            f2.vphi[q][i] = dup(t.vphi[q][i]);
+            f2.vdxi[q][i] = dup(t.vdxi_w[q][i]);
+            f2.veta[q][i] = dup(t.veta_w[q][i]);
+        }
+    for (int k = 0; k < 3; ++k)
+        for (int g = 0; g < kMaxNG; ++g)
+            for (int i = 0; i < kMaxNB; ++i) {
+                f2.ephi[k][g][i] = dup(t.ephi[k][g][i]);
+                f2.nephiw[k][g][i] = make_float2(-f.ephiw[k][g][i], -f.ephiw[k][g][i]);
+            }
     const int c = cfg_index(nq, ng);
     RKDG_CUDA_TRY(cudaMemcpyToSymbol(c_tab_d, &d, sizeof(d), sizeof(d) * c));
     RKDG_CUDA_TRY(cudaMemcpyToSymbol(c_tab_f, &f, sizeof(f), sizeof(f) * c));
+    RKDG_CUDA_TRY(cudaMemcpyToSymbol(c_tab_f2, &f2, sizeof(f2), sizeof(f2) * c));
 }
 
 // --------------------------------------------------------- state packs --

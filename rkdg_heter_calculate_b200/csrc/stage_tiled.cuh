@@ -134,6 +134,32 @@ __device__ __forceinline__ void get4(const Vec4<Real>* p, Real a[4]) {
     const Vec4<Real> t = *p;
     a[0] = t.x, a[1] = t.y, a[2] = t.z, a[3] = t.w;
 }
+// Per-element linear algebra on 4-vectors (the conservative components).
+// FP32 runs it in lane pairs (components 0-1 and 2-3) with the f32x2
+// helpers and the paired tables; FP64 runs the scalar form.  Both round
+// each product-sum exactly as the scalar form does.
+__device__ __forceinline__ float2 lo2(const float a[4]) { return make_float2(a[0], a[1]); }
+__device__ __forceinline__ float2 hi2(const float a[4]) { return make_float2(a[2], a[3]); }
+__device__ __forceinline__ void set4(float a[4], float2 l, float2 h) { a[0] = l.x, a[1] = l.y, a[2] = h.x, a[3] = h.y; }
+// out = c + sum_{i >= 1} tab[i] u_i
+template <int NB>
+__device__ __forceinline__ void comb_rows(const float2* tab, const float u[NB][4], float2 cl, float2 ch,
+                                          float out[4]) {
+#pragma unroll
+    for (int i = 1; i < NB; ++i) {
+        cl = f2fma(tab[i], lo2(u[i]), cl);
+        ch = f2fma(tab[i], hi2(u[i]), ch);
+    }
+    set4(out, cl, ch);
+}
+// R_i += f tab[i] for i >= I0
+template <int I0, int NB>
+__device__ __forceinline__ void acc_rows(float R[NB][4], const float f[4], const float2* tab) {
+    const float2 fl = lo2(f), fh = hi2(f);
+#pragma unroll
+    for (int i = I0; i < NB; ++i) set4(R[i], f2fma(fl, tab[i], lo2(R[i])), f2fma(fh, tab[i], hi2(R[i])));
+}
+
 template <typename Real>
 struct TiledLayout {
     // edge normals per element: FP32 (Nx, Ny) per edge, the length formed
@@ -268,10 +294,14 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     constexpr bool HALO_IN_STAGING = TiledSmem<Real, 3, FLUX>::HALO_IN_STAGING;
     V4* s_htr = HALO_IN_STAGING ? reinterpret_cast<V4*>(stg) : s_mean + MEANS * BT;
     V4* s_hmean = s_htr + NG * HM;
-    __shared__ Real s_ephi[3][NG][NB];
+    constexpr bool PK = sizeof(Real) == 4;  // FP32: lane-pair arithmetic, paired tables
+    const Tab2& t2 = c_tab_f2[CFG];
+    using SE = typename std::conditional<PK, float2, Real>::type;
+    __shared__ SE s_ephi[3][NG][NB];  // neighbour-side edge table (runtime edge index)
     for (int x = threadIdx.x; x < 3 * NG * NB; x += BT) {
         int k = x / (NG * NB), g = (x / NB) % NG, i = x % NB;
-        s_ephi[k][g][i] = tb.ephi[k][g][i];
+        if constexpr (PK) s_ephi[k][g][i] = t2.ephi[k][g][i];
+        else s_ephi[k][g][i] = tb.ephi[k][g][i];
     }
     const int sid = d0.z;
     StepCtl* ctl = a.ctl + sid;
@@ -378,8 +408,13 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 #pragma unroll
             for (int v = 0; v < 4; ++v) R[i][v] = Real(0);
         Real c0[4];
+        if constexpr (PK) {
+            const float2 kk = make_float2(k00, k00);
+            set4(c0, f2mul(kk, lo2(u[0])), f2mul(kk, hi2(u[0])));
+        } else {
 #pragma unroll
-        for (int v = 0; v < 4; ++v) c0[v] = k00 * u[0][v];
+            for (int v = 0; v < 4; ++v) c0[v] = k00 * u[0][v];
+        }
         // FP32: the quadrature loop stays rolled (a smaller body keeps the
         // instruction cache warm across the CTAs on an SM; 3 % faster);
         // FP64 unrolls it.  Each product is its own fused multiply-add, and
@@ -388,12 +423,16 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 #pragma unroll VOL_UNROLL
         for (int q = 0; q < NQ; ++q) {
             Real w[4];
+            if constexpr (PK) {
+                comb_rows<NB>(t2.vphi[q], u, lo2(c0), hi2(c0), w);
+            } else {
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                Real s = c0[v];
+                for (int v = 0; v < 4; ++v) {
+                    Real s = c0[v];
 #pragma unroll
-                for (int i = 1; i < NB; ++i) s += tb.vphi[q][i] * u[i][v];
-                w[v] = s;
+                    for (int i = 1; i < NB; ++i) s += tb.vphi[q][i] * u[i][v];
+                    w[v] = s;
+                }
             }
             Real fx[4], fy[4];
             if constexpr (DEV) {
@@ -413,12 +452,17 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                     fy[v] = j10 * F[v] + j11 * G[v];
                 }
             }
+            if constexpr (PK) {
+                acc_rows<1, NB>(R, fx, t2.vdxi[q]);
+                acc_rows<2, NB>(R, fy, t2.veta[q]);
+            } else {
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
+                for (int v = 0; v < 4; ++v) {
 #pragma unroll
-                for (int i = 1; i < NB; ++i) R[i][v] += fx[v] * tb.vdxi[q][i];
+                    for (int i = 1; i < NB; ++i) R[i][v] += fx[v] * tb.vdxi[q][i];
 #pragma unroll
-                for (int i = 2; i < NB; ++i) R[i][v] += fy[v] * tb.veta[q][i];
+                    for (int i = 2; i < NB; ++i) R[i][v] += fy[v] * tb.veta[q][i];
+                }
             }
         }
 #pragma unroll
@@ -426,12 +470,16 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 #pragma unroll
             for (int g = 0; g < NG; ++g) {
                 Real t[4];
+                if constexpr (PK) {
+                    comb_rows<NB>(t2.ephi[k][g], u, lo2(c0), hi2(c0), t);
+                } else {
 #pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    Real s = c0[v];
+                    for (int v = 0; v < 4; ++v) {
+                        Real s = c0[v];
 #pragma unroll
-                    for (int i = 1; i < NB; ++i) s += tb.ephi[k][g][i] * u[i][v];
-                    t[v] = s;
+                        for (int i = 1; i < NB; ++i) s += tb.ephi[k][g][i] * u[i][v];
+                        t[v] = s;
+                    }
                 }
                 put4(s_tr + (k * NG + g) * BT + tid, t);
             }
@@ -474,17 +522,26 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                 }
                 const int he = hh[r].y;
                 Real c0[4];
+                if constexpr (PK) {
+                    const float2 kk = make_float2(k00, k00);
+                    set4(c0, f2mul(kk, lo2(un[0])), f2mul(kk, hi2(un[0])));
+                } else {
 #pragma unroll
-                for (int v = 0; v < 4; ++v) c0[v] = k00 * un[0][v];
+                    for (int v = 0; v < 4; ++v) c0[v] = k00 * un[0][v];
+                }
 #pragma unroll
                 for (int g = 0; g < NG; ++g) {
                     Real t[4];
+                    if constexpr (PK) {
+                        comb_rows<NB>(s_ephi[he][g], un, lo2(c0), hi2(c0), t);
+                    } else {
 #pragma unroll
-                    for (int v = 0; v < 4; ++v) {
-                        Real s = c0[v];
+                        for (int v = 0; v < 4; ++v) {
+                            Real s = c0[v];
 #pragma unroll
-                        for (int i = 1; i < NB; ++i) s += s_ephi[he][g][i] * un[i][v];
-                        t[v] = s;
+                            for (int i = 1; i < NB; ++i) s += s_ephi[he][g][i] * un[i][v];
+                            t[v] = s;
+                        }
                     }
                     put4(s_htr + g * HM + h, t);
                 }
@@ -595,10 +652,14 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
         for (int g = 0; g < NG; ++g) {
             Real f[4];
             get4(s_tr + (k * NG + g) * BT + tid, f);
+            if constexpr (PK) {
+                acc_rows<0, NB>(R, f, t2.nephiw[k][g]);
+            } else {
 #pragma unroll
-            for (int v = 0; v < 4; ++v)
+                for (int v = 0; v < 4; ++v)
 #pragma unroll
-                for (int i = 0; i < NB; ++i) R[i][v] -= f[v] * tb.ephiw[k][g][i];
+                    for (int i = 0; i < NB; ++i) R[i][v] -= f[v] * tb.ephiw[k][g][i];
+            }
         }
 
     Real* __restrict__ Uout = static_cast<Real*>(a.Unew);
@@ -622,17 +683,32 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
         if (a.U0 != nullptr) {
             Real u0[NB][4];
             load_state<Real, NB>(static_cast<const Real*>(a.U0), a.ld, ee, u0);
+            if constexpr (PK) {
+                const float2 dt2 = make_float2(dt, dt), cb2 = make_float2(cb, cb);
 #pragma unroll
-            for (int i = 0; i < NB; ++i)
+                for (int i = 0; i < NB; ++i)
+                    set4(R[i], f2fma(cb2, f2fma(dt2, lo2(R[i]), f2sub(lo2(u[i]), lo2(u0[i]))), lo2(u0[i])),
+                         f2fma(cb2, f2fma(dt2, hi2(R[i]), f2sub(hi2(u[i]), hi2(u0[i]))), hi2(u0[i])));
+            } else {
 #pragma unroll
-                for (int v = 0; v < 4; ++v) R[i][v] = u0[i][v] + cb * ((u[i][v] - u0[i][v]) + dt * R[i][v]);
+                for (int i = 0; i < NB; ++i)
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) R[i][v] = u0[i][v] + cb * ((u[i][v] - u0[i][v]) + dt * R[i][v]);
+            }
 #pragma unroll
             for (int v = 0; v < 4; ++v) u0m[v] = u0[0][v];
         } else {
+            if constexpr (PK) {
+                const float2 dt2 = make_float2(dt, dt), cb2 = make_float2(cb, cb);
 #pragma unroll
-            for (int i = 0; i < NB; ++i)
+                for (int i = 0; i < NB; ++i)
+                    set4(R[i], f2mul(cb2, f2fma(dt2, lo2(R[i]), lo2(u[i]))), f2mul(cb2, f2fma(dt2, hi2(R[i]), hi2(u[i]))));
+            } else {
 #pragma unroll
-                for (int v = 0; v < 4; ++v) R[i][v] = cb * (u[i][v] + dt * R[i][v]);
+                for (int i = 0; i < NB; ++i)
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) R[i][v] = cb * (u[i][v] + dt * R[i][v]);
+            }
         }
     }
     if (active) store_state<Real, NB>(Uout, a.ld, e, R);
