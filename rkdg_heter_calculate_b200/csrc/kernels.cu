@@ -57,9 +57,10 @@ struct Tab2 {
 };
 __constant__ Tab2 c_tab_f2[kNumCfg];
 
-// Two-lane FP32 arithmetic (PTX fma/mul/add/sub .f32x2, sm_100a): each lane
-// is the IEEE single-precision operation of the scalar form, rounded once
-// per lane, so the results equal the scalar code's bit for bit.
+// Two-lane FP32 arithmetic (PTX fma/mul/sub .f32x2, sm_100a): each lane is
+// one IEEE single-precision operation (a fused multiply-add rounds once).
+// The pairing fixes the order of operations; a scalar build may contract a
+// sum of products differently and so differ in the last bit.
 __device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) {
     float2 r;
     asm("{\n .reg .b64 a, b, c, d;\n mov.b64 a, {%2, %3};\n mov.b64 b, {%4, %5};\n mov.b64 c, {%6, %7};\n"

@@ -136,8 +136,9 @@ __device__ __forceinline__ void get4(const Vec4<Real>* p, Real a[4]) {
 }
 // Per-element linear algebra on 4-vectors (the conservative components).
 // FP32 runs it in lane pairs (components 0-1 and 2-3) with the f32x2
-// helpers and the paired tables; FP64 runs the scalar form.  Both round
-// each product-sum exactly as the scalar form does.
+// helpers and the paired tables; FP64 runs the scalar form.  (Pairing the
+// two sides of the HLLC flux the same way executed fewer instructions but
+// more register moves and ran slower.)
 __device__ __forceinline__ float2 lo2(const float a[4]) { return make_float2(a[0], a[1]); }
 __device__ __forceinline__ float2 hi2(const float a[4]) { return make_float2(a[2], a[3]); }
 __device__ __forceinline__ void set4(float a[4], float2 l, float2 h) { a[0] = l.x, a[1] = l.y, a[2] = h.x, a[3] = h.y; }
