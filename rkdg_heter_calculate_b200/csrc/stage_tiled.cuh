@@ -416,11 +416,12 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 #pragma unroll
             for (int v = 0; v < 4; ++v) c0[v] = k00 * u[0][v];
         }
-        // FP32: the quadrature loop stays rolled (a smaller body keeps the
-        // instruction cache warm across the CTAs on an SM; 3 % faster);
-        // FP64 unrolls it.  Each product is its own fused multiply-add, and
-        // psi_1 (a function of xi alone) has no eta-derivative term.
-        constexpr int VOL_UNROLL = sizeof(Real) == 4 ? 1 : NQ;
+        // FP32: the quadrature loop is unrolled by two only (a smaller body
+        // keeps the instruction cache warm across the CTAs on an SM; full
+        // unrolling is 2 % slower, none 1 %); FP64 unrolls it.  Each product
+        // is its own fused multiply-add, and psi_1 (a function of xi alone)
+        // has no eta-derivative term.
+        constexpr int VOL_UNROLL = sizeof(Real) == 4 ? 2 : NQ;
 #pragma unroll VOL_UNROLL
         for (int q = 0; q < NQ; ++q) {
             Real w[4];
