@@ -57,7 +57,7 @@ struct Tab2 {
 };
 __constant__ Tab2 c_tab_f2[kNumCfg];
 
-// Two-lane FP32 arithmetic (PTX fma/mul/sub .f32x2, sm_100a): each lane is
+// Two-lane FP32 arithmetic (PTX fma/mul/add/sub .f32x2, sm_100a): each lane is
 // one IEEE single-precision operation (a fused multiply-add rounds once).
 // The pairing fixes the order of operations; a scalar build may contract a
 // sum of products differently and so differ in the last bit.
@@ -73,6 +73,14 @@ __device__ __forceinline__ float2 f2mul(float2 a, float2 b) {
     float2 r;
     asm("{\n .reg .b64 a, b, d;\n mov.b64 a, {%2, %3};\n mov.b64 b, {%4, %5};\n"
         " mul.rn.f32x2 d, a, b;\n mov.b64 {%0, %1}, d;\n}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) {
+    float2 r;
+    asm("{\n .reg .b64 a, b, d;\n mov.b64 a, {%2, %3};\n mov.b64 b, {%4, %5};\n"
+        " add.rn.f32x2 d, a, b;\n mov.b64 {%0, %1}, d;\n}"
         : "=f"(r.x), "=f"(r.y)
         : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
     return r;
@@ -423,8 +431,17 @@ __device__ __forceinline__ void hllc_dev(const Real dL[4], const Real dR[4], Rea
     const Real UK[4] = {r.rho + (left ? dL[0] : dR[0]), r.mx + (left ? dL[1] : dR[1]),
                         r.my + (left ? dL[2] : dR[2]), r.E + (left ? dL[3] : dR[3])};
     const Real ex[4] = {Real(0), k * nx, k * ny, k * SM + p};
+    if constexpr (sizeof(Real) == 4) {  // by component pairs, as the scalar form
+        const float2 cc = make_float2(c, c);
+        const float2 e01 = f2add(make_float2(UK[0], UK[1]), make_float2(ex[0], ex[1]));
+        const float2 e23 = f2add(make_float2(UK[2], UK[3]), make_float2(ex[2], ex[3]));
+        const float2 r01 = f2fma(cc, e01, make_float2(left ? FL[0] : FR[0], left ? FL[1] : FR[1]));
+        const float2 r23 = f2fma(cc, e23, make_float2(left ? FL[2] : FR[2], left ? FL[3] : FR[3]));
+        f[0] = r01.x, f[1] = r01.y, f[2] = r23.x, f[3] = r23.y;
+    } else {
 #pragma unroll
-    for (int v = 0; v < 4; ++v) f[v] = (left ? FL[v] : FR[v]) + c * (UK[v] + ex[v]);
+        for (int v = 0; v < 4; ++v) f[v] = (left ? FL[v] : FR[v]) + c * (UK[v] + ex[v]);
+    }
 }
 
 // ---------------------------------------------------------- reductions --

@@ -616,20 +616,35 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                         normal_flux<Real>(uL, Nx, Ny, gm1, fL, pL);
                         normal_flux<Real>(uR, Nx, Ny, gm1, fR, pR);
                     }
+                    if constexpr (PK) {
+                        const float2 na = make_float2(-alpha, -alpha);
+                        const float2 tl = f2fma(na, f2sub(lo2(uR), lo2(uL)), f2add(lo2(fL), lo2(fR)));
+                        const float2 th = f2fma(na, f2sub(hi2(uR), hi2(uL)), f2add(hi2(fL), hi2(fR)));
+                        const float2 hp = make_float2(0.5f, 0.5f), hn = make_float2(-0.5f, -0.5f);
+                        set4(fh, f2mul(hp, tl), f2mul(hp, th));
+                        set4(fn, f2mul(hn, tl), f2mul(hn, th));
+                    } else {
 #pragma unroll
-                    for (int v = 0; v < 4; ++v) {
-                        const Real t = fL[v] + fR[v] - alpha * (uR[v] - uL[v]);
-                        fh[v] = Real(0.5) * t;
-                        fn[v] = Real(-0.5) * t;
+                        for (int v = 0; v < 4; ++v) {
+                            const Real t = fL[v] + fR[v] - alpha * (uR[v] - uL[v]);
+                            fh[v] = Real(0.5) * t;
+                            fn[v] = Real(-0.5) * t;
+                        }
                     }
                 } else {
                     Real f[4];
                     if constexpr (DEV) hllc_dev<Real>(uL, uR, nx, ny, gamma, rs, f);
                     else hllc<Real>(uL, uR, nx, ny, gamma, f);
+                    if constexpr (PK) {
+                        const float2 l = make_float2(len, len), nl = make_float2(-len, -len);
+                        set4(fh, f2mul(lo2(f), l), f2mul(hi2(f), l));
+                        set4(fn, f2mul(lo2(f), nl), f2mul(hi2(f), nl));
+                    } else {
 #pragma unroll
-                    for (int v = 0; v < 4; ++v) {
-                        fh[v] = f[v] * len;
-                        fn[v] = f[v] * -len;
+                        for (int v = 0; v < 4; ++v) {
+                            fh[v] = f[v] * len;
+                            fn[v] = f[v] * -len;
+                        }
                     }
                 }
                 // each slot of an edge is read by this task alone: the
