@@ -272,11 +272,74 @@ __device__ __forceinline__ void load_staged(const unsigned char* stg, int x, Rea
 #define RKDG_HOLD_STATE 0
 #endif
 
+// The part of a tile's work that needs only its descriptors, J^-1 rows and
+// edge codes: edge normals and codes into shared memory, the solve's
+// reference state, the halo and task list entries.  Formed while the tile's
+// state rows are still in flight.
+template <typename Real>
+struct TilePre {
+    RefState<Real> rs;
+    Real inv_area, j00, j01, j10, j11;  // 1 / area; rows of 2 area J^-1
+    double det;                         // det J^-1 = 1 / (2 area)
+    int2 hh[3];
+    uint16_t tk[3];
+};
+template <typename Real>
+__device__ __forceinline__ TilePre<Real> tile_pre(const StageArgs& a, const TileArgs& ta, const int4 d0,
+                                                  const int4 d1, const double2 r0, const double2 r1,
+                                                  const int4 code, unsigned char* smem_raw) {
+    constexpr int BT = kTile, NC = TiledLayout<Real>::NC;
+    const int tid = threadIdx.x;
+    TilePre<Real> t;
+    // far-field / reference state by value (a pointer into the parameter
+    // block would put the parameter array in local memory)
+    double fs[4];
+    if (a.far_sid) {
+        const double* p = a.far_sid + 4 * d0.z;
+        fs[0] = p[0], fs[1] = p[1], fs[2] = p[2], fs[3] = p[3];
+    } else {
+        fs[0] = a.far[0], fs[1] = a.far[1], fs[2] = a.far[2], fs[3] = a.far[3];
+    }
+    t.rs = ref_state<Real>(fs, a.gamma);
+    // the halo and task lists (L2 hits: prefetched with the tile's rows)
+    const int h0 = d1.x, nh = d1.y, t0 = d1.z, nt = d1.w;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const int h = tid + r * BT;
+        t.hh[r] = h < nh ? __ldg(ta.halo + h0 + h) : make_int2(0, 0);
+        t.tk[r] = h < nt ? __ldg(ta.task + t0 + h) : (uint16_t)0;
+    }
+    reinterpret_cast<int4*>(smem_raw + TiledLayout<Real>::code_off)[tid] = code;
+    // edge normals N_k (length = edge length; N_k / area = 2(r0 + r1), -2 r0,
+    // -2 r1) from the FP64 J^-1 rows, kept in the working precision.  The
+    // residual is accumulated scaled by 2 area (= 1 / det J^-1): the volume
+    // term through 2 area J^-1 = (-N_1; -N_2), the surface term through the
+    // table 2 w_g psi_i, and the factor det J^-1 applied once in the update.
+    Real* s_nrm = reinterpret_cast<Real*>(smem_raw);  // [3][NC][BT] Nx, Ny (, len)
+    t.det = r0.x * r1.y - r0.y * r1.x;
+    t.inv_area = (Real)(2.0 * t.det);
+    // FP64 forms them in FP64; FP32 from the rounded J^-1 rows (a few ulp,
+    // without the FP64 reciprocal)
+    const Real area2 = rcp_((Real)t.det);
+    const Real ax = (Real)r0.x, ay = (Real)r0.y, bx = (Real)r1.x, by = (Real)r1.y;
+    const Real cx[3] = {ax + bx, -ax, -bx}, cy[3] = {ay + by, -ay, -by};
+    Real Nx[3], Ny[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        Nx[k] = cx[k] * area2, Ny[k] = cy[k] * area2;
+        s_nrm[(NC * k + 0) * BT + tid] = Nx[k];
+        s_nrm[(NC * k + 1) * BT + tid] = Ny[k];
+        if constexpr (NC == 3) s_nrm[(NC * k + 2) * BT + tid] = sqrt_(Nx[k] * Nx[k] + Ny[k] * Ny[k]);
+    }
+    t.j00 = -Nx[1], t.j01 = -Ny[1], t.j10 = -Nx[2], t.j11 = -Ny[2];
+    return t;
+}
+
 template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE>
 __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& ta, const int4 d0,
                                            const int4 d1, unsigned char* smem_raw, unsigned char* stg,
-                                           const int nxt, const int ntiles, uint64_t* bar, const double2 r0,
-                                           const double2 r1, const int4 code, Real (*s_red)[3]) {
+                                           const int nxt, const int ntiles, uint64_t* bar,
+                                           const TilePre<Real>& pre, Real (*s_red)[3]) {
     constexpr int CFG = cfg_index(NQ, NG);
     constexpr int BT = kTile;
     constexpr bool HOLD = RKDG_HOLD_STATE && sizeof(Real) == 4;
@@ -315,64 +378,24 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     const int sx = active ? tid : 0;  // staging row index
     const Real* __restrict__ U = static_cast<const Real*>(a.U);
     const Real gamma = (Real)a.gamma, gm1 = gamma - Real(1);
-    // far-field / reference state by value (a pointer into the parameter
-    // block would put the parameter array in local memory)
-    double fs[4];
-    if (a.far_sid) {
-        const double* p = a.far_sid + 4 * sid;
-        fs[0] = p[0], fs[1] = p[1], fs[2] = p[2], fs[3] = p[3];
-    } else {
-        fs[0] = a.far[0], fs[1] = a.far[1], fs[2] = a.far[2], fs[3] = a.far[3];
-    }
-    const Real far[4] = {(Real)fs[0], (Real)fs[1], (Real)fs[2], (Real)fs[3]};
     // FP32: traces and fluxes in deviation form about the reference state
     constexpr bool DEV = stores_deviation<Real>();
-    const RefState<Real> rs = ref_state<Real>(fs, a.gamma);
+    const RefState<Real> rs = pre.rs;
+    const Real far[4] = {rs.rho, rs.mx, rs.my, rs.E};
+    Real refv[4];  // the offset of a stored mean (FP32: the far field)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) refv[v] = DEV ? far[v] : Real(0);
 
     // ------------------------------------------------------------ phase A
-    // the halo and task lists first (L2 hits: prefetched with the tile's
-    // rows); their latency runs under the staged reads
     constexpr int SR = NB * (int)(sizeof(Real) / 4);  // 16-byte rows of a state
-    const int h0 = d1.x, nh = d1.y, t0 = d1.z, nt = d1.w;
-    int2 hh[3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-        const int h = tid + r * BT;
-        hh[r] = h < nh ? __ldg(ta.halo + h0 + h) : make_int2(0, 0);
-    }
-    uint16_t tk[3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-        const int j = tid + r * BT;
-        tk[r] = j < nt ? __ldg(ta.task + t0 + j) : (uint16_t)0;
-    }
+    const int nh = d1.y, nt = d1.w;
+    const int2* hh = pre.hh;
+    const uint16_t* tk = pre.tk;
     Real R[NB][4];
     Real u[NB][4];
-    s_code[tid] = code;
-    // edge normals N_k (length = edge length; N_k / area = 2(r0 + r1), -2 r0,
-    // -2 r1) from the FP64 J^-1 rows, kept in the working precision.  The
-    // residual is accumulated scaled by 2 area (= 1 / det J^-1): the volume
-    // term through 2 area J^-1 = (-N_1; -N_2), the surface term through the
-    // table 2 w_g psi_i, and the factor det J^-1 applied once in the update.
-    const double det = r0.x * r1.y - r0.y * r1.x;  // 1 / (2 area)
-    const Real inv_area = (Real)(2.0 * det);
-    Real j00, j01, j10, j11;  // rows of 2 area J^-1
-    {
-        // FP64 forms them in FP64; FP32 from the rounded J^-1 rows (a few
-        // ulp, without the FP64 reciprocal)
-        const Real area2 = rcp_((Real)det);
-        const Real ax = (Real)r0.x, ay = (Real)r0.y, bx = (Real)r1.x, by = (Real)r1.y;
-        const Real cx[3] = {ax + bx, -ax, -bx}, cy[3] = {ay + by, -ay, -by};
-        Real Nx[3], Ny[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            Nx[k] = cx[k] * area2, Ny[k] = cy[k] * area2;
-            s_nrm[(NC * k + 0) * BT + tid] = Nx[k];
-            s_nrm[(NC * k + 1) * BT + tid] = Ny[k];
-            if constexpr (NC == 3) s_nrm[(NC * k + 2) * BT + tid] = sqrt_(Nx[k] * Nx[k] + Ny[k] * Ny[k]);
-        }
-        j00 = -Nx[1], j01 = -Ny[1], j10 = -Nx[2], j11 = -Ny[2];
-    }
+    const double det = pre.det;
+    const Real inv_area = pre.inv_area;
+    const Real j00 = pre.j00, j01 = pre.j01, j10 = pre.j10, j11 = pre.j11;  // rows of 2 area J^-1
     Real m_st[4];  // the stored cell mean (a deviation in FP32)
     // psi_0 is the constant K00 at every volume and edge point: its term is
     // formed once per state
@@ -399,7 +422,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
                 m_st[v] = u[0][v];
-                mfull[v] = u[0][v] + ref_of<Real>(fs, v);  // the cell mean itself
+                mfull[v] = u[0][v] + refv[v];  // the cell mean itself
                 if constexpr (!DEV) u[0][v] = mfull[v];
             }
             if constexpr (MEANS) put4(s_mean + tid, mfull);
@@ -517,7 +540,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                     Real mfull[4];
 #pragma unroll
                     for (int v = 0; v < 4; ++v) {
-                        mfull[v] = un[0][v] + ref_of<Real>(fs, v);
+                        mfull[v] = un[0][v] + refv[v];
                         if constexpr (!DEV) un[0][v] = mfull[v];
                     }
                     if constexpr (MEANS) put4(s_hmean + h, mfull);
@@ -741,7 +764,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
             bool bad;
             Real m[4], len[3];
 #pragma unroll
-            for (int v = 0; v < 4; ++v) m[v] = R[0][v] + ref_of<Real>(fs, v);
+            for (int v = 0; v < 4; ++v) m[v] = R[0][v] + refv[v];
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const Real Nx = s_nrm[(NC * k + 0) * BT + tid], Ny = s_nrm[(NC * k + 1) * BT + tid];
@@ -815,10 +838,12 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
     for (; tile < ntiles; tile += gridDim.x) {
         const int4 d0 = __ldg(ta.desc + 2 * tile), d1 = __ldg(ta.desc + 2 * tile + 1);
         const int nxt = tile + gridDim.x;
-        // this thread's J^-1 rows and edge codes (L2 hits), under the wait
+        // this thread's J^-1 rows and edge codes, and the work that needs
+        // only them, while the state rows arrive
         const int ex = d0.x + ((int)threadIdx.x < d0.y ? (int)threadIdx.x : 0);
         const double2 r0 = __ldg(jinv2 + ex), r1 = __ldg(jinv2 + a.ld + ex);
         const int4 code = __ldg(ta.code + ex);
+        const TilePre<Real> pre = tile_pre<Real>(a, ta, d0, d1, r0, r1, code, smem_raw);
         const bool ok = mbar_wait(&s_bar, parity);
         if (__syncthreads_or(!ok)) {  // also: every thread has seen this phase complete
             if (threadIdx.x == 0) atomicOr(&a.ctl[d0.z].error, 2);
@@ -830,11 +855,9 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
             continue;
         }
         if (ORD == 2 || (ORD == 3 && d0.w == 2))
-            tile_stage<Real, 6, NQ2, 3, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, r0, r1, code,
-                                                   s_red);
+            tile_stage<Real, 6, NQ2, 3, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre, s_red);
         else
-            tile_stage<Real, 3, 3, 2, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, r0, r1, code,
-                                                 s_red);
+            tile_stage<Real, 3, 3, 2, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre, s_red);
         __syncthreads();  // shared memory is reused by the next tile
         if (MODE == MODE_STAGE && a.last_stage && threadIdx.x == 0) tile_maxima_atomic<Real>(a, a.ctl + d0.z, s_red);
     }
