@@ -843,6 +843,7 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
         const int ex = d0.x + ((int)threadIdx.x < d0.y ? (int)threadIdx.x : 0);
         const double2 r0 = __ldg(jinv2 + ex), r1 = __ldg(jinv2 + a.ld + ex);
         const int4 code = __ldg(ta.code + ex);
+        const int done = MODE == MODE_STAGE ? a.ctl[d0.z].done : 0;
         const TilePre<Real> pre = tile_pre<Real>(a, ta, d0, d1, r0, r1, code, smem_raw);
         const bool ok = mbar_wait(&s_bar, parity);
         if (__syncthreads_or(!ok)) {  // also: every thread has seen this phase complete
@@ -850,7 +851,7 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
             return;
         }
         parity ^= 1u;
-        if (MODE == MODE_STAGE && a.ctl[d0.z].done) {  // finished solve: pass the tile on
+        if (done) {  // finished solve: pass the tile on
             if (threadIdx.x == 0 && nxt < ntiles) stage_copy<Real>(a, __ldg(ta.desc + 2 * nxt), stg, &s_bar);
             continue;
         }
