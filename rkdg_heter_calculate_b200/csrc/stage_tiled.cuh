@@ -339,7 +339,7 @@ template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE>
 __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& ta, const int4 d0,
                                            const int4 d1, unsigned char* smem_raw, unsigned char* stg,
                                            const int nxt, const int ntiles, uint64_t* bar,
-                                           const TilePre<Real>& pre, Real (*s_red)[3]) {
+                                           const TilePre<Real>& pre, Real (*s_red)[3], const double* s_dt) {
     constexpr int CFG = cfg_index(NQ, NG);
     constexpr int BT = kTile;
     constexpr bool HOLD = RKDG_HOLD_STATE && sizeof(Real) == 4;
@@ -712,7 +712,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
         if (active) store_state<Real, NB>(Uout, a.ld, e, R);
         return;
     }
-    const double dtd = ctl->dt;
+    const double dtd = *s_dt;
     // a U^n + b (U + dt L) as U^n + b ((U - U^n) + dt L): a + b = 1 holds
     // exactly (1/3 and 2/3 both round up in FP32, and a scale of 1 + 3e-8
     // per step would accumulate into the state); L = det J^-1 R
@@ -820,6 +820,7 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t s_bar;
     __shared__ Real s_red[kTile / 32][3];  // per-warp maxima of a last stage
+    __shared__ double s_dt;                // the tile's solve's dt (read before the staging wait)
     unsigned char* stg = smem_raw + SM::stage_offset(ta.max_halo);
     const int ntiles = ta.ntiles_dev ? *ta.ntiles_dev : ta.ntiles;
     int tile = blockIdx.x;
@@ -844,6 +845,7 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
         const double2 r0 = __ldg(jinv2 + ex), r1 = __ldg(jinv2 + a.ld + ex);
         const int4 code = __ldg(ta.code + ex);
         const int done = MODE == MODE_STAGE ? a.ctl[d0.z].done : 0;
+        if (MODE == MODE_STAGE && threadIdx.x == 0) s_dt = a.ctl[d0.z].dt;
         const TilePre<Real> pre = tile_pre<Real>(a, ta, d0, d1, r0, r1, code, smem_raw);
         const bool ok = mbar_wait(&s_bar, parity);
         if (__syncthreads_or(!ok)) {  // also: every thread has seen this phase complete
@@ -856,9 +858,11 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
             continue;
         }
         if (ORD == 2 || (ORD == 3 && d0.w == 2))
-            tile_stage<Real, 6, NQ2, 3, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre, s_red);
+            tile_stage<Real, 6, NQ2, 3, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre, s_red,
+                                                   &s_dt);
         else
-            tile_stage<Real, 3, 3, 2, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre, s_red);
+            tile_stage<Real, 3, 3, 2, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre, s_red,
+                                                 &s_dt);
         __syncthreads();  // shared memory is reused by the next tile
         if (MODE == MODE_STAGE && a.last_stage && threadIdx.x == 0) tile_maxima_atomic<Real>(a, a.ctl + d0.z, s_red);
     }
