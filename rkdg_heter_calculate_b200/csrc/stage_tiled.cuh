@@ -282,7 +282,6 @@ struct TilePre {
     Real inv_area, j00, j01, j10, j11;  // 1 / area; rows of 2 area J^-1
     double det;                         // det J^-1 = 1 / (2 area)
     int2 hh[3];
-    uint16_t tk[3];
 };
 template <typename Real>
 __device__ __forceinline__ TilePre<Real> tile_pre(const StageArgs& a, const TileArgs& ta, const int4 d0,
@@ -303,13 +302,16 @@ __device__ __forceinline__ TilePre<Real> tile_pre(const StageArgs& a, const Tile
     t.rs = ref_state<Real>(fs, a.gamma);
     // the halo and task lists (L2 hits: prefetched with the tile's rows)
     const int h0 = d1.x, nh = d1.y, t0 = d1.z, nt = d1.w;
+    int4* s_code = reinterpret_cast<int4*>(smem_raw + TiledLayout<Real>::code_off);  // [BT]
+    uint16_t* s_task = reinterpret_cast<uint16_t*>(s_code + BT);                     // [3 BT]
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
         const int h = tid + r * BT;
         t.hh[r] = h < nh ? __ldg(ta.halo + h0 + h) : make_int2(0, 0);
-        t.tk[r] = h < nt ? __ldg(ta.task + t0 + h) : (uint16_t)0;
+        // the flux tasks straight into the work area (not the staging area)
+        if (h < nt) s_task[h] = __ldg(ta.task + t0 + h);
     }
-    reinterpret_cast<int4*>(smem_raw + TiledLayout<Real>::code_off)[tid] = code;
+    s_code[tid] = code;
     // edge normals N_k (length = edge length; N_k / area = 2(r0 + r1), -2 r0,
     // -2 r1) from the FP64 J^-1 rows, kept in the working precision.  The
     // residual is accumulated scaled by 2 area (= 1 / det J^-1): the volume
@@ -390,7 +392,6 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     constexpr int SR = NB * (int)(sizeof(Real) / 4);  // 16-byte rows of a state
     const int nh = d1.y, nt = d1.w;
     const int2* hh = pre.hh;
-    const uint16_t* tk = pre.tk;
     Real R[NB][4];
     Real u[NB][4];
     const double det = pre.det;
@@ -413,8 +414,6 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                     for (int q = 0; q < SR; ++q)
                         cp_async16(stg + ((size_t)q * HM + h) * 16, Ub + ((size_t)q * a.ld + hh[r].x) * 16);
                 }
-                const int j = tid + r * BT;
-                if (j < nt) s_task[j] = tk[r];
             }
         }
         {
