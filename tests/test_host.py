@@ -61,6 +61,20 @@ def test_native_basis_is_orthonormal_and_hierarchical():
     np.testing.assert_allclose(a[0] - 2 * a[1] + a[2], 0.0, atol=1e-14)
 
 
+def test_native_basis_structure_the_stage_kernel_relies_on():
+    # the tile kernel forms the psi_0 term once per state and skips the
+    # eta-derivative of psi_1; the library checks both on its tables, here
+    # they are checked bit for bit on the basis values
+    rng = np.random.default_rng(7)
+    xi = rng.uniform(0, 1, 64)
+    eta = rng.uniform(0, 1, 64) * (1 - xi)
+    psi = capi.native_basis(6, xi, eta)
+    assert (psi[:, 0] == psi[0, 0]).all()
+    psi_shift = capi.native_basis(6, xi, rng.uniform(0, 1, 64) * (1 - xi))
+    np.testing.assert_array_equal(psi[:, 1], psi_shift[:, 1])
+    assert not np.array_equal(psi[:, 2], psi_shift[:, 2])
+
+
 def test_connectivity_matches_generator():
     for m in (meshgen.box_with_obstacle(n=10), meshgen.channel(10, 4)):
         nb, sh, bc = capi.build_connectivity(m.vertices, m.tris, None, m.bc)
