@@ -267,7 +267,7 @@ __device__ __forceinline__ void load_staged(const unsigned char* stg, int x, Rea
 
 // With RKDG_HOLD_STATE 1, FP32 tiles keep the stage input in registers from
 // phase A to the update; by default both precisions read it again (an L2
-// hit), which leaves FP32 P2 tiles at 96 registers.
+// hit), which keeps FP32 tiles within the 80 registers of six CTAs per SM.
 #ifndef RKDG_HOLD_STATE
 #define RKDG_HOLD_STATE 0
 #endif
