@@ -59,8 +59,8 @@ def parse():
     ap.add_argument("--workload", default="batched", choices=["batched", "vortex", "serving", "step"])
     ap.add_argument("--no-step", action="store_true", help="skip the Mach-3 step FP32/FP64 comparison")
     ap.add_argument("--step-h", type=int, default=400, help="1/h of the Mach-3 step lattice")
-    ap.add_argument("--step-sensitivity", action="store_true",
-                    help="also run FP64 from an initial state perturbed at FP32 rounding level")
+    ap.add_argument("--no-step-sensitivity", action="store_true",
+                    help="skip the FP64 run from an initial state perturbed at FP32 rounding level")
     ap.add_argument("--nsolves", type=int, default=64)
     ap.add_argument("--lattice", type=int, default=700)
     ap.add_argument("--plain-steps", type=int, default=50)
@@ -68,7 +68,10 @@ def parse():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the single-solve measurements")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--precision", default="both", choices=["both", "fp32", "fp64"])
+    ap.add_argument("--precision", default="all",
+                    help="comma list of fp32, fp32c, fp64, or 'all'")
+    ap.add_argument("--headline", default="fp32", choices=["fp32", "fp32c"],
+                    help="FP32 form whose batched rate is the line's value")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI run")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving sweep")
@@ -230,9 +233,20 @@ def batched_problems(n=64, seed=4):
     return meshes, orders, states, fars, par
 
 
-def bytes_per_elem_stage(nb: int, word: int, rk: int = 3) -> float:
+def bytes_per_elem_stage(nb: int, prec: str, rk: int = 3) -> float:
+    """Algorithmic HBM bytes of one element-stage: the stage input read and
+    the output written (2), U^n read where the stage combines with it (mean
+    r over the scheme's stages), 16-byte state rows (FP64 two per basis
+    function, FP32 one, FP32C one plus the row of the cell means' low
+    parts), and 56 B of geometry, edge codes and tile tables."""
     r = {3: 2.0 / 3.0, 2: 0.5}[rk]
-    return 4 * nb * word * (2 + r) + 56
+    rows = {"fp64": 2 * nb, "fp32": nb, "fp32c": nb + 1}[prec]
+    return 16 * rows * (2 + r) + 56
+
+
+def precisions(args):
+    sel = ["fp32", "fp32c", "fp64"] if args.precision == "all" else args.precision.split(",")
+    return [p for p in ("fp32", "fp32c", "fp64") if p in sel]
 
 
 def measured_peak():
@@ -303,9 +317,7 @@ def run_batched(args, dist, peak, peak_kind):
     nbs = [3 if o == 1 else 6 for o in orders]
     dofs = sum(m.ntri * 4 * nb for m, nb in zip(meshes, nbs))
     out = {}
-    precs = [p for p in ("fp32", "fp64") if args.precision in ("both", p)]
-    for prec in precs:
-        word = 4 if prec == "fp32" else 8
+    for prec in precisions(args):
         b = Batch(meshes, orders, precision=prec, flux="hllc", rk=3, nq=6, cfl=0.2, farfields=fars)
         for i, U in enumerate(states):
             b.set_state(i, U)
@@ -315,15 +327,11 @@ def run_batched(args, dist, peak, peak_kind):
             b.set_time(i, 0.0)
         b.advance(W)
         sp = b.stream()
-        clocks = None
-        if prec == "fp32":
-            with ClockSampler(dist.local) as cs:
-                ms = event_time(sp, lambda: b.advance(K), dist)
-            clocks = cs.summary()
-        else:
+        with ClockSampler(dist.local) as cs:
             ms = event_time(sp, lambda: b.advance(K), dist)
+        clocks = cs.summary()
         value = dist.sum(dofs * 3 * K) / (ms * 1e-3)
-        alg = sum(m.ntri * bytes_per_elem_stage(nb, word) for m, nb in zip(meshes, nbs))
+        alg = sum(m.ntri * bytes_per_elem_stage(nb, prec) for m, nb in zip(meshes, nbs))
         roof = roofline(b.time_stage(0, 10), b.time_stage(1, 10), b.time_stage(2, 10), alg, peak, peak_kind,
                         "tiled_stage_kernel (P1+P2 tiles, one launch per stage)",
                         measured_traffic("tiled_stage_kernel_batched_fp32.md")
@@ -384,15 +392,13 @@ def run_plain(args, dist, peak, peak_kind, K):
     T = mesh.ntri
     U0 = vortex.project_native(mesh, lambda X, Y: vortex.exact(X, Y, 0.0), 6, n=4)
     out = {}
-    precs = [p for p in ("fp32", "fp64") if args.precision in ("both", p)]
-    for prec in precs:
-        word = 4 if prec == "fp32" else 8
+    for prec in precisions(args):
         s = solver_for(mesh, prec)
         s.setFreedom(U0, basis="native")
         s.advance(args.warmup)
         ms = event_time(s.stream(), lambda: s.advance(K), dist)
         value = dist.sum(T * 24 * 3 * K) / (ms * 1e-3)
-        roof = roofline(s.time_stage(0, 10), s.time_stage(1, 10), s.time_stage(2, 10), T * bytes_per_elem_stage(6, word),
+        roof = roofline(s.time_stage(0, 10), s.time_stage(1, 10), s.time_stage(2, 10), T * bytes_per_elem_stage(6, prec),
                         peak, peak_kind, "tiled_stage_kernel (P2)")
         e2e = None
         if not args.no_e2e:
@@ -427,13 +433,16 @@ def run_plain(args, dist, peak, peak_kind, K):
 
 
 # ------------------------------------------------------ Mach-3 step (C3) --
-def run_step(args, dist):
+def run_step(args, dist, peak, peak_kind):
     """Mach-3 wind-tunnel step: jittered Delaunay mesh, h = 1/400 (seed 3),
     P1, LLF, TVB limiter M = 50 on characteristic variables, SSP-RK3, CFL 0.3,
-    uniform inflow (1.4, 3, 0, 1) to t = 0.5; FP32 (FP64 geometry and dt)
-    against FP64.  Reports the relative L1 difference of the cell-mean
-    density, sum_e A_e |rho32 - rho64| / sum_e A_e |rho64|, at t = 0.05 and
-    t = 0.5, and each precision's DOF-stage/s over the run (CUDA events)."""
+    uniform inflow (1.4, 3, 0, 1) to t = 0.5; FP32 and FP32C (FP64 geometry
+    and dt) against FP64.  Reports the relative L1 difference of the
+    cell-mean density, sum_e A_e |rho_x - rho64| / sum_e A_e |rho64|, at
+    t = 0.05 and t = 0.5, the same difference for an FP64 run started from a
+    state perturbed by 6e-8 relative (the control: how far FP64 moves under
+    FP32-sized input noise), each precision's DOF-stage/s over the run (CUDA
+    events), and the roofline of one stage (stage kernel + limiter)."""
     from rkdg_heter_calculate_b200 import CUDARkdgSolver, meshgen
 
     m = meshgen.forward_step(h=1.0 / args.step_h, seed=3)
@@ -442,15 +451,16 @@ def run_step(args, dist):
     U[:, 0, :] = far[:, None]
     a = m.areas()
     kw = dict(order=1, nq=3, ng=2, flux="llf", rk=3, limiter="tvb", tvb_m=50.0, cfl=0.3, farfield=far)
-    runs = [("fp64", U), ("fp32", U)]
-    if args.step_sensitivity:
+    runs = [("fp64", U), ("fp32", U), ("fp32c", U)]
+    if not args.no_step_sensitivity:
         rng = np.random.default_rng(7)
         Up = U.copy()
         Up[:, 0, :] *= 1.0 + 6e-8 * rng.uniform(-1.0, 1.0, (4, m.ntri))
         runs.append(("fp64_perturbed", Up))
     res = {}
     for name, U0 in runs:
-        s = CUDARkdgSolver(m, precision="fp32" if name == "fp32" else "fp64", **kw)
+        prec = name.split("_")[0]
+        s = CUDARkdgSolver(m, precision=prec, **kw)
         s.setFreedom(U0, basis="native")
         out = {}
         steps = 0
@@ -460,8 +470,9 @@ def run_step(args, dist):
             ms += event_time(s.stream(), lambda: box.update(r=s.advance(10 ** 8, t_final=tt)), dist)
             steps += box["r"][1]
             out[tt] = s.copyFreedomToHost(basis="native")[0, 0]
+        stage_ms = [s.time_stage(k, 10) for k in range(3)] if name in ("fp32", "fp32c", "fp64") else None
         s.close()
-        res[name] = {"rho": out, "steps": steps, "ms": ms}
+        res[name] = {"rho": out, "steps": steps, "ms": ms, "stage_ms": stage_ms}
 
     def rel(x, y):
         return float(np.sum(a * np.abs(x - y)) / np.sum(a * np.abs(y)))
@@ -470,11 +481,27 @@ def run_step(args, dist):
                         "SSP-RK3, CFL 0.3, to t = 0.5" % (args.step_h, m.ntri),
             "triangles": int(m.ntri),
             "rel_L1_rho_fp32_vs_fp64": {str(t): rel(res["fp32"]["rho"][t], res["fp64"]["rho"][t]) for t in (0.05, 0.5)},
-            "definition": "sum_e A_e |rho32 - rho64| / sum_e A_e |rho64| over cell means"}
+            "rel_L1_rho_fp32c_vs_fp64": {str(t): rel(res["fp32c"]["rho"][t], res["fp64"]["rho"][t]) for t in (0.05, 0.5)},
+            "definition": "sum_e A_e |rho_x - rho64| / sum_e A_e |rho64| over cell means"}
     for name in res:
         r = res[name]
-        line[name] = {"steps": r["steps"], "ms": round(r["ms"], 1),
-                      "dof_stage_per_s": dist.sum(r["steps"] * 3 * 12 * m.ntri / (r["ms"] * 1e-3))}
+        per_stage_ms = r["ms"] / (3 * r["steps"])
+        d = {"steps": r["steps"], "ms": round(r["ms"], 1),
+             "dof_stage_per_s": dist.sum(r["steps"] * 3 * 12 * m.ntri / (r["ms"] * 1e-3))}
+        if r["stage_ms"]:
+            prec = name
+            alg = m.ntri * bytes_per_elem_stage(3, prec)
+            # the whole stage (fused stage kernel, TVB limiter, the step's dt
+            # kernel shared out) as it runs in the time loop, and the stage
+            # kernel alone (event-timed launches, epilogue included)
+            d["roofline"] = {"bound": "hbm", "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                             "algorithmic_bytes_per_stage": alg,
+                             "stage_with_limiter": {"ms": round(per_stage_ms, 5),
+                                                    "achieved": round(alg / (per_stage_ms * 1e-3) / 1e9, 1),
+                                                    "frac": round(alg / (per_stage_ms * 1e-3) / 1e9 / peak, 4)},
+                             "stage_kernel_only": roofline(*r["stage_ms"], alg, peak, peak_kind,
+                                                           "tiled_stage_kernel (P1, LLF)")}
+        line[name] = d
     if "fp64_perturbed" in res:
         line["rel_L1_rho_fp64_perturbed_vs_fp64"] = {
             str(t): rel(res["fp64_perturbed"]["rho"][t], res["fp64"]["rho"][t]) for t in (0.05, 0.5)}
@@ -705,10 +732,10 @@ def main():
         plain = None
         if not args.no_plain:
             plain, T2 = run_plain(args, dist, peak, peak_kind, args.plain_steps)
-        head = "fp32" if "fp32" in res else "fp64"
+        head = next((p for p in (args.headline, "fp32", "fp32c", "fp64") if p in res))
         r = res[head]
         serving = None if args.no_serving else run_serving(args, dist)
-        step = None if (args.no_step or args.no_accuracy) else run_step(args, dist)
+        step = None if (args.no_step or args.no_accuracy) else run_step(args, dist, peak, peak_kind)
         cpu = None
         if dist.rank == 0 and not args.no_cpu:
             _, cpu = cpu_reference_sample(args.cpu_seconds)
@@ -716,50 +743,59 @@ def main():
             cpu["single_core"] = {"value": v1, "sample": d1["sample"]}
             cpu["host_cpu"] = host_cpu_model()
         if dist.rank == 0:
-            l2 = None
-            if r.get("l2") is not None and "fp64" in res and res["fp64"].get("l2") is not None:
-                ratio = np.array(r["l2"]) / np.array(res["fp64"]["l2"])
+            def l2_summary(prec):
+                if res.get(prec, {}).get("l2") is None or res.get("fp64", {}).get("l2") is None:
+                    return None
+                x, ref = np.array(res[prec]["l2"]), np.array(res["fp64"]["l2"])
+                ratio = x / ref
                 w = int(np.argmax(ratio))
-                l2 = {"batched_fp32_over_fp64_max": float(ratio.max()),
-                      "batched_fp32_over_fp64_median": float(np.median(ratio)),
-                      "batched_fp64_l2_rho_median": float(np.median(res["fp64"]["l2"])),
-                      "solves_over_1.05": int((ratio > 1.05).sum()),
-                      "worst": {"triangles": r["tris"][w], "order": r["orders"][w],
-                                "fp64_l2_rho": float(res["fp64"]["l2"][w]),
-                                "fp32_l2_rho": float(r["l2"][w])},
-                      "steps": 200}
+                return {"over_fp64_max": float(ratio.max()), "over_fp64_median": float(np.median(ratio)),
+                        "solves_over_1.05": int((ratio > 1.05).sum()),
+                        "worst": {"triangles": r["tris"][w], "order": r["orders"][w],
+                                  "fp64_l2_rho": float(ref[w]), "l2_rho": float(x[w])}}
+            l2 = None
+            if "fp64" in res and res["fp64"].get("l2") is not None:
+                l2 = {"steps": 200, "batched_fp64_l2_rho_median": float(np.median(res["fp64"]["l2"]))}
+                for p in ("fp32", "fp32c"):
+                    if l2_summary(p):
+                        l2["batched_" + p] = l2_summary(p)
             if plain and plain.get("fp64", {}).get("l2"):
                 l2 = dict(l2 or {})
-                l2["plain_980k_fp64"] = plain["fp64"]["l2"]
-                if plain.get("fp32", {}).get("l2"):
-                    l2["plain_980k_fp32"] = plain["fp32"]["l2"]
+                for p in plain:
+                    if plain[p].get("l2"):
+                        l2["plain_980k_" + p] = plain[p]["l2"]
             pf64 = plain["fp64"]["value"] if plain and "fp64" in plain else None
             line = {
                 "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": dist.world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32" if head == "fp32" else "f64", "data": "synthetic",
+                "dtype": "f32" if head != "fp64" else "f64", "data": "synthetic",
                 "config": {"workload": f"batched uneven solves: {info['solves']} isentropic vortices "
                                        f"(strength U[1,5], angle U[0,2pi), seed 4) on periodic jittered "
                                        f"Delaunay meshes, {info['min_tris']}-{info['max_tris']} triangles "
                                        f"(log-uniform 5k-200k), {info['p1_solves']} P1 + {info['p2_solves']} P2, "
-                                       "FP32 state (FP64 geometry, dt), HLLC, SSP-RK3, CFL 0.2, one launch "
-                                       "per RK stage for all solves, CUDA graph, autotuned shape",
-                           **info, "launch_shape": r["shape"],
+                                       + {"fp32": "FP32 state (FP64 geometry, dt)",
+                                          "fp32c": "FP32 arithmetic, FP32 state with cell means as high + low "
+                                                   "float pairs updated in FP64 (FP64 geometry, dt)",
+                                          "fp64": "FP64"}[head]
+                                       + ", HLLC, SSP-RK3, CFL 0.2, one launch per RK stage for all solves, "
+                                       "CUDA graph, autotuned shape",
+                           "precision_form": head, **info, "launch_shape": r["shape"],
                            "parallelism": f"{dist.world} independent replica(s), no collective",
                            "l2_flush": "inputs larger than L2 (3 state buffers of the packed solves)"},
                 "roofline": r["roofline"], "e2e": r["e2e"],
-                "batched_fp64": ({k: res["fp64"][k] for k in ("value", "ms_per_step", "roofline")}
-                                 if "fp64" in res and head == "fp32" else None),
+                "batched_forms": {p: {k: res[p][k] for k in ("value", "ms_per_step", "roofline", "clocks", "shape")}
+                                  for p in res},
                 "plain_fp64": pf64,
-                "batched_fp32_over_plain_fp64": (r["value"] / pf64) if pf64 else None,
+                "batched_over_plain_fp64": ({p: res[p]["value"] / pf64 for p in res if p != "fp64"}
+                                            if pf64 else None),
                 "plain": ({p: {k: v for k, v in plain[p].items() if k != "l2"} for p in plain}
                           if plain else None),
                 "cpu_baseline": cpu, "clocks": r["clocks"], "gpu_launches": 4 * args.steps,
                 "l2": l2, "serving": serving, "step_fp32_vs_fp64": step,
             }
     elif args.workload == "step":
-        step = run_step(args, dist)
+        step = run_step(args, dist, *measured_peak())
         if dist.rank == 0:
             print(json.dumps({"workload": "step", "n_gpus": dist.world, "step_fp32_vs_fp64": step}), flush=True)
     elif args.workload == "serving":
@@ -768,7 +804,7 @@ def main():
             print(json.dumps({"workload": "serving", "n_gpus": dist.world, "serving": serving}), flush=True)
     else:
         res, T = run_plain(args, dist, peak, peak_kind, args.steps)
-        head = "fp32" if "fp32" in res else "fp64"
+        head = next((p for p in (args.headline, "fp32", "fp32c", "fp64") if p in res))
         r = res[head]
         cpu = None
         if dist.rank == 0 and not args.no_cpu:
@@ -778,14 +814,14 @@ def main():
                 "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": dist.world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32" if head == "fp32" else "f64", "data": "synthetic",
+                "dtype": "f32" if head != "fp64" else "f64", "data": "synthetic",
                 "config": {"workload": "unstructured isentropic vortex: periodic Delaunay of a "
                                        f"{args.lattice}x{args.lattice} lattice jittered +-0.3h (seed 2), "
                                        f"{T} triangles, P2, 6-pt volume / 3-pt edge, HLLC, SSP-RK3, CFL 0.2",
                            "triangles": T, "parallelism": f"{dist.world} independent replica(s)",
                            "l2_flush": "inputs larger than L2"},
                 "roofline": r["roofline"], "e2e": r["e2e"],
-                "fp64": res.get("fp64") if head == "fp32" else None,
+                "forms": {p: res[p] for p in res if p != head},
                 "cpu_baseline": cpu, "gpu_launches": 4 * args.steps,
                 "l2": {p: res[p]["l2"] for p in res},
             }

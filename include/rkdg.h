@@ -42,11 +42,16 @@ extern "C" {
 
 /* ---- enumerations ------------------------------------------------------ */
 #define RKDG_FLUX_LLF 0        /* local Lax-Friedrichs, alpha from cell means */
-#define RKDG_FLUX_HLLC 1       /* HLLC with Roe-averaged wave speeds          */
+#define RKDG_FLUX_HLLC 1       /* HLLC, Davis wave-speed bounds (Toro 10.48)  */
 #define RKDG_LIMITER_NONE 0
 #define RKDG_LIMITER_TVB 1     /* TVB minmod on characteristic variables      */
 #define RKDG_FP64 0            /* FP64 state and arithmetic                   */
 #define RKDG_FP32 1            /* FP32 state/arithmetic, FP64 geometry and dt */
+#define RKDG_FP32C 2           /* as RKDG_FP32, with each cell mean stored as a
+                                  high + low float pair (about 48 significant
+                                  bits) and updated in FP64: the state's
+                                  storage rounding no longer accumulates over
+                                  long runs; one more 16-byte row per element */
 #define RKDG_BASIS_REFERENCE 0 /* the reference's per-element basis           */
 #define RKDG_BASIS_NATIVE 1    /* reference-element orthonormal basis         */
 
@@ -86,7 +91,7 @@ typedef struct rkdg_params {
     int32_t flux;         /* RKDG_FLUX_*                                     */
     int32_t limiter;      /* RKDG_LIMITER_*                                  */
     int32_t rk;           /* 2 or 3 (SSP Runge-Kutta stages)                 */
-    int32_t precision;    /* RKDG_FP64 or RKDG_FP32                          */
+    int32_t precision;    /* RKDG_FP64, RKDG_FP32 or RKDG_FP32C              */
     int32_t reorder;      /* 1: Morton-reorder elements in HBM for locality  */
     double gamma;
     double cfl;           /* dt = cfl / max (|u|+c) perimeter/area           */
@@ -242,8 +247,9 @@ typedef struct rkdg_batch rkdg_batch;
 
 /* orders[s]: 1 or 2 per solve; P2 solves use params->nq (6 or 7 for a
  * P2-only batch, 6 when P1 and P2 are mixed) and 3 edge points, P1 solves
- * the 3/2-point rules.  params->precision, flux, rk, gamma, cfl are shared;
- * farfields [nsolves][4] gives each solve's far-field state (NULL: params). */
+ * the 3/2-point rules.  params->precision, flux, rk, gamma, cfl and reorder
+ * (Morton order within each solve) are shared; farfields [nsolves][4] gives
+ * each solve's far-field state (NULL: params). */
 int rkdg_batch_create(int32_t nsolves, const rkdg_mesh_desc* meshes, const int32_t* orders,
                       const double* farfields, const rkdg_params* params, rkdg_batch** out);
 int rkdg_batch_destroy(rkdg_batch* b);

@@ -25,6 +25,20 @@ _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _lib = None
 
 
+def reference_dir() -> str:
+    """The reference checkout's multi_gpuRkdg directory: $RKDG_REF_DIR when
+    set, else the REF_DIR default of oracle/Makefile (the recipe that
+    compiles the reference's sources)."""
+    env = os.environ.get("RKDG_REF_DIR")
+    if env:
+        return env
+    with open(os.path.join(HERE, "Makefile")) as f:
+        for line in f:
+            if line.startswith("REF_DIR") and "?=" in line:
+                return line.split("?=", 1)[1].strip()
+    return ""
+
+
 def available() -> bool:
     return os.path.exists(LIB_PATH)
 

@@ -38,6 +38,7 @@ def lib():
         L.rkdg_refgpu_get_dofs.argtypes = [C.c_void_p, _dp]
         L.rkdg_refgpu_residual.argtypes = [C.c_void_p, _dp]
         L.rkdg_refgpu_steps.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+        L.rkdg_refgpu_write_solution.argtypes = [C.c_void_p, _dp, C.c_char_p]
         _lib = L
     return _lib
 
@@ -89,6 +90,13 @@ class RefGpuCase:
         out = np.zeros((4, 6, self.num))
         assert lib().rkdg_refgpu_residual(self.h, out.ctypes.data_as(_dp)) == 0
         return out[:, :, : self.tnum]
+
+    def write_solution(self, means, path: str):
+        """The reference's own solution.plt writer (CCUDARkdgSolver::
+        outputSolution) on this mesh with the cell means [4][tnum]."""
+        m = np.ascontiguousarray(means, dtype=np.float64)
+        assert m.shape == (4, self.tnum)
+        assert lib().rkdg_refgpu_write_solution(self.h, m.ctypes.data_as(_dp), path.encode()) == 0
 
     def steps(self, n: int):
         """n steps; returns (device ms, last dt)."""

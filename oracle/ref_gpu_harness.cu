@@ -16,6 +16,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "cudarkdgsolver.h"
 
@@ -142,6 +143,21 @@ int rkdg_refgpu_residual(void* h, double* R) {
         cudaMemcpy2D(R + (size_t)v * BASIS_FUNCTIONS * c->num, row, src[v], pitch, row, BASIS_FUNCTIONS,
                      cudaMemcpyDeviceToHost);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+/* The reference's own Tecplot writer, CCUDARkdgSolver::outputSolution
+ * (src/cudarkdgsolver.cu:860-1001), on the opened mesh with the given cell
+ * means M [4][tnum] (rho, rhou, rhov, rhoE) as its single rank's results.
+ * It prints its progress lines to stdout, as the reference does. */
+int rkdg_refgpu_write_solution(void* h, const double* M, const char* path) {
+    RefGpu* c = static_cast<RefGpu*>(h);
+    CCUDARkdgSolver& s = c->s;
+    const size_t T = (size_t)c->tnum;
+    std::vector<double> r(M, M + 4 * T);
+    int data_size[1] = {c->tnum};
+    s.solution_file = path;
+    s.outputSolution(data_size, r.data(), r.data() + T, r.data() + 2 * T, r.data() + 3 * T);
+    return 0;
 }
 
 /* n steps; *ms = device milliseconds between events recorded before the

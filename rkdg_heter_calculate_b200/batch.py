@@ -18,8 +18,9 @@ from .solver import _FLUX, _PREC
 
 class Batch:
     def __init__(self, meshes, orders, precision="fp32", flux="hllc", rk=3, nq=6, gamma=1.4,
-                 cfl=0.2, farfields=None):
+                 cfl=0.2, farfields=None, reorder=True):
         p = capi.default_params()
+        p.reorder = 1 if reorder else 0
         p.order = 2
         p.nq = nq
         p.ng = 3

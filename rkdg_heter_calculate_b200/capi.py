@@ -20,7 +20,7 @@ RKDG_ERR_NODEVICE, RKDG_ERR_IO, RKDG_ERR_BUSY = 5, 6, 7
 ERRORS = {1: "INVALID", 2: "CUDA", 3: "NOMEM", 4: "STATE", 5: "NODEVICE", 6: "IO", 7: "BUSY"}
 FLUX_LLF, FLUX_HLLC = 0, 1
 LIMITER_NONE, LIMITER_TVB = 0, 1
-FP64, FP32 = 0, 1
+FP64, FP32, FP32C = 0, 1, 2
 BASIS_REFERENCE, BASIS_NATIVE = 0, 1
 BC_FARFIELD, BC_OUTFLOW, BC_REFLECTION = 1, 2, 3
 

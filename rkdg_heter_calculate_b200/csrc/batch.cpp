@@ -83,7 +83,11 @@ void h2d(rkdg_batch* b, T* dst, const std::vector<T>& src) {
         RKDG_CUDA_TRY(cudaMemcpyAsync(dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, b->stream));
 }
 
-size_t state_bytes(const rkdg_batch* b) { return (size_t)24 * b->word * b->ld; }
+// the P2 row layout for every solve (RKDG_FP32C: row 6 holds the low parts
+// of the cell means, for P1 and P2 solves alike)
+size_t state_bytes(const rkdg_batch* b) { return (size_t)16 * state_rows(b->p.precision, 6) * b->ld; }
+int kprec(const rkdg_batch* b) { return kernel_prec(b->p.precision); }
+int lo_row(const rkdg_batch* b) { return b->p.precision == RKDG_FP32C ? 6 : -1; }
 
 void sync(rkdg_batch* b) { RKDG_CUDA_TRY(cudaStreamSynchronize(b->stream)); }
 
@@ -120,6 +124,7 @@ StageArgs stage_args(const rkdg_batch* b) {
     a.gamma = b->p.gamma;
     for (int v = 0; v < 4; ++v) a.far[v] = b->p.farfield[v];
     a.far_sid = b->far;
+    a.lo_row = lo_row(b);
     return a;
 }
 
@@ -137,7 +142,7 @@ void enqueue_stage(rkdg_batch* b, int s, int in, int u0, int out, bool last) {
     a.U0 = s == 0 ? nullptr : b->U[u0];
     a.Unew = b->U[out];
     a.last_stage = last ? 1 : 0;
-    launch_stage(a, b->tiles, 1, b->ord, b->p.nq, 3, b->p.flux, b->p.precision, b->ctas, b->stream);
+    launch_stage(a, b->tiles, b->ord, b->p.nq, b->p.flux, kprec(b), b->ctas, b->stream);
 }
 
 void enqueue_step(rkdg_batch* b) {
@@ -190,7 +195,8 @@ int rkdg_batch_create(int32_t nsolves, const rkdg_mesh_desc* meshes, const int32
             throw Error{RKDG_ERR_INVALID, "rkdg_batch_create: bad arguments"};
         *out = nullptr;
         const rkdg_params& p = *params;
-        if (p.precision != RKDG_FP32 && p.precision != RKDG_FP64) throw Error{RKDG_ERR_INVALID, "unknown precision"};
+        if (p.precision != RKDG_FP32 && p.precision != RKDG_FP64 && p.precision != RKDG_FP32C)
+            throw Error{RKDG_ERR_INVALID, "unknown precision"};
         if (p.rk != 2 && p.rk != 3) throw Error{RKDG_ERR_INVALID, "rk must be 2 or 3"};
         if (p.limiter != RKDG_LIMITER_NONE) throw Error{RKDG_ERR_INVALID, "batches run without the limiter"};
         if (!(p.gamma > 1.0) || !(p.cfl > 0.0)) throw Error{RKDG_ERR_INVALID, "gamma > 1 and cfl > 0 required"};
@@ -216,7 +222,7 @@ int rkdg_batch_create(int32_t nsolves, const rkdg_mesh_desc* meshes, const int32
         b->device = dev;
         b->p = p;
         b->S = nsolves;
-        b->word = p.precision == RKDG_FP32 ? 4 : 8;
+        b->word = p.precision == RKDG_FP64 ? 8 : 4;
         b->ord = has1 && has2 ? 3 : (has2 ? 2 : 1);
         b->order.assign(orders, orders + nsolves);
         b->have_state.assign(nsolves, false);
@@ -234,7 +240,7 @@ int rkdg_batch_create(int32_t nsolves, const rkdg_mesh_desc* meshes, const int32
         int maxT = 0;
         for (int s = 0; s < nsolves; ++s) {
             HostMesh m = build_mesh(meshes[s]);
-            m = permute_mesh(m, morton_order(m));
+            if (p.reorder) m = permute_mesh(m, morton_order(m));
             HostGeometry g = build_geometry(m, orders[s], false, false);
             TileTables tt = build_tiles(m, (int)total, s, orders[s], (int)(halo.size() / 2), (int)task.size());
             b->T.push_back(m.T);
@@ -315,7 +321,7 @@ int rkdg_batch_set_state(rkdg_batch* b, int32_t s, const double* U, int32_t ld) 
                                         sizeof(double) * T, 4 * nb, cudaMemcpyHostToDevice, b->stream));
         char* base = static_cast<char*>(b->U[0]) + (size_t)16 * b->off[s];
         launch_import(T, b->ld, b->staging, T, nullptr, b->perm + b->off[s], base, b->order[s],
-                      b->p.precision, &b->far_host[4 * s], b->stream);
+                      kprec(b), &b->far_host[4 * s], lo_row(b), b->stream);
         b->have_state[s] = true;
         b->wave_valid = false;
         sync(b);
@@ -330,7 +336,7 @@ int rkdg_batch_get_state(rkdg_batch* b, int32_t s, double* U, int32_t ld) {
         const int T = b->T[s], nb = b->order[s] == 1 ? 3 : 6;
         const char* base = static_cast<const char*>(b->U[0]) + (size_t)16 * b->off[s];
         launch_export(T, b->ld, base, nullptr, b->perm + b->off[s], b->staging, T, b->order[s],
-                      b->p.precision, 0, nullptr, &b->far_host[4 * s], b->stream);
+                      kprec(b), 0, nullptr, &b->far_host[4 * s], lo_row(b), b->stream);
         RKDG_CUDA_TRY(cudaMemcpy2DAsync(U, sizeof(double) * ld, b->staging, sizeof(double) * T,
                                         sizeof(double) * T, 4 * nb, cudaMemcpyDeviceToHost, b->stream));
         sync(b);
@@ -356,7 +362,7 @@ int rkdg_batch_advance(rkdg_batch* b, int32_t nsteps, const double* t_final, dou
             if (!b->have_state[s]) throw Error{RKDG_ERR_INVALID, "solve " + std::to_string(s) + " has no state"};
         RKDG_CUDA_TRY(cudaSetDevice(b->device));
         if (!b->wave_valid) {
-            launch_wave(b->tiles, b->ld, b->U[0], b->p.precision, b->jinv, b->p.gamma, b->ctl, b->S,
+            launch_wave(b->tiles, b->ld, b->U[0], kprec(b), b->jinv, b->p.gamma, b->ctl, b->S,
                         b->far, b->stream);
             b->wave_valid = true;
         }
@@ -426,10 +432,10 @@ int rkdg_batch_time_stage(rkdg_batch* b, int32_t s, int32_t reps, double* ms) {
         cudaEvent_t e0, e1;
         RKDG_CUDA_TRY(cudaEventCreate(&e0));
         RKDG_CUDA_TRY(cudaEventCreate(&e1));
-        launch_stage(a, b->tiles, 1, b->ord, b->p.nq, 3, b->p.flux, b->p.precision, b->ctas, b->stream);
+        launch_stage(a, b->tiles, b->ord, b->p.nq, b->p.flux, kprec(b), b->ctas, b->stream);
         RKDG_CUDA_TRY(cudaEventRecord(e0, b->stream));
         for (int i = 0; i < reps; ++i)
-            launch_stage(a, b->tiles, 1, b->ord, b->p.nq, 3, b->p.flux, b->p.precision, b->ctas, b->stream);
+            launch_stage(a, b->tiles, b->ord, b->p.nq, b->p.flux, kprec(b), b->ctas, b->stream);
         RKDG_CUDA_TRY(cudaEventRecord(e1, b->stream));
         RKDG_CUDA_TRY(cudaEventSynchronize(e1));
         float tms = 0;
@@ -463,7 +469,7 @@ int rkdg_batch_autotune(rkdg_batch* b, int32_t* ctas_out, int32_t* order_out) {
         RKDG_CUDA_TRY(cudaSetDevice(b->device));
         cudaDeviceProp prop;
         RKDG_CUDA_TRY(cudaGetDeviceProperties(&prop, b->device));
-        const int per_sm = std::max(1, tiled_max_ctas_per_sm(b->p.precision, b->ord, b->p.nq, b->p.flux,
+        const int per_sm = std::max(1, tiled_max_ctas_per_sm(kprec(b), b->ord, b->p.nq, b->p.flux,
                                                               b->tiles.max_halo));
         const int wave = prop.multiProcessorCount * per_sm;
         std::vector<int> cand_ctas = {0, wave, 2 * wave, 4 * wave};

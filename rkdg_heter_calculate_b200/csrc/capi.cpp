@@ -30,7 +30,6 @@ struct rkdg_ctx {
     rkdg_params p{};
     int T = 0, ld = 0, nb = 0;
     int device = 0;
-    int block = 128;
     HostMesh mesh;  // internal (possibly reordered) order
     std::vector<double> area;
     DeviceArrays d;
@@ -43,7 +42,6 @@ struct rkdg_ctx {
     cudaGraphExec_t graph = nullptr;
     StepCtl* h_ctl = nullptr;  // pinned mirror of the device control block
     TileArgs tiles{};
-    int variant = 1;  // 1 tile-staged (default), 0 owner-computes
     int ctas = 0;     // tiled grid size (0: one CTA per tile)
     std::unique_ptr<std::ofstream> reslog;  // residual history file (rkdg_set_residual_log)
     bool graph_monitor = false;  // the captured step forms the residual monitor
@@ -80,10 +78,11 @@ void* dev_alloc(rkdg_ctx* c, size_t bytes) {
     return p;
 }
 
-size_t state_bytes(const rkdg_ctx* c) {
-    const size_t word = c->p.precision == RKDG_FP32 ? 4 : 8;
-    return (size_t)4 * c->nb * word * c->ld;
-}
+size_t state_bytes(const rkdg_ctx* c) { return (size_t)16 * state_rows(c->p.precision, c->nb) * c->ld; }
+
+// arithmetic type of the kernels, and the RKDG_FP32C row of the means' low parts
+int kprec(const rkdg_ctx* c) { return kernel_prec(c->p.precision); }
+int lo_row(const rkdg_ctx* c) { return c->p.precision == RKDG_FP32C ? c->nb : -1; }
 
 void check_params(const rkdg_params& p) {
     if (p.order != 1 && p.order != 2) throw Error{RKDG_ERR_INVALID, "order must be 1 or 2"};
@@ -98,7 +97,7 @@ void check_params(const rkdg_params& p) {
     if (p.limiter != RKDG_LIMITER_NONE && p.limiter != RKDG_LIMITER_TVB)
         throw Error{RKDG_ERR_INVALID, "unknown limiter"};
     if (p.rk != 2 && p.rk != 3) throw Error{RKDG_ERR_INVALID, "rk must be 2 or 3"};
-    if (p.precision != RKDG_FP64 && p.precision != RKDG_FP32)
+    if (p.precision != RKDG_FP64 && p.precision != RKDG_FP32 && p.precision != RKDG_FP32C)
         throw Error{RKDG_ERR_INVALID, "unknown precision"};
     if (!(p.gamma > 1.0) || !(p.cfl > 0.0)) throw Error{RKDG_ERR_INVALID, "gamma > 1 and cfl > 0 required"};
     if (!(p.farfield[0] > 0.0)) throw Error{RKDG_ERR_INVALID, "far-field density must be positive"};
@@ -148,7 +147,7 @@ void normalise_buffers(rkdg_ctx* c) {
 
 void ensure_wave(rkdg_ctx* c) {
     if (c->wave_valid) return;
-    launch_wave(c->tiles, c->ld, c->d.U[c->cur], c->p.precision, c->d.jinv, c->p.gamma, c->d.ctl, 1,
+    launch_wave(c->tiles, c->ld, c->d.U[c->cur], kprec(c), c->d.jinv, c->p.gamma, c->d.ctl, 1,
                 c->d.far, c->stream);
     c->wave_valid = true;
 }
@@ -162,6 +161,7 @@ StageArgs base_args(const rkdg_ctx* c) {
     a.ctl = c->d.ctl;
     a.gamma = c->p.gamma;
     for (int v = 0; v < 4; ++v) a.far[v] = c->p.farfield[v];
+    a.lo_row = lo_row(c);
     return a;
 }
 
@@ -185,10 +185,10 @@ void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out, bool monitor 
     a.Unew = c->d.U[out];
     a.last_stage = s == c->p.rk - 1;
     a.monitor = monitor ? 1 : 0;
-    launch_stage(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->variant == 1 ? c->ctas : c->block, c->stream);
+    launch_stage(a, c->tiles, c->p.order, c->p.nq, c->p.flux, kprec(c), c->ctas, c->stream);
     if (c->p.limiter == RKDG_LIMITER_TVB)
         launch_tiled_limiter(c->tiles, 0, c->ld, c->d.U[out], c->d.conn, c->d.lim, c->d.jinv, nullptr,
-                             c->d.far, c->p.precision, c->p.nq, c->p.gamma, c->p.tvb_m, c->d.ctl,
+                             c->d.far, kprec(c), c->p.nq, c->p.gamma, c->p.tvb_m, c->d.ctl,
                              c->stream);
 }
 
@@ -268,13 +268,16 @@ void rkdg_default_params(rkdg_params* p) {
     p->gamma = 1.4;
     p->cfl = 0.18;
     p->tvb_m = 50.0;
-    // the reference's default far field: Mach 0.4, alpha 5 deg, rho = p = 1
-    // (src/cudarkdgsolver.cu:3-32, src/rkdgadvance.cpp:31-34)
-    const double ut = std::sqrt(1.4) * 0.4, al = 5.0 * std::atan(1.0) * 4 / 180;
+    // the reference's default far field: Mach 0.4, alpha 5 deg, rho = p = 1,
+    // formed by its own expressions (src/cudarkdgsolver.cu:3-32,116,
+    // src/rkdgadvance.cpp:31-34: ut = sqrt(gamma pref / rhoref) mach,
+    // rhoE = 1/2 rhoref ut^2 + pref / (gamma - 1))
+    const double gamma = p->gamma, ut = std::sqrt(gamma * 1.0 / 1.0) * 0.4;
+    const double al = 5.0 * std::atan(1.0) * 4 / 180;
     p->farfield[0] = 1.0;
-    p->farfield[1] = ut * std::cos(al);
-    p->farfield[2] = ut * std::sin(al);
-    p->farfield[3] = 0.5 * ut * ut + 1.0 / 0.4;
+    p->farfield[1] = 1.0 * ut * std::cos(al);
+    p->farfield[2] = 1.0 * ut * std::sin(al);
+    p->farfield[3] = 0.5 * 1.0 * ut * ut + 1.0 / (gamma - 1);
 }
 
 int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx** out) {
@@ -330,7 +333,8 @@ int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx*
         std::vector<int4> cn(ld, make_int4(-1, -1, -1, 0));
         for (int t = 0; t < T; ++t)
             cn[t] = make_int4(c->mesh.nbr[3 * t], c->mesh.nbr[3 * t + 1], c->mesh.nbr[3 * t + 2],
-                              (int)pack_info(&c->mesh.shared[3 * t], &c->mesh.bc[3 * t]));
+                              (int)pack_info(&c->mesh.shared[3 * t], &c->mesh.bc[3 * t],
+                                             g.lim_pair.empty() ? 0u : g.lim_pair[t]));
         c->d.conn = (int4*)dev_alloc(c, sizeof(int4) * ld);
         RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.conn, cn.data(), sizeof(int4) * ld, cudaMemcpyHostToDevice,
                                       c->stream));
@@ -338,9 +342,8 @@ int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx*
         RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.perm, c->mesh.perm.data(), sizeof(int32_t) * T,
                                       cudaMemcpyHostToDevice, c->stream));
         if (params->limiter == RKDG_LIMITER_TVB) {
-            c->d.lim = (double*)dev_alloc(c, sizeof(double) * g.lim.size());
-            RKDG_CUDA_TRY(cudaMemcpyAsync(c->d.lim, g.lim.data(), sizeof(double) * g.lim.size(),
-                                          cudaMemcpyHostToDevice, c->stream));
+            c->d.lim = dev_alloc(c, (size_t)3 * ld * (kprec(c) == RKDG_FP64 ? 16 : 8));
+            upload_limiter(c->d.lim, ld, 0, g.lim, T, kprec(c), c->stream);
         }
         {
             TileTables tt = build_tiles(c->mesh, 0, 0, params->order, 0, 0);
@@ -365,7 +368,6 @@ int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx*
             c->tiles.ntiles = tt.ntiles;
             sync(c);  // host tables go out of scope
         }
-        if (const char* v = std::getenv("RKDG_STAGE_VARIANT")) c->variant = std::atoi(v) == 0 ? 0 : 1;
         c->d.partial = (double*)dev_alloc(c, sizeof(double) * 4 * (totals_partial_count(T) + 1));
         c->d.ctl = (StepCtl*)dev_alloc(c, sizeof(StepCtl));
         c->d.far = (double*)dev_alloc(c, sizeof(double) * 4);
@@ -414,7 +416,7 @@ int rkdg_set_state(rkdg_ctx* c, const double* U, int32_t ld, int32_t basis) {
         c->old = 0;
         launch_import(c->T, c->ld, c->d.staging, c->T,
                       basis == RKDG_BASIS_REFERENCE ? c->d.conv_in : nullptr, c->d.perm, c->d.U[0],
-                      c->p.order, c->p.precision, c->p.farfield, c->stream);
+                      c->p.order, kprec(c), c->p.farfield, lo_row(c), c->stream);
         c->have_state = true;
         c->wave_valid = false;
         ensure_wave(c);
@@ -443,8 +445,8 @@ int rkdg_get_state(rkdg_ctx* c, double* U, int32_t ld, int32_t basis) {
         if (basis == RKDG_BASIS_REFERENCE) ensure_conversion(c);
         else if (basis != RKDG_BASIS_NATIVE) throw Error{RKDG_ERR_INVALID, "unknown basis"};
         launch_export(c->T, c->ld, c->d.U[c->cur], basis == RKDG_BASIS_REFERENCE ? c->d.conv_out : nullptr,
-                      c->d.perm, c->d.staging, c->T, c->p.order, c->p.precision, 0, c->d.jinv,
-                      c->p.farfield, c->stream);
+                      c->d.perm, c->d.staging, c->T, c->p.order, kprec(c), 0, c->d.jinv,
+                      c->p.farfield, lo_row(c), c->stream);
         RKDG_CUDA_TRY(cudaMemcpy2DAsync(U, sizeof(double) * ld, c->d.staging, sizeof(double) * c->T,
                                         sizeof(double) * c->T, 4 * c->nb, cudaMemcpyDeviceToHost,
                                         c->stream));
@@ -469,10 +471,11 @@ int rkdg_residual(rkdg_ctx* c, double* R, int32_t ld, int32_t basis) {
         a.Unew = c->d.U[scratch];
         a.a = 0;
         a.b = 1;
-        launch_residual(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->variant == 1 ? c->ctas : c->block, c->stream);
+        a.lo_row = -1;
+        launch_residual(a, c->tiles, c->p.order, c->p.nq, c->p.flux, kprec(c), c->ctas, c->stream);
         launch_export(c->T, c->ld, c->d.U[scratch], basis == RKDG_BASIS_REFERENCE ? c->d.conv_in : nullptr,
-                      c->d.perm, c->d.staging, c->T, c->p.order, c->p.precision, 1, c->d.jinv,
-                      c->p.farfield, c->stream);
+                      c->d.perm, c->d.staging, c->T, c->p.order, kprec(c), 1, c->d.jinv,
+                      c->p.farfield, -1, c->stream);
         RKDG_CUDA_TRY(cudaMemcpy2DAsync(R, sizeof(double) * ld, c->d.staging, sizeof(double) * c->T,
                                         sizeof(double) * c->T, 4 * c->nb, cudaMemcpyDeviceToHost,
                                         c->stream));
@@ -535,7 +538,7 @@ int rkdg_limit(rkdg_ctx* c) {
         if (c->p.limiter != RKDG_LIMITER_TVB) throw Error{RKDG_ERR_INVALID, "context created without limiter"};
         RKDG_CUDA_TRY(cudaSetDevice(c->device));
         launch_tiled_limiter(c->tiles, 0, c->ld, c->d.U[c->cur], c->d.conn, c->d.lim, c->d.jinv,
-                             nullptr, c->d.far, c->p.precision, c->p.nq, c->p.gamma, c->p.tvb_m,
+                             nullptr, c->d.far, kprec(c), c->p.nq, c->p.gamma, c->p.tvb_m,
                              nullptr, c->stream);
         sync(c);
     });
@@ -650,10 +653,10 @@ int rkdg_time_stage(rkdg_ctx* c, int32_t s, int32_t reps, double* ms) {
         cudaEvent_t e0, e1;
         RKDG_CUDA_TRY(cudaEventCreate(&e0));
         RKDG_CUDA_TRY(cudaEventCreate(&e1));
-        launch_stage(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->variant == 1 ? c->ctas : c->block, c->stream);
+        launch_stage(a, c->tiles, c->p.order, c->p.nq, c->p.flux, kprec(c), c->ctas, c->stream);
         RKDG_CUDA_TRY(cudaEventRecord(e0, c->stream));
         for (int i = 0; i < reps; ++i)
-            launch_stage(a, c->tiles, c->variant, c->p.order, c->p.nq, c->p.ng, c->p.flux, c->p.precision, c->variant == 1 ? c->ctas : c->block, c->stream);
+            launch_stage(a, c->tiles, c->p.order, c->p.nq, c->p.flux, kprec(c), c->ctas, c->stream);
         RKDG_CUDA_TRY(cudaEventRecord(e1, c->stream));
         RKDG_CUDA_TRY(cudaEventSynchronize(e1));
         float t = 0;
@@ -693,8 +696,8 @@ int rkdg_conservation_totals(rkdg_ctx* c, double totals[4]) {
         RKDG_CUDA_TRY(cudaSetDevice(c->device));
         const int n = totals_partial_count(c->T);
         double* out4 = c->d.partial + (size_t)4 * n;
-        launch_totals(c->T, c->ld, c->d.U[c->cur], c->p.order, c->p.precision, c->d.jinv,
-                      c->d.partial, out4, c->p.farfield, c->stream);
+        launch_totals(c->T, c->ld, c->d.U[c->cur], c->p.order, kprec(c), c->d.jinv,
+                      c->d.partial, out4, c->p.farfield, lo_row(c), c->stream);
         RKDG_CUDA_TRY(cudaMemcpyAsync(totals, out4, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         sync(c);
     });
@@ -791,7 +794,7 @@ uint64_t mesh_hash(const HostMesh& m) {
 }
 
 // 16-byte packs per element in the state layout
-int state_packs(const rkdg_ctx* c) { return c->nb * (c->p.precision == RKDG_FP32 ? 1 : 2); }
+int state_packs(const rkdg_ctx* c) { return state_rows(c->p.precision, c->nb); }
 
 }  // namespace
 
@@ -845,7 +848,7 @@ int rkdg_checkpoint_load(rkdg_ctx* c, const char* path) {
             throw Error{RKDG_ERR_INVALID, "checkpoint was written for another triangle count, order or precision"};
         if (h.mesh_hash != mesh_hash(c->mesh))
             throw Error{RKDG_ERR_INVALID, "checkpoint was written for another mesh (or triangle ordering)"};
-        if (c->p.precision == RKDG_FP32)
+        if (c->p.precision != RKDG_FP64)
             for (int v = 0; v < 4; ++v)
                 if (h.farfield[v] != c->p.farfield[v])
                     throw Error{RKDG_ERR_INVALID, "FP32 checkpoint was written with another far-field state"};

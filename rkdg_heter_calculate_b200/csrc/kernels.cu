@@ -1,18 +1,21 @@
 // sm_100a kernels of the RKDG residual and time-step path.
 //
 // One fused kernel per Runge-Kutta stage replaces the reference's chain of
-// nine launches per stage (src/kernelfunctions.cu:84-748): each thread owns
-// one triangle, evaluates its state at the volume points, projects the
-// contravariant Euler fluxes onto the basis gradients, evaluates the
-// Riemann flux at the Gauss points of its three edges against the
-// neighbours' traces (owner-computes: deterministic, no atomics), and
-// applies the SSP-RK stage update in its epilogue.  Nothing but the state is
-// written to HBM: traces, fluxes and residuals live in registers.
+// nine launches per stage (src/kernelfunctions.cu:84-748): the tile-staged
+// stage kernel (stage_tiled.cuh) evaluates each element's state at the
+// volume points, projects the contravariant Euler fluxes onto the basis
+// gradients, forms the edge traces and the Riemann flux at the Gauss points
+// of every edge once per tile, and applies the SSP-RK stage update in its
+// epilogue.  Nothing but the state is written to HBM: traces, fluxes and
+// residuals live in registers and shared memory.  This file also holds the
+// physics helpers, the TVB limiter, the CFL/step kernels and the boundary
+// conversions.
 //
 // HBM layout (element-interleaved packs for 128-bit accesses):
 //   state  : row r = 4*i + v (basis i, variable v), packs of W = 16/sizeof(Real)
 //            rows; pack p of element e at ((p*ld + e) * W)  -> one 16-byte
-//            load per pack, a warp reads 512 contiguous bytes;
+//            load per pack, a warp reads 512 contiguous bytes; RKDG_FP32C
+//            adds one pack row holding the low parts of the cell means;
 //   jinv   : FP64 rows of J^-1, [2][ld] double2 = (r0x, r0y), (r1x, r1y);
 //   conn   : [ld] int4 = (neighbour 0, 1, 2, packed shared-edge/boundary tags).
 // The basis is orthonormal under the area average on the reference
@@ -234,6 +237,15 @@ __device__ __forceinline__ void store_state(Real* __restrict__ U, int ld, int e,
 #pragma unroll
         for (int i = 0; i < NB; ++i) p[(size_t)i * ld + e] = make_float4(u[i][0], u[i][1], u[i][2], u[i][3]);
     }
+}
+
+// rows I0..NB-1 of a state (the FP32 form's one 16-byte pack per basis function)
+template <typename Real, int I0, int NB>
+__device__ __forceinline__ void store_rows(Real* __restrict__ U, int ld, int e, const Real u[NB][4]) {
+    static_assert(sizeof(Real) == 4, "one pack per row: FP32 states");
+    float4* p = reinterpret_cast<float4*>(U);
+#pragma unroll
+    for (int i = I0; i < NB; ++i) p[(size_t)i * ld + e] = make_float4(u[i][0], u[i][1], u[i][2], u[i][3]);
 }
 
 // ------------------------------------------------------------- physics --
@@ -528,218 +540,9 @@ __device__ __forceinline__ double wave_of(const Real m[4], Real gamma, const Rea
 }
 
 // ------------------------------------------------------------ the stage --
-enum { MODE_STAGE = 0, MODE_RESIDUAL = 1 };
-
-template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE>
-__global__ void __launch_bounds__(128) stage_kernel(const StageArgs a) {
-    constexpr int CFG = cfg_index(NQ, NG);
-    const Tab<Real>& tb = tab<Real>(CFG);
-    __shared__ Real s_ephi[3][NG][NB];  // neighbour-side edge table (runtime edge index)
-    for (int x = threadIdx.x; x < 3 * NG * NB; x += blockDim.x) {
-        int k = x / (NG * NB), g = (x / NB) % NG, i = x % NB;
-        s_ephi[k][g][i] = tb.ephi[k][g][i];
-    }
-    __syncthreads();
-    if (MODE == MODE_STAGE && a.ctl->done) return;
-
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool active = e < a.T;
-    const int ee = active ? e : 0;  // inactive lanes still join the block reduction
-
-    const Real* __restrict__ U = static_cast<const Real*>(a.U);
-    Real u[NB][4];
-    load_state<Real, NB>(U, a.ld, ee, u);
-    Real dev0[4];  // stored means (deviations in FP32) for the stage update
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-        dev0[v] = u[0][v];
-        u[0][v] += ref_of<Real>(a.far, v);
-    }
-    const double2* jinv2 = reinterpret_cast<const double2*>(a.jinv);
-    const double2 r0 = __ldg(jinv2 + ee), r1 = __ldg(jinv2 + a.ld + ee);
-    const int4 cn = __ldg(a.conn + ee);
-    const Real gamma = (Real)a.gamma, gm1 = gamma - Real(1);
-    const Real j00 = (Real)r0.x, j01 = (Real)r0.y, j10 = (Real)r1.x, j11 = (Real)r1.y;
-
-    Real R[NB][4];
-#pragma unroll
-    for (int i = 0; i < NB; ++i)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) R[i][v] = Real(0);
-
-    // ---- volume integral: sum_q w_q (J^-1 (F, G)) . grad_xi psi_i
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-        Real w[4];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            Real s = Real(0);
-#pragma unroll
-            for (int i = 0; i < NB; ++i) s += tb.vphi[q][i] * u[i][v];
-            w[v] = s;
-        }
-        Real ri = rcp_(w[0]);
-        Real vx = w[1] * ri, vy = w[2] * ri;
-        Real p = gm1 * (w[3] - Real(0.5) * (w[1] * vx + w[2] * vy));
-        Real F[4] = {w[1], w[1] * vx + p, w[2] * vx, (w[3] + p) * vx};
-        Real G[4] = {w[2], w[1] * vy, w[2] * vy + p, (w[3] + p) * vy};
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            Real fx = j00 * F[v] + j01 * G[v];
-            Real fy = j10 * F[v] + j11 * G[v];
-#pragma unroll
-            for (int i = 1; i < NB; ++i) R[i][v] += fx * tb.vdxi[q][i] + fy * tb.veta[q][i];
-        }
-    }
-
-    // ---- edge integrals (owner computes all three of its edges)
-    Real far[4] = {(Real)a.far[0], (Real)a.far[1], (Real)a.far[2], (Real)a.far[3]};
-    Real mL[4] = {u[0][0], u[0][1], u[0][2], u[0][3]};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const int ne = k == 0 ? cn.x : (k == 1 ? cn.y : cn.z);
-        const unsigned info = (unsigned)cn.w;
-        const int se = (info >> (2 * k)) & 3u;
-        const int tag = (info >> (6 + 2 * k)) & 3u;
-        // scaled normal N_k / area and its length, FP64 geometry
-        double Nxd, Nyd;
-        if (k == 0) {
-            Nxd = 2.0 * (r0.x + r1.x);
-            Nyd = 2.0 * (r0.y + r1.y);
-        } else if (k == 1) {
-            Nxd = -2.0 * r0.x;
-            Nyd = -2.0 * r0.y;
-        } else {
-            Nxd = -2.0 * r1.x;
-            Nyd = -2.0 * r1.y;
-        }
-        const double lend = sqrt(Nxd * Nxd + Nyd * Nyd);
-        const Real Nx = (Real)Nxd, Ny = (Real)Nyd, len = (Real)lend;
-        const Real nx = (Real)(Nxd / lend), ny = (Real)(Nyd / lend);
-
-        Real un[NB][4];
-        Real mR[4];
-        const bool interior = ne >= 0;
-        if (interior) {
-            load_state<Real, NB>(U, a.ld, ne, un);
-#pragma unroll
-            for (int v = 0; v < 4; ++v) un[0][v] += ref_of<Real>(a.far, v);
-            mR[0] = un[0][0], mR[1] = un[0][1], mR[2] = un[0][2], mR[3] = un[0][3];
-        } else {
-#pragma unroll
-            for (int i = 0; i < NB; ++i)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) un[i][v] = Real(0);
-            ghost<Real>(tag, mL, far, nx, ny, mR);
-        }
-        // LLF coefficient from the average of the two cell means
-        // (src/kernelfunctions.cu:370-387), scaled by |N|
-        Real alpha = Real(0);
-        if (FLUX == RKDG_FLUX_LLF) {
-            Real rho = Real(0.5) * (mL[0] + mR[0]);
-            Real ir = rcp_(rho);
-            Real vx = Real(0.5) * (mL[1] + mR[1]) * ir;
-            Real vy = Real(0.5) * (mL[2] + mR[2]) * ir;
-            Real E = Real(0.5) * (mL[3] + mR[3]);
-            Real p = gm1 * (E - Real(0.5) * rho * (vx * vx + vy * vy));
-            alpha = fabs(vx * Nx + vy * Ny) + sqrt_(gamma * p * ir) * len;
-        }
-#pragma unroll
-        for (int g = 0; g < NG; ++g) {
-            Real uL[4], uR[4];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                Real s = Real(0);
-#pragma unroll
-                for (int i = 0; i < NB; ++i) s += tb.ephi[k][g][i] * u[i][v];
-                uL[v] = s;
-            }
-            if (interior) {
-                // the neighbour's point NG-1-g on its edge se pairs with ours
-                // (src/kernelfunctions.cu:545-549)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    Real s = Real(0);
-#pragma unroll
-                    for (int i = 0; i < NB; ++i) s += s_ephi[se][NG - 1 - g][i] * un[i][v];
-                    uR[v] = s;
-                }
-            } else {
-                ghost<Real>(tag, uL, far, nx, ny, uR);
-            }
-            Real fh[4];
-            if (FLUX == RKDG_FLUX_LLF) {
-                Real fL[4], fR[4], pL, pR;
-                normal_flux<Real>(uL, Nx, Ny, gm1, fL, pL);
-                normal_flux<Real>(uR, Nx, Ny, gm1, fR, pR);
-#pragma unroll
-                for (int v = 0; v < 4; ++v) fh[v] = Real(0.5) * (fL[v] + fR[v] - alpha * (uR[v] - uL[v]));
-            } else {
-                hllc<Real>(uL, uR, nx, ny, gamma, fh);
-#pragma unroll
-                for (int v = 0; v < 4; ++v) fh[v] *= len;
-            }
-            const Real wg = tb.ew[g];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                Real c = wg * fh[v];
-#pragma unroll
-                for (int i = 0; i < NB; ++i) R[i][v] -= c * tb.ephi[k][g][i];
-            }
-        }
-    }
-
-    Real* __restrict__ Uout = static_cast<Real*>(a.Unew);
-    if (MODE == MODE_RESIDUAL) {
-        if (active) store_state<Real, NB>(Uout, a.ld, e, R);
-        return;
-    }
-
-    // ---- stage update: Unew = a U0 + b (U + dt L(U)), on the stored values
-    const double dtd = a.ctl->dt;
-    // a U^n + b (U + dt L) as U^n + b ((U - U^n) + dt L): a + b = 1 holds
-    // exactly (1/3 and 2/3 both round up in FP32, and a scale of 1 + 3e-8
-    // per step would accumulate into the state)
-    const Real dt = (Real)dtd, cb = (Real)a.b;
-    Real u0m[4] = {Real(0), Real(0), Real(0), Real(0)};
-#pragma unroll
-    for (int v = 0; v < 4; ++v) u[0][v] = dev0[v];
-    if (a.U0 != nullptr) {
-        Real u0[NB][4];
-        load_state<Real, NB>(static_cast<const Real*>(a.U0), a.ld, ee, u0);
-#pragma unroll
-        for (int i = 0; i < NB; ++i)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) R[i][v] = u0[i][v] + cb * ((u[i][v] - u0[i][v]) + dt * R[i][v]);
-#pragma unroll
-        for (int v = 0; v < 4; ++v) u0m[v] = u0[0][v];
-    } else {
-#pragma unroll
-        for (int i = 0; i < NB; ++i)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) R[i][v] = cb * (u[i][v] + dt * R[i][v]);
-    }
-    if (active) store_state<Real, NB>(Uout, a.ld, e, R);
-
-    if (a.last_stage) {
-        // next step's CFL measure, residual monitor, state check (FP64)
-        double wv = 0.0, m0 = 0.0, m1 = 0.0;
-        if (active) {
-            bool bad;
-            Real m[4], len[3], ia;
-#pragma unroll
-            for (int v = 0; v < 4; ++v) m[v] = R[0][v] + ref_of<Real>(a.far, v);
-            elem_lengths<Real>(r0, r1, len, ia);
-            wv = wave_of<Real>(m, gamma, len, ia, bad);
-            if (bad) atomicOr(&a.ctl->error, 1);
-            if (a.monitor) {
-                m0 = fabs((double)R[0][0] - (double)u0m[0]);
-                m1 = fabs((double)R[0][3] - (double)u0m[3]);
-            }
-        }
-        block_max3_atomic(wv, m0, m1, &a.ctl->wave_bits, &a.ctl->mon_bits[0], &a.ctl->mon_bits[1]);
-    }
-}
+// MODE_STAGE_COMP: the FP32 stage of RKDG_FP32C (cell means updated in FP64
+// from their high and low parts)
+enum { MODE_STAGE = 0, MODE_RESIDUAL = 1, MODE_STAGE_COMP = 2 };
 
 #include "stage_tiled.cuh"
 
@@ -812,14 +615,22 @@ __global__ void step_begin_kernel(StepCtl* ctls, int n) {
 // ------------------------------------------------------------ limiter --
 // TVB minmod on characteristic variables for the P1 part (Cockburn & Shu,
 // J. Comput. Phys. 141 (1998) 199-224, sec. 2.4/3.3).  In place: only
-// modes >= 1 change, and neighbours read only cell means.
+// modes >= 1 change, and neighbours read only cell means.  Per edge k the
+// table holds (alpha, beta) of m_k - b0 = alpha (b_k - b0) + beta (b_j - b0)
+// in the working precision (rows k of [3][ld]); the pairing edge j is bit
+// 12 + k of the packed connectivity word, and the direction m_k - b0 (edge
+// midpoint minus centroid) with its length, the TVB threshold's scale, are
+// formed here from J^-1: m_k - b0 = J d_k with the reference-element offsets
+// d_0 = (1/6, 1/6), d_1 = (-1/3, 1/6), d_2 = (1/6, -1/3), and J = (J^-1)^-1.
 template <typename Real, int NB>
 __device__ __forceinline__ void limit_element(int e, int ld, Real* __restrict__ U,
                                               const int4* __restrict__ conn,
-                                              const double* __restrict__ lim,
+                                              const void* __restrict__ limv,
                                               const double* __restrict__ jinv, double gammad,
                                               double f0, double f1, double f2, double f3,
                                               double tvb_m, const Tab<Real>& tb) {
+    using Pair = typename std::conditional<sizeof(Real) == 8, double2, float2>::type;
+    const Pair* lim = static_cast<const Pair*>(limv);
     const double2* j2 = reinterpret_cast<const double2*>(jinv);
     const double2 r0 = __ldg(j2 + e), r1 = __ldg(j2 + ld + e);
     Real u[3][4];
@@ -835,7 +646,10 @@ __device__ __forceinline__ void limit_element(int e, int ld, Real* __restrict__ 
         mean[v] = u[0][v] + ref_of<Real>(fref, v);
     }
     Real nbm[3][4], tilde[3][4];
-    const double* L = lim + (size_t)18 * e;
+    const unsigned pair_bits = ((unsigned)cn.w >> 12) & 7u;
+    const double idet = 1.0 / (r0.x * r1.y - r0.y * r1.x);  // det J
+    // columns of J: x_1 - x_0 and x_2 - x_0
+    const double c0x = r1.y * idet, c0y = -r1.x * idet, c1x = -r0.y * idet, c1y = r0.x * idet;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         int ne = k == 0 ? cn.x : (k == 1 ? cn.y : cn.z);
@@ -859,10 +673,14 @@ __device__ __forceinline__ void limit_element(int e, int ld, Real* __restrict__ 
     Real delta[3][4];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const Real al = (Real)L[6 * k], be = (Real)L[6 * k + 1];
-        const int j = (int)L[6 * k + 2];
-        const Real nx = (Real)L[6 * k + 3], ny = (Real)L[6 * k + 4];
-        const Real thr = (Real)(tvb_m * L[6 * k + 5]);
+        const Pair ab = __ldg(lim + (size_t)k * ld + e);
+        const Real al = (Real)ab.x, be = (Real)ab.y;
+        const int j = (pair_bits >> k) & 1u ? (k + 2) % 3 : (k + 1) % 3;
+        const double dxi = k == 1 ? -1.0 / 3.0 : 1.0 / 6.0, deta = k == 2 ? -1.0 / 3.0 : 1.0 / 6.0;
+        const double dx = c0x * dxi + c1x * deta, dy = c0y * dxi + c1y * deta;
+        const double r2 = dx * dx + dy * dy, irl = 1.0 / sqrt(r2);
+        const Real nx = (Real)(dx * irl), ny = (Real)(dy * irl);
+        const Real thr = (Real)(tvb_m * (4.0 * r2));
         Real dbar[4];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
@@ -946,7 +764,7 @@ template <typename Real>
 __global__ void __launch_bounds__(kTile) tiled_limiter_kernel(const TileArgs ta, int ld,
                                                               Real* __restrict__ U,
                                                               const int4* __restrict__ conn,
-                                                              const double* __restrict__ lim,
+                                                              const void* __restrict__ lim,
                                                               const double* __restrict__ jinv,
                                                               const int* __restrict__ flags,
                                                               const double* __restrict__ refs,
@@ -972,7 +790,7 @@ __global__ void __launch_bounds__(kTile) tiled_limiter_kernel(const TileArgs ta,
 template <typename Real, int NB>
 __global__ void import_kernel(int T, int ld, const double* __restrict__ st, int ldh,
                               const double* __restrict__ conv, const int32_t* __restrict__ perm,
-                              Real* __restrict__ U, Ref4 ref) {
+                              Real* __restrict__ U, Ref4 ref, int lo_row) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= T) return;
     const int c = perm ? perm[e] : e;
@@ -999,6 +817,7 @@ __global__ void import_kernel(int T, int ld, const double* __restrict__ st, int 
 #pragma unroll
             for (int v = 0; v < 4; ++v) b[i][v] = (Real)a[i][v];
     }
+    float lo[4] = {0.f, 0.f, 0.f, 0.f};
     if (stores_deviation<Real>()) {  // mean row = basis 0 (basis-invariant)
         const double* Cm = conv ? conv + (size_t)36 * e : nullptr;
 #pragma unroll
@@ -1011,16 +830,19 @@ __global__ void import_kernel(int T, int ld, const double* __restrict__ st, int 
                 m = a[0][v];
             }
             b[0][v] = (Real)(m - ref.v[v]);
+            lo[v] = (float)((m - ref.v[v]) - (double)b[0][v]);
         }
     }
     store_state<Real, NB>(U, ld, e, b);
+    if (sizeof(Real) == 4 && lo_row >= 0)  // FP32C: the low parts of the cell means
+        reinterpret_cast<float4*>(U)[(size_t)lo_row * ld + e] = make_float4(lo[0], lo[1], lo[2], lo[3]);
 }
 
 template <typename Real, int NB>
 __global__ void export_kernel(int T, int ld, const Real* __restrict__ U,
                               const double* __restrict__ conv, const int32_t* __restrict__ perm,
                               double* __restrict__ st, int ldh, int residual_scale,
-                              const double* __restrict__ jinv, Ref4 ref) {
+                              const double* __restrict__ jinv, Ref4 ref, int lo_row) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= T) return;
     const int c = perm ? perm[e] : e;
@@ -1031,6 +853,10 @@ __global__ void export_kernel(int T, int ld, const Real* __restrict__ U,
     for (int i = 0; i < NB; ++i)
 #pragma unroll
         for (int v = 0; v < 4; ++v) b[i][v] = (double)bl[i][v];
+    if (sizeof(Real) == 4 && lo_row >= 0 && !residual_scale) {  // FP32C: add the low parts
+        const float4 l = reinterpret_cast<const float4*>(U)[(size_t)lo_row * ld + e];
+        b[0][0] += (double)l.x, b[0][1] += (double)l.y, b[0][2] += (double)l.z, b[0][3] += (double)l.w;
+    }
     if (stores_deviation<Real>() && !residual_scale)
 #pragma unroll
         for (int v = 0; v < 4; ++v) b[0][v] += ref.v[v];
@@ -1066,7 +892,7 @@ __global__ void __launch_bounds__(kTotBlock) totals_partial_kernel(int T, int ld
                                                                    const Real* __restrict__ U,
                                                                    const double* __restrict__ jinv,
                                                                    double* __restrict__ partial,
-                                                                   Ref4 ref) {
+                                                                   Ref4 ref, int lo_row) {
     __shared__ double s[4][kTotBlock];
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     double v4[4] = {0, 0, 0, 0};
@@ -1076,8 +902,13 @@ __global__ void __launch_bounds__(kTotBlock) totals_partial_kernel(int T, int ld
         const double2* j2 = reinterpret_cast<const double2*>(jinv);
         double2 r0 = j2[e], r1 = j2[ld + e];
         double area = 0.5 / (r0.x * r1.y - r0.y * r1.x);
+        double lo[4] = {0.0, 0.0, 0.0, 0.0};
+        if (sizeof(Real) == 4 && lo_row >= 0) {  // FP32C: the low parts of the means
+            const float4 l = reinterpret_cast<const float4*>(U)[(size_t)lo_row * ld + e];
+            lo[0] = l.x, lo[1] = l.y, lo[2] = l.z, lo[3] = l.w;
+        }
         for (int v = 0; v < 4; ++v)
-            v4[v] = area * ((double)m[v] + (stores_deviation<Real>() ? ref.v[v] : 0.0));
+            v4[v] = area * (((double)m[v] + lo[v]) + (stores_deviation<Real>() ? ref.v[v] : 0.0));
     }
     for (int v = 0; v < 4; ++v) s[v][threadIdx.x] = v4[v];
     __syncthreads();
@@ -1156,56 +987,33 @@ void dispatch_tiled(const StageArgs& a, const TileArgs& t, int order, int nq, in
     throw Error{RKDG_ERR_INVALID, "unsupported order/rule combination for the tiled kernel"};
 }
 
-template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE>
-void launch_owner(const StageArgs& a, int block, cudaStream_t s) {
-    const int grid = (a.T + block - 1) / block;
-    stage_kernel<Real, NB, NQ, NG, FLUX, MODE><<<grid, block, 0, s>>>(a);
-}
-
-template <typename Real, int FLUX, int MODE>
-void dispatch_owner(const StageArgs& a, int order, int nq, int ng, int block, cudaStream_t s) {
-    if (block != 64 && block != 128) block = 128;
-    if (order == 2 && nq == 7 && ng == 3) return launch_owner<Real, 6, 7, 3, FLUX, MODE>(a, block, s);
-    if (order == 2 && nq == 6 && ng == 3) return launch_owner<Real, 6, 6, 3, FLUX, MODE>(a, block, s);
-    if (order == 1 && nq == 3 && ng == 2) return launch_owner<Real, 3, 3, 2, FLUX, MODE>(a, block, s);
-    throw Error{RKDG_ERR_INVALID, "unsupported quadrature combination"};
-}
-
 template <int MODE>
-void dispatch(const StageArgs& a, const TileArgs& t, int variant, int order, int nq, int ng,
-              int flux, int prec, int block, cudaStream_t s) {
+void dispatch(const StageArgs& a, const TileArgs& t, int order, int nq, int flux, int prec, int ctas,
+              cudaStream_t s) {
     const bool hllc = flux == RKDG_FLUX_HLLC;
-    if (variant == 1) {
-        if (prec == RKDG_FP32) {
-            if (hllc) dispatch_tiled<float, RKDG_FLUX_HLLC, MODE>(a, t, order, nq, block, s);
-            else dispatch_tiled<float, RKDG_FLUX_LLF, MODE>(a, t, order, nq, block, s);
-        } else {
-            if (hllc) dispatch_tiled<double, RKDG_FLUX_HLLC, MODE>(a, t, order, nq, block, s);
-            else dispatch_tiled<double, RKDG_FLUX_LLF, MODE>(a, t, order, nq, block, s);
-        }
+    if (prec == RKDG_FP32) {
+        if (hllc) dispatch_tiled<float, RKDG_FLUX_HLLC, MODE>(a, t, order, nq, ctas, s);
+        else dispatch_tiled<float, RKDG_FLUX_LLF, MODE>(a, t, order, nq, ctas, s);
+    } else if constexpr (MODE != MODE_STAGE_COMP) {
+        if (hllc) dispatch_tiled<double, RKDG_FLUX_HLLC, MODE>(a, t, order, nq, ctas, s);
+        else dispatch_tiled<double, RKDG_FLUX_LLF, MODE>(a, t, order, nq, ctas, s);
     } else {
-        if (order == 3) throw Error{RKDG_ERR_INVALID, "the owner-computes kernel takes one order"};
-        if (prec == RKDG_FP32) {
-            if (hllc) dispatch_owner<float, RKDG_FLUX_HLLC, MODE>(a, order, nq, ng, block, s);
-            else dispatch_owner<float, RKDG_FLUX_LLF, MODE>(a, order, nq, ng, block, s);
-        } else {
-            if (hllc) dispatch_owner<double, RKDG_FLUX_HLLC, MODE>(a, order, nq, ng, block, s);
-            else dispatch_owner<double, RKDG_FLUX_LLF, MODE>(a, order, nq, ng, block, s);
-        }
+        throw Error{RKDG_ERR_INVALID, "a low-part row needs the FP32 stage"};
     }
     RKDG_CUDA_TRY(cudaGetLastError());
 }
 
 }  // namespace
 
-void launch_stage(const StageArgs& a, const TileArgs& t, int variant, int order, int nq, int ng,
-                  int flux, int prec, int block, cudaStream_t stream) {
-    dispatch<MODE_STAGE>(a, t, variant, order, nq, ng, flux, prec, block, stream);
+void launch_stage(const StageArgs& a, const TileArgs& t, int order, int nq, int flux, int prec, int ctas,
+                  cudaStream_t stream) {
+    if (a.lo_row >= 0) dispatch<MODE_STAGE_COMP>(a, t, order, nq, flux, prec, ctas, stream);
+    else dispatch<MODE_STAGE>(a, t, order, nq, flux, prec, ctas, stream);
 }
 
-void launch_residual(const StageArgs& a, const TileArgs& t, int variant, int order, int nq, int ng,
-                     int flux, int prec, int block, cudaStream_t stream) {
-    dispatch<MODE_RESIDUAL>(a, t, variant, order, nq, ng, flux, prec, block, stream);
+void launch_residual(const StageArgs& a, const TileArgs& t, int order, int nq, int flux, int prec, int ctas,
+                     cudaStream_t stream) {
+    dispatch<MODE_RESIDUAL>(a, t, order, nq, flux, prec, ctas, stream);
 }
 
 void wait_selftest(double limit_s, int* timed_out, double* waited_s) {
@@ -1261,7 +1069,7 @@ int tiled_max_ctas_per_sm(int prec, int order, int nq, int flux, int max_halo) {
 }
 
 void launch_tiled_limiter(const TileArgs& t, int ctas, int ld, void* U, const int4* conn,
-                          const double* lim, const double* jinv, const int* flags,
+                          const void* lim, const double* jinv, const int* flags,
                           const double* refs, int prec, int nq2, double gamma, double tvb_m,
                           const StepCtl* ctl, cudaStream_t stream) {
     const int cfg1 = cfg_index(3, 2), cfg2 = cfg_index(nq2, 3);
@@ -1274,44 +1082,44 @@ void launch_tiled_limiter(const TileArgs& t, int ctas, int ld, void* U, const in
 }
 
 void launch_import(int T, int ld, const double* staging, int ldh, const double* conv,
-                   const int32_t* perm, void* U, int order, int prec, const double* ref,
+                   const int32_t* perm, void* U, int order, int prec, const double* ref, int lo_row,
                    cudaStream_t stream) {
     Ref4 r{{ref[0], ref[1], ref[2], ref[3]}};
     const int grid = (T + 127) / 128;
     if (prec == RKDG_FP32) {
-        if (order == 1) import_kernel<float, 3><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<float*>(U), r);
-        else import_kernel<float, 6><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<float*>(U), r);
+        if (order == 1) import_kernel<float, 3><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<float*>(U), r, lo_row);
+        else import_kernel<float, 6><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<float*>(U), r, lo_row);
     } else {
-        if (order == 1) import_kernel<double, 3><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<double*>(U), r);
-        else import_kernel<double, 6><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<double*>(U), r);
+        if (order == 1) import_kernel<double, 3><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<double*>(U), r, -1);
+        else import_kernel<double, 6><<<grid, 128, 0, stream>>>(T, ld, staging, ldh, conv, perm, static_cast<double*>(U), r, -1);
     }
     RKDG_CUDA_TRY(cudaGetLastError());
 }
 
 void launch_export(int T, int ld, const void* U, const double* conv, const int32_t* perm,
                    double* staging, int ldh, int order, int prec, int residual_scale,
-                   const double* jinv, const double* ref, cudaStream_t stream) {
+                   const double* jinv, const double* ref, int lo_row, cudaStream_t stream) {
     Ref4 r{{ref[0], ref[1], ref[2], ref[3]}};
     const int grid = (T + 127) / 128;
     if (prec == RKDG_FP32) {
-        if (order == 1) export_kernel<float, 3><<<grid, 128, 0, stream>>>(T, ld, static_cast<const float*>(U), conv, perm, staging, ldh, residual_scale, jinv, r);
-        else export_kernel<float, 6><<<grid, 128, 0, stream>>>(T, ld, static_cast<const float*>(U), conv, perm, staging, ldh, residual_scale, jinv, r);
+        if (order == 1) export_kernel<float, 3><<<grid, 128, 0, stream>>>(T, ld, static_cast<const float*>(U), conv, perm, staging, ldh, residual_scale, jinv, r, lo_row);
+        else export_kernel<float, 6><<<grid, 128, 0, stream>>>(T, ld, static_cast<const float*>(U), conv, perm, staging, ldh, residual_scale, jinv, r, lo_row);
     } else {
-        if (order == 1) export_kernel<double, 3><<<grid, 128, 0, stream>>>(T, ld, static_cast<const double*>(U), conv, perm, staging, ldh, residual_scale, jinv, r);
-        else export_kernel<double, 6><<<grid, 128, 0, stream>>>(T, ld, static_cast<const double*>(U), conv, perm, staging, ldh, residual_scale, jinv, r);
+        if (order == 1) export_kernel<double, 3><<<grid, 128, 0, stream>>>(T, ld, static_cast<const double*>(U), conv, perm, staging, ldh, residual_scale, jinv, r, -1);
+        else export_kernel<double, 6><<<grid, 128, 0, stream>>>(T, ld, static_cast<const double*>(U), conv, perm, staging, ldh, residual_scale, jinv, r, -1);
     }
     RKDG_CUDA_TRY(cudaGetLastError());
 }
 
 void launch_totals(int T, int ld, const void* U, int order, int prec, const double* jinv,
-                   double* partial, double* out4, const double* ref, cudaStream_t stream) {
+                   double* partial, double* out4, const double* ref, int lo_row, cudaStream_t stream) {
     Ref4 r{{ref[0], ref[1], ref[2], ref[3]}};
     (void)order;
     const int n = totals_partial_count(T);
     if (prec == RKDG_FP32)
-        totals_partial_kernel<float><<<n, kTotBlock, 0, stream>>>(T, ld, static_cast<const float*>(U), jinv, partial, r);
+        totals_partial_kernel<float><<<n, kTotBlock, 0, stream>>>(T, ld, static_cast<const float*>(U), jinv, partial, r, lo_row);
     else
-        totals_partial_kernel<double><<<n, kTotBlock, 0, stream>>>(T, ld, static_cast<const double*>(U), jinv, partial, r);
+        totals_partial_kernel<double><<<n, kTotBlock, 0, stream>>>(T, ld, static_cast<const double*>(U), jinv, partial, r, -1);
     totals_final_kernel<<<1, kTotBlock, 0, stream>>>(n, partial, out4);
     RKDG_CUDA_TRY(cudaGetLastError());
 }

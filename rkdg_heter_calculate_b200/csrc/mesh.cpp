@@ -21,14 +21,36 @@
 
 namespace rkdg {
 
-uint32_t pack_info(const int8_t* shared3, const int8_t* bc3) {
+uint32_t pack_info(const int8_t* shared3, const int8_t* bc3, uint32_t lim_pair) {
     uint32_t w = 0;
     for (int k = 0; k < 3; ++k) {
         uint32_t s = shared3[k] < 0 ? 3u : (uint32_t)shared3[k];
         w |= (s & 3u) << (2 * k);
         w |= ((uint32_t)bc3[k] & 3u) << (6 + 2 * k);
     }
-    return w;
+    return w | ((lim_pair & 7u) << 12);
+}
+
+void upload_limiter(void* dev, int ld, int64_t e0, const std::vector<double>& lim, int T, int prec,
+                    cudaStream_t stream) {
+    const size_t w = prec == RKDG_FP64 ? 16 : 8;  // double2 or float2 per element and edge
+    std::vector<unsigned char> rows((size_t)3 * T * w);
+    for (int k = 0; k < 3; ++k)
+        for (int t = 0; t < T; ++t) {
+            unsigned char* d = rows.data() + ((size_t)k * T + t) * w;
+            const double a = lim[(size_t)6 * t + 2 * k], b = lim[(size_t)6 * t + 2 * k + 1];
+            if (prec == RKDG_FP64) {
+                std::memcpy(d, &a, 8);
+                std::memcpy(d + 8, &b, 8);
+            } else {
+                const float af = (float)a, bf = (float)b;
+                std::memcpy(d, &af, 4);
+                std::memcpy(d + 4, &bf, 4);
+            }
+        }
+    RKDG_CUDA_TRY(cudaMemcpy2DAsync(static_cast<unsigned char*>(dev) + (size_t)e0 * w, (size_t)ld * w, rows.data(),
+                                    (size_t)T * w, (size_t)T * w, 3, cudaMemcpyHostToDevice, stream));
+    RKDG_CUDA_TRY(cudaStreamSynchronize(stream));  // the host rows are temporaries
 }
 
 HostMesh build_mesh(const rkdg_mesh_desc& d) {
@@ -262,7 +284,10 @@ HostGeometry build_geometry(const HostMesh& m, int order, bool with_conversion, 
         g.conv_in.assign((size_t)36 * T, 0.0);
         g.conv_out.assign((size_t)36 * T, 0.0);
     }
-    if (with_limiter) g.lim.assign((size_t)18 * T, 0.0);
+    if (with_limiter) {
+        g.lim.assign((size_t)6 * T, 0.0);
+        g.lim_pair.assign(T, 0);
+    }
     double l[kMaxNQ][3], w[kMaxNQ];
     volume_rule(6, l, w);
     double psi[6][6];  // native basis at the 6 rule points
@@ -312,8 +337,10 @@ HostGeometry build_geometry(const HostMesh& m, int order, bool with_conversion, 
     }
     if (with_limiter) {
         // Cockburn & Shu (1998, J. Comput. Phys. 141:199-224, sec. 2.4) geometry
-        // per edge k: (alpha, beta, j, dir_x, dir_y, h2) with
-        // m_k - b0 = alpha (b_k - b0) + beta (b_j - b0).
+        // per edge k: (alpha, beta) and the pairing edge j with
+        // m_k - b0 = alpha (b_k - b0) + beta (b_j - b0); the direction
+        // m_k - b0 and its length (the TVB threshold scale) are formed on the
+        // device from J^-1.
         for (int t = 0; t < T; ++t) {
             const double* p = &m.xy[6 * t];
             double b0x = (p[0] + p[2] + p[4]) / 3.0, b0y = (p[1] + p[3] + p[5]) / 3.0;
@@ -358,14 +385,9 @@ HostGeometry build_geometry(const HostMesh& m, int order, bool with_conversion, 
                         bj = j;
                     }
                 }
-                double r = std::sqrt(rx * rx + ry * ry);
-                double* L = &g.lim[(size_t)18 * t + 6 * k];
-                L[0] = ba;
-                L[1] = bb;
-                L[2] = bj;
-                L[3] = rx / r;
-                L[4] = ry / r;
-                L[5] = 4 * r * r;
+                g.lim[(size_t)6 * t + 2 * k] = ba;
+                g.lim[(size_t)6 * t + 2 * k + 1] = bb;
+                if (bj == (k + 2) % 3) g.lim_pair[t] |= (uint8_t)(1u << k);
             }
         }
     }

@@ -64,7 +64,8 @@ struct HostGeometry {
     std::vector<double> area;   // [T]
     std::vector<double> conv_in;   // [T][6][6] native <- reference: b_j = sum_i a_i C[i][j]
     std::vector<double> conv_out;  // [T][6][6] reference <- native: a_i = sum_j b_j D[i][j]
-    std::vector<double> lim;       // [T][3][6] limiter geometry per edge (see kernels)
+    std::vector<double> lim;       // [T][3][2] limiter (alpha, beta) per edge (see kernels)
+    std::vector<uint8_t> lim_pair; // [T] bit k: edge k pairs with edge (k+2)%3, else (k+1)%3
 };
 
 // ------------------------------------------------------------------ mesh --
@@ -86,8 +87,15 @@ std::vector<int32_t> morton_order(const HostMesh& m);
 HostMesh permute_mesh(const HostMesh& m, const std::vector<int32_t>& perm);
 HostGeometry build_geometry(const HostMesh& m, int order, bool with_conversion, bool with_limiter);
 // Packed connectivity word: bits 0-5 shared edge (2 bits per edge),
-// bits 6-11 boundary tag (2 bits per edge).
-uint32_t pack_info(const int8_t* shared3, const int8_t* bc3);
+// bits 6-11 boundary tag (2 bits per edge), bits 12-14 the limiter's edge
+// pairing (HostGeometry::lim_pair).
+uint32_t pack_info(const int8_t* shared3, const int8_t* bc3, uint32_t lim_pair = 0);
+// The limiter table on the device: rows k = 0..2 of (alpha, beta) per
+// element, double2 (prec RKDG_FP64) or float2 (RKDG_FP32), row k of element
+// e at index k ld + e; uploads elements [e0, e0 + T) from lim [T][3][2] and
+// waits for the copy.
+void upload_limiter(void* dev, int ld, int64_t e0, const std::vector<double>& lim, int T, int prec,
+                    cudaStream_t stream);
 
 // ---------------------------------------------------------------- tiles --
 // Work decomposition of the tile-staged stage kernel: a CTA owns kTile
@@ -146,7 +154,7 @@ struct DeviceArrays {
     void* U[3] = {nullptr, nullptr, nullptr};  // state buffers (A holds U^n)
     double* jinv = nullptr;     // [2][ld][2]
     int4* conn = nullptr;       // [ld]
-    double* lim = nullptr;      // [3][ld][6] limiter geometry (when enabled)
+    void* lim = nullptr;        // [3][ld] (alpha, beta) of the limiter (when enabled)
     int32_t* perm = nullptr;    // [T]
     double* conv_in = nullptr;  // [T][36]
     double* conv_out = nullptr; // [T][36]
@@ -186,19 +194,32 @@ struct StageArgs {
     const double* far_sid;  // per-solve far-field states [solves][4], or nullptr
     int last_stage;      // compute wave max / error (and the monitor when asked) in the epilogue
     int monitor;         // last stage: also form the residual monitor max |d mean| (rho, rhoE)
+    int lo_row;          // RKDG_FP32C: state row of the cell means' low parts (in U, U0, Unew), else -1
 };
 
-// Launchers (kernels.cu).  All asynchronous on `stream`.
+// Arithmetic type of the kernels for a precision setting: RKDG_FP32C runs
+// the FP32 kernels (its extra cell-mean row is read and written in the
+// stage update only).
+inline int kernel_prec(int precision) { return precision == RKDG_FP64 ? RKDG_FP64 : RKDG_FP32; }
+// 16-byte state rows per element: FP64 two per basis function, FP32 one,
+// FP32C one plus the row of the cell means' low parts.
+inline int state_rows(int precision, int nb) {
+    return precision == RKDG_FP64 ? 2 * nb : (precision == RKDG_FP32C ? nb + 1 : nb);
+}
+
+// Launchers (kernels.cu).  All asynchronous on `stream`.  `prec` is the
+// arithmetic type of a kernel (RKDG_FP64 or RKDG_FP32; kernel_prec maps the
+// RKDG_FP32C setting to RKDG_FP32).
 void upload_tables(int nq, int ng);
-// variant: 0 owner-computes (one thread per element, both sides of every
-// edge; single solve, block = threads per block), 1 tile-staged (each
-// interior flux once per tile, traces shared; `block` = CTAs per launch,
-// 0 = one CTA per tile).  `order` 1 or 2, or 3 for a pack of P1 and P2
-// tiles (P2 tiles use nq, P1 tiles the 3/2-point rules).
-void launch_stage(const StageArgs& a, const TileArgs& t, int variant, int order, int nq, int ng,
-                  int flux, int prec, int block, cudaStream_t stream);
-void launch_residual(const StageArgs& a, const TileArgs& t, int variant, int order, int nq,
-                     int ng, int flux, int prec, int block, cudaStream_t stream);
+// The tile-staged stage kernel: one CTA per tile of kTile elements (each
+// interior flux once per tile, traces shared in shared memory), `ctas` CTAs
+// per launch looping over the tiles (0 = one CTA per tile).  `order` 1 or 2,
+// or 3 for a pack of P1 and P2 tiles (P2 tiles use nq, P1 tiles the
+// 3/2-point rules).
+void launch_stage(const StageArgs& a, const TileArgs& t, int order, int nq, int flux, int prec, int ctas,
+                  cudaStream_t stream);
+void launch_residual(const StageArgs& a, const TileArgs& t, int order, int nq, int flux, int prec, int ctas,
+                     cudaStream_t stream);
 // CFL measure per solve, one CTA per tile (resets the wave slots of solves
 // 0..nsolves-1 first; nsolves 0 leaves them as they are)
 // FP32 states store cell means as deviations from a per-solve reference
@@ -214,17 +235,21 @@ int tiled_max_ctas_per_sm(int prec, int order, int nq, int flux, int max_halo);
 // solve, solves whose control block (ctl may be null) says done are skipped;
 // ctas 0 = one CTA per tile
 void launch_tiled_limiter(const TileArgs& t, int ctas, int ld, void* U, const int4* conn,
-                          const double* lim, const double* jinv, const int* flags,
+                          const void* lim, const double* jinv, const int* flags,
                           const double* refs, int prec, int nq2, double gamma, double tvb_m,
                           const StepCtl* ctl, cudaStream_t stream);
+// Caller layout [4][nb][ldh] FP64 <-> HBM state packs.  lo_row >= 0: the
+// state is RKDG_FP32C and row lo_row holds the low part of each cell mean
+// (import splits the FP64 mean into high and low floats, export and the
+// totals add them back).
 void launch_import(int T, int ld, const double* staging, int ldh, const double* conv,
-                   const int32_t* perm, void* U, int order, int prec, const double* ref,
+                   const int32_t* perm, void* U, int order, int prec, const double* ref, int lo_row,
                    cudaStream_t stream);
 void launch_export(int T, int ld, const void* U, const double* conv, const int32_t* perm,
                    double* staging, int ldh, int order, int prec, int residual_scale,
-                   const double* jinv, const double* ref, cudaStream_t stream);
+                   const double* jinv, const double* ref, int lo_row, cudaStream_t stream);
 void launch_totals(int T, int ld, const void* U, int order, int prec, const double* jinv,
-                   double* partial, double* out4, const double* ref, cudaStream_t stream);
+                   double* partial, double* out4, const double* ref, int lo_row, cudaStream_t stream);
 int totals_partial_count(int T);
 
 }  // namespace rkdg

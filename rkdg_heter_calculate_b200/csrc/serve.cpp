@@ -92,7 +92,7 @@ struct Request {
     bool limiter = false;
     double t_final = 0, far[4] = {0, 0, 0, 0};
     std::vector<double> jinv;   // [T][4]
-    std::vector<double> lim;    // [T][18]
+    std::vector<double> lim;    // [T][3][2]
     std::vector<int32_t> conn;  // [T][4] local neighbours + packed info
     std::vector<int32_t> perm;
     TileTables tiles;           // offsets 0
@@ -120,7 +120,7 @@ struct rkdg_server {
     double* jinv = nullptr;
     int4* tcode = nullptr;
     int4* conn = nullptr;
-    double* lim = nullptr;
+    void* lim = nullptr;
     int32_t* perm = nullptr;
     int2* halo = nullptr;
     uint16_t* task = nullptr;
@@ -185,7 +185,11 @@ void* salloc(rkdg_server* s, size_t bytes) {
     return p;
 }
 
-size_t state_bytes(const rkdg_server* s) { return (size_t)24 * s->word * s->ld; }
+// the P2 row layout for every request (RKDG_FP32C: row 6 holds the low
+// parts of the cell means)
+size_t state_bytes(const rkdg_server* s) { return (size_t)16 * state_rows(s->p.precision, 6) * s->ld; }
+int kprec(const rkdg_server* s) { return kernel_prec(s->p.precision); }
+int lo_row(const rkdg_server* s) { return s->p.precision == RKDG_FP32C ? 6 : -1; }
 
 void coeffs(int rk, int st, double& a, double& c) {
     if (st == 0) a = 0, c = 1;
@@ -213,9 +217,10 @@ void enqueue_step(rkdg_server* s) {
         a.U0 = st == 0 ? nullptr : s->U[pl[1]];
         a.Unew = s->U[pl[2]];
         a.last_stage = st == s->p.rk - 1;
-        launch_stage(a, s->tiles, 1, 3, s->p.nq, 3, s->p.flux, s->p.precision, s->ctas, s->stream);
+        a.lo_row = lo_row(s);
+        launch_stage(a, s->tiles, 3, s->p.nq, s->p.flux, kprec(s), s->ctas, s->stream);
         launch_tiled_limiter(s->tiles, s->ctas, s->ld, s->U[pl[2]], s->conn, s->lim, s->jinv, s->flags,
-                             s->far, s->p.precision, s->p.nq, s->p.gamma, s->p.tvb_m, s->ctl, s->stream);
+                             s->far, kprec(s), s->p.nq, s->p.gamma, s->p.tvb_m, s->ctl, s->stream);
     }
 }
 
@@ -244,7 +249,7 @@ void upload(rkdg_server* s, Request& r) {
         for (int k = 0; k < 3; ++k)
             if (cn[4 * t + k] >= 0) cn[4 * t + k] += (int32_t)e;
     h2d(s, reinterpret_cast<int32_t*>(s->conn) + 4 * e, cn.data(), cn.size());
-    if (r.limiter) h2d(s, s->lim + 18 * e, r.lim.data(), r.lim.size());
+    if (r.limiter) upload_limiter(s->lim, s->ld, e, r.lim, T, kprec(s), s->stream);
     h2d(s, s->perm + e, r.perm.data(), r.perm.size());
     std::vector<int32_t> hl(r.tiles.halo);
     for (size_t i = 0; i < hl.size(); i += 2) hl[i] += (int32_t)e;
@@ -254,7 +259,7 @@ void upload(rkdg_server* s, Request& r) {
     RKDG_CUDA_TRY(cudaMemcpyAsync(s->staging, r.U0.data(), sizeof(double) * r.U0.size(),
                                   cudaMemcpyHostToDevice, s->stream));
     launch_import(T, s->ld, s->staging, T, nullptr, s->perm + e, static_cast<char*>(s->U[0]) + 16 * e,
-                  r.order, s->p.precision, r.far, s->stream);
+                  r.order, kprec(s), r.far, lo_row(s), s->stream);
     StepCtl c{};
     c.cfl = s->p.cfl;
     c.t_final = r.t_final > 0 ? r.t_final : 1e-300;
@@ -302,7 +307,7 @@ void rebuild_tiles(rkdg_server* s, const std::vector<std::shared_ptr<Request>>& 
         t.desc = scratch;
         t.ntiles = (int)(dn.size() / 8);
         t.ntiles_dev = nullptr;
-        launch_wave(t, s->ld, s->U[0], s->p.precision, s->jinv, s->p.gamma, s->ctl, 0, s->far, s->stream);
+        launch_wave(t, s->ld, s->U[0], kprec(s), s->jinv, s->p.gamma, s->ctl, 0, s->far, s->stream);
     }
     RKDG_CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->tiles_dirty = false;
@@ -312,7 +317,7 @@ void retire(rkdg_server* s, Request& r, bool failed) {
     if (!failed) {
         r.result.assign((size_t)4 * r.nb * r.T, 0.0);
         launch_export(r.T, s->ld, static_cast<char*>(s->U[0]) + 16 * r.e_off, nullptr, s->perm + r.e_off,
-                      s->staging, r.T, r.order, s->p.precision, 0, nullptr, r.far, s->stream);
+                      s->staging, r.T, r.order, kprec(s), 0, nullptr, r.far, lo_row(s), s->stream);
         RKDG_CUDA_TRY(cudaMemcpyAsync(r.result.data(), s->staging, sizeof(double) * r.result.size(),
                                       cudaMemcpyDeviceToHost, s->stream));
         RKDG_CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -488,7 +493,7 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
         s = new rkdg_server();
         s->p = p;
         s->device = dev;
-        s->word = p.precision == RKDG_FP32 ? 4 : 8;
+        s->word = p.precision == RKDG_FP64 ? 8 : 4;
         s->max_slots = max_slots;
         // per element: 3 state buffers (P2 rows), J^-1, tile codes, connectivity,
         // limiter geometry, permutation, ~1 halo entry, 2 task entries, descriptors
@@ -496,7 +501,8 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
         // codes, connectivity, limiter geometry, permutation, one halo entry,
         // three flux tasks, tile descriptors; plus the FP64 staging buffer
         // of the largest admissible request and a fixed reserve
-        const size_t per_elem = (size_t)3 * 24 * s->word + 32 + 16 + 16 + 144 + 4 + 8 + 6 + 1;
+        const size_t per_elem = (size_t)3 * 16 * state_rows(p.precision, 6) + 32 + 16 + 16 +
+                                (kernel_prec(p.precision) == RKDG_FP64 ? 48 : 24) + 4 + 8 + 6 + 1;
         const size_t fixed = (size_t)64 << 20, stage_per_elem = 24 * sizeof(double);
         if (budget < fixed + 4096 * (per_elem + stage_per_elem))
             throw Error{RKDG_ERR_NOMEM, "HBM budget too small"};
@@ -522,7 +528,7 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
         RKDG_CUDA_TRY(cudaMemsetAsync(s->jinv, 0, sizeof(double) * 4 * (size_t)s->ld, s->stream));
         s->tcode = (int4*)salloc(s, sizeof(int4) * (size_t)s->cap);
         s->conn = (int4*)salloc(s, sizeof(int4) * (size_t)s->cap);
-        s->lim = (double*)salloc(s, sizeof(double) * 18 * (size_t)s->cap);
+        s->lim = salloc(s, (size_t)3 * s->ld * (kernel_prec(p.precision) == RKDG_FP64 ? 16 : 8));
         s->perm = (int32_t*)salloc(s, sizeof(int32_t) * (size_t)s->cap);
         s->halo = (int2*)salloc(s, sizeof(int2) * (size_t)s->hcap + kTablePad);
         s->task = (uint16_t*)salloc(s, sizeof(uint16_t) * (size_t)s->kcap + kTablePad);
@@ -552,7 +558,7 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
         for (int i = max_slots - 1; i >= 0; --i) s->free_slots.push_back(i);
         s->active.assign(max_slots, nullptr);
         // persistent grid, and a graph of one step whose tile count is read on the device
-        const int per_sm = std::max(1, tiled_max_ctas_per_sm(p.precision, 3, p.nq, p.flux, kPoolHalo));
+        const int per_sm = std::max(1, tiled_max_ctas_per_sm(kernel_prec(p.precision), 3, p.nq, p.flux, kPoolHalo));
         s->ctas = prop.multiProcessorCount * per_sm;
         s->tiles.code = s->tcode;
         s->tiles.desc = s->desc;
@@ -608,7 +614,8 @@ int rkdg_server_submit(rkdg_server* s, const rkdg_mesh_desc* mesh, int32_t order
         r->conn.resize((size_t)4 * m.T);
         for (int t = 0; t < m.T; ++t) {
             for (int k = 0; k < 3; ++k) r->conn[4 * t + k] = m.nbr[3 * t + k];
-            r->conn[4 * t + 3] = (int32_t)pack_info(&m.shared[3 * t], &m.bc[3 * t]);
+            r->conn[4 * t + 3] = (int32_t)pack_info(&m.shared[3 * t], &m.bc[3 * t],
+                                                    g.lim_pair.empty() ? 0u : g.lim_pair[t]);
         }
         r->perm = m.perm;
         r->tiles = build_tiles(m, 0, 0, order, 0, 0);

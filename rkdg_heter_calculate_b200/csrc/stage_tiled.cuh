@@ -265,13 +265,6 @@ __device__ __forceinline__ void load_staged(const unsigned char* stg, int x, Rea
     }
 }
 
-// With RKDG_HOLD_STATE 1, FP32 tiles keep the stage input in registers from
-// phase A to the update; by default both precisions read it again (an L2
-// hit), which keeps FP32 tiles within the 80 registers of six CTAs per SM.
-#ifndef RKDG_HOLD_STATE
-#define RKDG_HOLD_STATE 0
-#endif
-
 // The part of a tile's work that needs only its descriptors, J^-1 rows and
 // edge codes: edge normals and codes into shared memory, the solve's
 // reference state, the halo and task list entries.  Formed while the tile's
@@ -344,7 +337,6 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                                            const TilePre<Real>& pre, Real (*s_red)[3], const double* s_dt) {
     constexpr int CFG = cfg_index(NQ, NG);
     constexpr int BT = kTile;
-    constexpr bool HOLD = RKDG_HOLD_STATE && sizeof(Real) == 4;
     using V4 = Vec4<Real>;
     const Tab<Real>& tb = tab<Real>(CFG);
     const int HM = ta.max_halo;
@@ -397,7 +389,6 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     const double det = pre.det;
     const Real inv_area = pre.inv_area;
     const Real j00 = pre.j00, j01 = pre.j01, j10 = pre.j10, j11 = pre.j11;  // rows of 2 area J^-1
-    Real m_st[4];  // the stored cell mean (a deviation in FP32)
     // psi_0 is the constant K00 at every volume and edge point: its term is
     // formed once per state
     const Real k00 = tb.vphi[0][0];
@@ -420,7 +411,6 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
             Real mfull[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
-                m_st[v] = u[0][v];
                 mfull[v] = u[0][v] + refv[v];  // the cell mean itself
                 if constexpr (!DEV) u[0][v] = mfull[v];
             }
@@ -507,10 +497,6 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
                 }
                 put4(s_tr + (k * NG + g) * BT + tid, t);
             }
-        if constexpr (HOLD && !DEV) {
-#pragma unroll
-            for (int v = 0; v < 4; ++v) u[0][v] = m_st[v];  // the stored values for the update
-        }
     }
     cp_async_wait_all();
     __syncthreads();  // s_ephi visible below; own traces complete; halo states landed
@@ -717,17 +703,21 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     // per step would accumulate into the state); L = det J^-1 R
     const Real dt = (Real)(dtd * det), cb = (Real)a.b;
     Real u0m[4] = {Real(0), Real(0), Real(0), Real(0)};
+    // RKDG_FP32C (comp): row 0 is updated in FP64 below, not here
+    constexpr bool comp = PK && MODE == MODE_STAGE_COMP;
     {
-        if constexpr (!HOLD) load_state<Real, NB>(U, a.ld, ee, u);  // stored values (L2 hit)
+        load_state<Real, NB>(U, a.ld, ee, u);  // stored values (L2 hit)
         if (a.U0 != nullptr) {
             Real u0[NB][4];
             load_state<Real, NB>(static_cast<const Real*>(a.U0), a.ld, ee, u0);
             if constexpr (PK) {
                 const float2 dt2 = make_float2(dt, dt), cb2 = make_float2(cb, cb);
 #pragma unroll
-                for (int i = 0; i < NB; ++i)
-                    set4(R[i], f2fma(cb2, f2fma(dt2, lo2(R[i]), f2sub(lo2(u[i]), lo2(u0[i]))), lo2(u0[i])),
-                         f2fma(cb2, f2fma(dt2, hi2(R[i]), f2sub(hi2(u[i]), hi2(u0[i]))), hi2(u0[i])));
+                for (int i = 0; i < NB; ++i) {
+                    const float2 l = f2fma(cb2, f2fma(dt2, lo2(R[i]), f2sub(lo2(u[i]), lo2(u0[i]))), lo2(u0[i]));
+                    const float2 h = f2fma(cb2, f2fma(dt2, hi2(R[i]), f2sub(hi2(u[i]), hi2(u0[i]))), hi2(u0[i]));
+                    if (i > 0 || !comp) set4(R[i], l, h);
+                }
             } else {
 #pragma unroll
                 for (int i = 0; i < NB; ++i)
@@ -740,8 +730,11 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
             if constexpr (PK) {
                 const float2 dt2 = make_float2(dt, dt), cb2 = make_float2(cb, cb);
 #pragma unroll
-                for (int i = 0; i < NB; ++i)
-                    set4(R[i], f2mul(cb2, f2fma(dt2, lo2(R[i]), lo2(u[i]))), f2mul(cb2, f2fma(dt2, hi2(R[i]), hi2(u[i]))));
+                for (int i = 0; i < NB; ++i) {
+                    const float2 l = f2mul(cb2, f2fma(dt2, lo2(R[i]), lo2(u[i])));
+                    const float2 h = f2mul(cb2, f2fma(dt2, hi2(R[i]), hi2(u[i])));
+                    if (i > 0 || !comp) set4(R[i], l, h);
+                }
             } else {
 #pragma unroll
                 for (int i = 0; i < NB; ++i)
@@ -750,7 +743,41 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
             }
         }
     }
-    if (active) store_state<Real, NB>(Uout, a.ld, e, R);
+    if constexpr (comp) {
+        // RKDG_FP32C: the cell mean is the unevaluated sum of its stored high
+        // part (row 0) and low part (row lo_row).  Rows 1.. are stored as
+        // updated above; R[0] still holds the mean's residual, and the
+        // mean's update runs in FP64 from both parts, split again into a
+        // high and a low float, so the mean's storage rounding does not
+        // accumulate over the stages.
+        if (active) store_rows<Real, 1, NB>(Uout, a.ld, e, R);
+        const size_t lr = (size_t)a.lo_row * a.ld;
+        const float4 h = __ldg(reinterpret_cast<const float4*>(a.U) + ee);
+        const float4 l = __ldg(reinterpret_cast<const float4*>(a.U) + lr + ee);
+        float4 h0 = make_float4(0.f, 0.f, 0.f, 0.f), l0 = h0;
+        if (a.U0 != nullptr) {
+            h0 = __ldg(reinterpret_cast<const float4*>(a.U0) + ee);
+            l0 = __ldg(reinterpret_cast<const float4*>(a.U0) + lr + ee);
+        }
+        const double dtdet = dtd * det;
+        const float hv[4] = {h.x, h.y, h.z, h.w}, lv[4] = {l.x, l.y, l.z, l.w};
+        const float h0v[4] = {h0.x, h0.y, h0.z, h0.w}, l0v[4] = {l0.x, l0.y, l0.z, l0.w};
+        float nl[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const double m = (double)hv[v] + (double)lv[v], m0 = (double)h0v[v] + (double)l0v[v];
+            const double y = m0 + a.b * ((m - m0) + dtdet * (double)R[0][v]);
+            const float yh = (float)y;
+            R[0][v] = yh;
+            nl[v] = (float)(y - (double)yh);
+        }
+        if (active) {
+            reinterpret_cast<float4*>(a.Unew)[e] = make_float4(R[0][0], R[0][1], R[0][2], R[0][3]);
+            reinterpret_cast<float4*>(a.Unew)[lr + e] = make_float4(nl[0], nl[1], nl[2], nl[3]);
+        }
+    } else {
+        if (active) store_state<Real, NB>(Uout, a.ld, e, R);
+    }
     if (a.last_stage) {
         // CFL wave maximum (and the residual monitor when asked) of the new
         // state: a max over each warp in the working precision into s_red;
@@ -843,8 +870,8 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
         const int ex = d0.x + ((int)threadIdx.x < d0.y ? (int)threadIdx.x : 0);
         const double2 r0 = __ldg(jinv2 + ex), r1 = __ldg(jinv2 + a.ld + ex);
         const int4 code = __ldg(ta.code + ex);
-        const int done = MODE == MODE_STAGE ? a.ctl[d0.z].done : 0;
-        if (MODE == MODE_STAGE && threadIdx.x == 0) s_dt = a.ctl[d0.z].dt;
+        const int done = MODE != MODE_RESIDUAL ? a.ctl[d0.z].done : 0;
+        if (MODE != MODE_RESIDUAL && threadIdx.x == 0) s_dt = a.ctl[d0.z].dt;
         const TilePre<Real> pre = tile_pre<Real>(a, ta, d0, d1, r0, r1, code, smem_raw);
         const bool ok = mbar_wait(&s_bar, parity);
         if (__syncthreads_or(!ok)) {  // also: every thread has seen this phase complete
@@ -863,6 +890,6 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
             tile_stage<Real, 3, 3, 2, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre, s_red,
                                                  &s_dt);
         __syncthreads();  // shared memory is reused by the next tile
-        if (MODE == MODE_STAGE && a.last_stage && threadIdx.x == 0) tile_maxima_atomic<Real>(a, a.ctl + d0.z, s_red);
+        if (MODE != MODE_RESIDUAL && a.last_stage && threadIdx.x == 0) tile_maxima_atomic<Real>(a, a.ctl + d0.z, s_red);
     }
 }

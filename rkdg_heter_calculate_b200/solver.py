@@ -32,7 +32,7 @@ from . import capi
 
 _FLUX = {"llf": capi.FLUX_LLF, "hllc": capi.FLUX_HLLC}
 _LIM = {None: capi.LIMITER_NONE, "none": capi.LIMITER_NONE, "tvb": capi.LIMITER_TVB}
-_PREC = {"fp64": capi.FP64, "fp32": capi.FP32}
+_PREC = {"fp64": capi.FP64, "fp32": capi.FP32, "fp32c": capi.FP32C}
 _BASIS = {"reference": capi.BASIS_REFERENCE, "native": capi.BASIS_NATIVE}
 
 

@@ -4,7 +4,13 @@ oracle/_ref/librkdg_ref.so by oracle/Makefile) on small seeded meshes.
 
     make -C oracle libref && python tests/golden/make_golden.py
 
-Each .npz holds the mesh (vertices, triangles, neighbours, boundary tags),
+It also stores the reference's own NACA0012 mesh set (input/previous/ of the
+checkout: vertices, triangles and neighbours as its files give them, and
+the boundary tags of its |x|,|y| > 15 far-field rule) as
+naca0012_previous.npz, the mesh the C++ caller test drives through the C
+ABI where the checkout is absent.
+
+Each vortex/box .npz holds the mesh (vertices, triangles, neighbours, boundary tags),
 the reference-native parameters (P2, 7-point volume rule, 3-point edges,
 LLF, SSP-RK3), an initial state in the reference basis, and the reference's
 outputs: dt, R(U0), the state after each of the three stages of the first
@@ -16,6 +22,7 @@ from __future__ import annotations
 
 import os
 import sys
+import tempfile
 
 import numpy as np
 
@@ -60,7 +67,25 @@ def run_case(name, mesh, alpha_deg, mach, state_fn):
     print(out, mesh.ntri, "tris, dt0", dt0, "monitor", res1[0])
 
 
+def naca_fixture():
+    """The reference's NACA0012 mesh set, read by the library's reader of its
+    file format (rkdg_read_mesh) from the checkout."""
+    from rkdg_heter_calculate_b200 import capi
+
+    src = os.path.join(ref.reference_dir(), "input", "previous")
+    with tempfile.TemporaryDirectory() as d:
+        os.symlink(src, os.path.join(d, "input"))
+        V, T, N = capi.read_mesh(d, "input/mesh.conf")
+    nb, _, bc = capi.build_connectivity(V, T)
+    assert (nb == N).all()
+    out = os.path.join(HERE, "naca0012_previous.npz")
+    np.savez_compressed(out, vertices=V, tris=T.astype(np.int32), neighbours=N.astype(np.int32),
+                        bc=bc.astype(np.int8))
+    print(out, T.shape[0], "tris,", V.shape[0], "vertices")
+
+
 def main():
+    naca_fixture()
     m1 = meshgen.periodic_structured(8, 8, jitter=0.15, seed=5)
     run_case("periodic_8x8_vortex", m1, 45.0, 0.4,
              lambda m, c: vortex_state(m, c, 6))

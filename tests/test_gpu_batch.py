@@ -41,7 +41,7 @@ def solo(m, order, U, far, precision, steps, t_final=0.0):
     return out, t, n
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("precision", ["fp32", "fp32c", "fp64"])
 def test_batch_equals_solo_runs(precision):
     cs = cases()
     b = Batch([c[0] for c in cs], [c[1] for c in cs], precision=precision, flux="hllc", cfl=0.2,

@@ -19,7 +19,7 @@ def solver(mesh, precision, order=2, limiter=None, far=FAR):
                           limiter=limiter, **kw)
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("precision", ["fp32", "fp32c", "fp64"])
 @pytest.mark.parametrize("order", [1, 2])
 def test_resume_is_bitwise(tmp_path, precision, order):
     mesh = meshgen.periodic_delaunay(16, seed=5)

@@ -67,7 +67,7 @@ def submit(srv, req):
     return srv.submit(m, order, U, tf, farfield=far, limiter=lim)
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("precision", ["fp32", "fp32c", "fp64"])
 def test_results_same_alone_and_in_the_mix(precision):
     reqs = requests()
     with Server(256 * MB, max_slots=8, precision=precision, **SERVER) as srv:

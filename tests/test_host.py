@@ -7,10 +7,12 @@ import tempfile
 import numpy as np
 import pytest
 
+from oracle import ref
 from rkdg_heter_calculate_b200 import capi, meshgen, vortex
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_MESH = "/root/reference/multi_gpuRkdg/input/previous"
+# the reference's NACA0012 mesh set (present where the reference checkout is)
+REF_MESH = os.path.join(ref.reference_dir(), "input", "previous")
 
 
 def declared_symbols():
@@ -154,3 +156,24 @@ def test_delaunay_generators():
     s = meshgen.forward_step(h=1.0 / 40, seed=3)
     assert (s.bc[s.neighbours < 0] > 0).all()
     assert np.isclose(s.areas().sum(), 3.0 - 2.4 * 0.2)
+
+
+def test_cpp_caller_compiles_and_links():
+    """The C++ program that keeps the reference's call sequence
+    (tests/cpp/reference_sequence.cpp) compiles against include/rkdg.h and
+    links against librkdg.so; without its mesh files it reports the reader's
+    error and exits non-zero (no device is touched)."""
+    import shutil
+    import subprocess
+
+    if shutil.which("g++") is None:
+        pytest.skip("g++ absent")
+    pkg = os.path.join(ROOT, "rkdg_heter_calculate_b200")
+    with tempfile.TemporaryDirectory() as d:
+        exe = os.path.join(d, "reference_sequence")
+        subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror",
+                        os.path.join(ROOT, "tests", "cpp", "reference_sequence.cpp"),
+                        "-I", os.path.join(ROOT, "include"), "-L", pkg, "-lrkdg", f"-Wl,-rpath,{pkg}",
+                        "-o", exe], check=True, capture_output=True, text=True)
+        r = subprocess.run([exe, "1"], cwd=d, capture_output=True, text=True, timeout=60)
+        assert r.returncode == 1 and "rkdg_read_mesh" in r.stderr
