@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--workload", default="batched", choices=["batched", "vortex", "serving", "step"])
     ap.add_argument("--no-step", action="store_true", help="skip the Mach-3 step FP32/FP64 comparison")
     ap.add_argument("--step-h", type=int, default=400, help="1/h of the Mach-3 step lattice")
+    ap.add_argument("--step-times", default="0.05,0.5", help="output times of the Mach-3 step runs")
     ap.add_argument("--no-step-sensitivity", action="store_true",
                     help="skip the FP64 run from an initial state perturbed at FP32 rounding level")
     ap.add_argument("--nsolves", type=int, default=64)
@@ -70,13 +71,14 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--precision", default="all",
                     help="comma list of fp32, fp32c, fp64, or 'all'")
-    ap.add_argument("--headline", default="fp32", choices=["fp32", "fp32c"],
-                    help="FP32 form whose batched rate is the line's value")
+    ap.add_argument("--headline", default="fp32c", choices=["fp32", "fp32c"],
+                    help="FP32 form whose batched rate is the line's value (fp32c: the form that "
+                         "holds the vortex L2 error within 1.05x of FP64)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI run")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving sweep")
-    ap.add_argument("--serve-requests", type=int, default=16, help="requests per arrival-rate point")
-    ap.add_argument("--serve-loads", default="0.5,0.9",
+    ap.add_argument("--serve-requests", type=int, default=100, help="requests per arrival-rate point")
+    ap.add_argument("--serve-loads", default="0.5,0.7,0.8,0.9",
                     help="arrival rates as fractions of the measured saturated request rate")
     return ap.parse_args()
 
@@ -321,7 +323,7 @@ def run_batched(args, dist, peak, peak_kind):
         b = Batch(meshes, orders, precision=prec, flux="hllc", rk=3, nq=6, cfl=0.2, farfields=fars)
         for i, U in enumerate(states):
             b.set_state(i, U)
-        ctas, torder = b.autotune()
+        ctas, torder, tile = b.autotune()
         for i, U in enumerate(states):
             b.set_state(i, U)
             b.set_time(i, 0.0)
@@ -334,8 +336,8 @@ def run_batched(args, dist, peak, peak_kind):
         alg = sum(m.ntri * bytes_per_elem_stage(nb, prec) for m, nb in zip(meshes, nbs))
         roof = roofline(b.time_stage(0, 10), b.time_stage(1, 10), b.time_stage(2, 10), alg, peak, peak_kind,
                         "tiled_stage_kernel (P1+P2 tiles, one launch per stage)",
-                        measured_traffic("tiled_stage_kernel_batched_fp32.md")
-                        if prec == "fp32" and args.nsolves == 64 else None)
+                        measured_traffic(f"tiled_stage_kernel_batched_{prec}.md")
+                        if args.nsolves == 64 else None)
         e2e = None
         if not args.no_e2e:
             hosts = [pinned_like(U) for U in states]
@@ -367,7 +369,7 @@ def run_batched(args, dist, peak, peak_kind):
                 beta, ui, vi = par[i]
                 acc.append(vortex.l2_error(m, b.state(i), lambda X, Y: vortex.exact(X, Y, t_end[i], beta, GAMMA, ui, vi)))
         out[prec] = {"value": value, "ms_per_step": ms / K, "roofline": roof, "e2e": e2e,
-                     "clocks": clocks, "shape": {"ctas": ctas, "tile_order": torder},
+                     "clocks": clocks, "shape": {"ctas": ctas, "tile_order": torder, "tile": tile},
                      "l2": acc, "tris": [int(m.ntri) for m in meshes], "orders": [int(o) for o in orders]}
         b.close()
     info = {"solves": len(meshes), "triangles": int(sum(m.ntri for m in meshes)),
@@ -451,8 +453,9 @@ def run_step(args, dist, peak, peak_kind):
     U[:, 0, :] = far[:, None]
     a = m.areas()
     kw = dict(order=1, nq=3, ng=2, flux="llf", rk=3, limiter="tvb", tvb_m=50.0, cfl=0.3, farfield=far)
-    runs = [("fp64", U), ("fp32", U), ("fp32c", U)]
-    if not args.no_step_sensitivity:
+    times = [float(x) for x in args.step_times.split(",")]
+    runs = [(p, U) for p in precisions(args)]
+    if "fp64" in precisions(args) and not args.no_step_sensitivity:
         rng = np.random.default_rng(7)
         Up = U.copy()
         Up[:, 0, :] *= 1.0 + 6e-8 * rng.uniform(-1.0, 1.0, (4, m.ntri))
@@ -465,7 +468,7 @@ def run_step(args, dist, peak, peak_kind):
         out = {}
         steps = 0
         ms = 0.0
-        for tt in (0.05, 0.5):
+        for tt in times:
             box = {}
             ms += event_time(s.stream(), lambda: box.update(r=s.advance(10 ** 8, t_final=tt)), dist)
             steps += box["r"][1]
@@ -478,11 +481,12 @@ def run_step(args, dist, peak, peak_kind):
         return float(np.sum(a * np.abs(x - y)) / np.sum(a * np.abs(y)))
 
     line = {"workload": "Mach-3 step, jittered Delaunay h = 1/%d (seed 3), %d triangles, P1, LLF, TVB M = 50, "
-                        "SSP-RK3, CFL 0.3, to t = 0.5" % (args.step_h, m.ntri),
+                        "SSP-RK3, CFL 0.3, to t = %g" % (args.step_h, m.ntri, times[-1]),
             "triangles": int(m.ntri),
-            "rel_L1_rho_fp32_vs_fp64": {str(t): rel(res["fp32"]["rho"][t], res["fp64"]["rho"][t]) for t in (0.05, 0.5)},
-            "rel_L1_rho_fp32c_vs_fp64": {str(t): rel(res["fp32c"]["rho"][t], res["fp64"]["rho"][t]) for t in (0.05, 0.5)},
             "definition": "sum_e A_e |rho_x - rho64| / sum_e A_e |rho64| over cell means"}
+    for p in ("fp32", "fp32c"):
+        if p in res and "fp64" in res:
+            line[f"rel_L1_rho_{p}_vs_fp64"] = {str(t): rel(res[p]["rho"][t], res["fp64"]["rho"][t]) for t in times}
     for name in res:
         r = res[name]
         per_stage_ms = r["ms"] / (3 * r["steps"])
@@ -504,7 +508,7 @@ def run_step(args, dist, peak, peak_kind):
         line[name] = d
     if "fp64_perturbed" in res:
         line["rel_L1_rho_fp64_perturbed_vs_fp64"] = {
-            str(t): rel(res["fp64_perturbed"]["rho"][t], res["fp64"]["rho"][t]) for t in (0.05, 0.5)}
+            str(t): rel(res["fp64_perturbed"]["rho"][t], res["fp64"]["rho"][t]) for t in times}
     return line
 
 
@@ -541,8 +545,11 @@ def serving_catalogue(seed=5):
 
 def serving_requests(cat, sizes, n, rng):
     """n requests: kind 50/50, triangle count log-uniform in [2k, 500k]
-    (snapped to the nearest catalogue size), vortex P1/P2 50/50 without
-    limiter, step P1 with the TVB limiter, final time U[0.1, 1.0]."""
+    (snapped to the nearest catalogue size), vortex P1/P2 50/50 with HLLC and
+    no limiter, step P1 with LLF and the TVB limiter (the limited-flow
+    configuration's method; with Davis wave-speed bounds the HLLC flux goes
+    non-physical at the step corner under P1 + TVB), final time U[0.1, 1.0].
+    Each: (mesh, order, U0, t_final, far field, limiter, flux)."""
     out = []
     lo, hi = math.log(sizes[0]), math.log(sizes[-1])
     for _ in range(n):
@@ -552,17 +559,18 @@ def serving_requests(cat, sizes, n, rng):
         if kind == "vortex":
             m, U2, U1, far = cat["vortex"][lvl]
             order = 2 if rng.random() < 0.5 else 1
-            out.append((m, order, U2 if order == 2 else U1, tf, far, False))
+            out.append((m, order, U2 if order == 2 else U1, tf, far, False, "hllc"))
         else:
             m, U1, far = cat["step"][lvl]
-            out.append((m, 1, U1, tf, far, True))
+            out.append((m, 1, U1, tf, far, True, "llf"))
     return out
 
 
 def serve_point(srv, reqs, rate):
     """Submits reqs with Poisson arrivals at `rate` requests/s (inf: all at
     once) from a pool of submitter threads; returns per-request latencies
-    (completion - arrival, seconds), DOF-stage/s over the point and counts."""
+    (completion - arrival, seconds), DOF-stage/s over the point, the split of
+    DOF-stage updates by request kind and where the loop's time went."""
     import concurrent.futures as cf
 
     from rkdg_heter_calculate_b200 import capi
@@ -572,29 +580,35 @@ def serve_point(srv, reqs, rate):
     gaps = rng.exponential(1.0 / rate, len(reqs)) if math.isfinite(rate) else np.zeros(len(reqs))
     gaps[0] = 0.0
     arrive = np.cumsum(gaps)
-    st0 = srv.stats()
+    st0, tm0 = srv.stats(), srv.timing()
     pool = cf.ThreadPoolExecutor(8)
     t0 = clock()
     futs = []
-    for (m, order, U, tf, far, lim), at in zip(reqs, arrive):
+    for (m, order, U, tf, far, lim, flux), at in zip(reqs, arrive):
         d = t0 + at - clock()
         if d > 0:
             time.sleep(d)
-        futs.append(pool.submit(srv.submit, m, order, U, tf, far, lim))
-    lat, failed, t_end = [], 0, t0
-    for f, at in zip(futs, arrive):
+        futs.append(pool.submit(srv.submit, m, order, U, tf, far, lim, flux))
+    lat, queue_wait, failed, t_end = [], [], 0, t0
+    kind_dofs = {"vortex": 0.0, "step": 0.0}
+    for f, at, (m, order, U, tf, far, lim, flux) in zip(futs, arrive, reqs):
         try:
             r = srv.wait(f.result())
             lat.append(r.completed - (t0 + at))
+            queue_wait.append(r.admitted - r.submitted)
             t_end = max(t_end, r.completed)
+            kind_dofs["step" if lim else "vortex"] += r.steps * 3 * 4 * (3 if order == 1 else 6) * m.ntri
         except capi.RkdgError:
             failed += 1
     pool.shutdown()
-    st1 = srv.stats()
+    st1, tm1 = srv.stats(), srv.timing()
     wall = t_end - t0
-    return {"latency": np.array(lat), "dof_per_s": (st1["dof_stage_updates"] - st0["dof_stage_updates"]) / wall,
+    return {"latency": np.array(lat), "queue_wait": np.array(queue_wait),
+            "dof_per_s": (st1["dof_stage_updates"] - st0["dof_stage_updates"]) / wall,
             "wall_s": wall, "failed": failed, "busy_frac": (st1["busy_seconds"] - st0["busy_seconds"]) / wall,
-            "peak_in_flight": st1["peak_in_flight"]}
+            "peak_in_flight": st1["peak_in_flight"],
+            "loop_s": {k: tm1[k] - tm0[k] for k in ("admit_s", "retire_s", "step_s")},
+            "chunks": tm1["chunks"] - tm0["chunks"], "kind_dofs": kind_dofs}
 
 
 def run_serving(args, dist):
@@ -607,9 +621,9 @@ def run_serving(args, dist):
                 tvb_m=50.0) as srv:
         # warm-up: one small request of each kind
         for r in (serving_requests(cat, sizes, 4, np.random.default_rng(99))):
-            m, order, U, tf, far, lim = r
+            m, order, U, tf, far, lim, flux = r
             try:
-                srv.wait(srv.submit(m, order, U, min(tf, 0.05), far, lim))
+                srv.wait(srv.submit(m, order, U, min(tf, 0.05), far, lim, flux))
             except Exception:
                 pass
         # one request set, offered all at once and then at Poisson rates that
@@ -623,18 +637,29 @@ def run_serving(args, dist):
     out = []
     for f, rate, p in points:
         lat = p["latency"]
+        pc = {q: dist.max(float(np.percentile(lat, q))) if len(lat) else None for q in (50, 90, 99)}
+        kd = p["kind_dofs"]
+        tot = max(1.0, kd["vortex"] + kd["step"])
         out.append({"load": f, "lambda_req_per_s": None if not math.isfinite(rate) else round(rate, 3),
-                    "p50_s": dist.max(float(np.percentile(lat, 50))) if len(lat) else None,
-                    "p99_s": dist.max(float(np.percentile(lat, 99))) if len(lat) else None,
+                    "p50_s": pc[50], "p90_s": pc[90], "p99_s": pc[99],
+                    "mean_s": float(lat.mean()) if len(lat) else None,
+                    "max_s": float(lat.max()) if len(lat) else None,
+                    "queue_wait_p50_s": float(np.percentile(p["queue_wait"], 50)) if len(lat) else None,
                     "dof_stage_per_s": dist.sum(p["dof_per_s"]), "wall_s": round(p["wall_s"], 3),
                     "completed": int(len(lat)), "failed": p["failed"],
-                    "busy_frac": round(p["busy_frac"], 3), "peak_in_flight": p["peak_in_flight"]})
+                    "busy_frac": round(p["busy_frac"], 3), "peak_in_flight": p["peak_in_flight"],
+                    "loop_time_frac": {k: round(v / p["wall_s"], 4) for k, v in p["loop_s"].items()},
+                    "step_chunks": p["chunks"],
+                    "dof_share_step_requests": round(kd["step"] / tot, 4)})
     return {"workload": f"Poisson arrivals (default_rng(5)) of isentropic-vortex and Mach-3-step requests "
                         f"50/50, triangles log-uniform in [2k, 500k] snapped to {SERVE_LEVELS} mesh sizes "
-                        "per kind, vortex P1/P2 50/50, step P1 with TVB (M=50), final time U[0.1, 1.0]; "
-                        "FP32, LLF, SSP-RK3, CFL 0.2; 8 GiB pool, 64 slots",
+                        "per kind, vortex P1/P2 50/50 with HLLC, step P1 with LLF and TVB (M=50), final time "
+                        "U[0.1, 1.0]; FP32, SSP-RK3, CFL 0.2; 8 GiB pool, 64 slots",
             "requests_per_point": n, "saturated_req_per_s": round(cap_rate, 3),
             "latency": "completion - arrival, host preprocessing and result read-back included",
+            "loop_time": "fractions of each point's wall time the serving loop spent uploading admitted "
+                         "requests, retiring finished ones, and running step chunks (graph launches and the "
+                         "control-block read that ends each chunk of 4 steps)",
             "points": out}
 
 

@@ -201,10 +201,50 @@ int rkdg_time_stage(rkdg_ctx* ctx, int32_t s, int32_t reps, double* ms_per_launc
  * loads it until exit; ntri is limited to 1,048,576 (larger meshes are
  * rejected with RKDG_ERR_INVALID).  The first call on a device looks up that
  * array's device address (cudaGetSymbolAddress), so make it before any
- * stream capture.  Calls that overlap on one GPU share the array and race;
- * serialise them.  Calls no cudaMalloc/cudaFree. */
+ * stream capture; the address is kept for the process, so resetting the
+ * device (cudaDeviceReset) between calls is not supported.  Calls that
+ * overlap on one GPU share the array and race; serialise them.  Calls no
+ * cudaMalloc/cudaFree.  The means may be the caller's whole state in the
+ * reference layout [4][nbasis][ld0], passed in place with ld = nbasis ld0. */
 int rkdg_conservation_totals_noalloc(int32_t ntri, const double* d_means, int32_t ld,
                                      const double* d_area, double* d_totals, void* stream);
+
+/* ---- domain decomposition (one partition of a mesh per device) ---------- */
+/* A partition of a mesh shared by several devices (one process per GPU):
+ * elements [0, n_owned) are the partition's own, in the caller's order (no
+ * reordering: the caller orders them for locality), and elements
+ * [n_owned, ntri) are halo copies of the neighbouring partitions' elements
+ * that share an edge with an owned one (their other edges may be given as
+ * boundary edges with any tag; they are never used).  Halo copies are not
+ * updated, and are left out of the CFL maximum and the conservation totals.
+ * The caller refreshes them before every stage from their owners
+ * (rkdg_gather_rows on the owner, a device-to-device transfer such as NCCL
+ * send/recv, rkdg_scatter_rows here), takes the minimum of the partitions'
+ * rkdg_compute_dt for each step, and advances with rkdg_save_old and
+ * rkdg_stage; with the TVB limiter, rkdg_stage leaves it out, and the caller
+ * refreshes the halo means (the first mean_rows rows) of the stage output
+ * and then calls rkdg_limit.  rkdg_step and rkdg_advance refuse a
+ * partition.
+ * Replaces the reference's per-rank set-up of its MPI decomposition
+ * (partition file and interface elements, src/unstructuredgrid.cpp:290-318;
+ * inner-boundary ghost cells, src/unstructuredgrid.cpp:502-526; the
+ * interface-index handshake, src/sendboundaryindex.cpp:8-37). */
+int rkdg_create_part(const rkdg_mesh_desc* mesh, const rkdg_params* params, int32_t n_owned,
+                     rkdg_ctx** out);
+/* 16-byte state rows per element: all of them (a full halo refresh) and the
+ * leading rows that hold the cell means (a means-only refresh). */
+int rkdg_part_rows(const rkdg_ctx* ctx, int32_t* state_rows, int32_t* mean_rows);
+/* Rows 0..nrows-1 of the current state of elements d_index[0..n) (device
+ * int32, caller element numbers of a partition) to or from the device
+ * buffer d_buf [n][nrows][16 bytes], ordered on the context's stream and
+ * asynchronous (rkdg_sync waits and reports an index out of range as
+ * RKDG_ERR_INVALID).  They replace the device-host copies and the buffer
+ * packing around the reference's MPI_Isend/MPI_Irecv halo exchange
+ * (RkdgAdvance::commuInfo, src/rkdgadvance.cpp:287-409). */
+int rkdg_gather_rows(rkdg_ctx* ctx, const int32_t* d_index, int32_t n, int32_t nrows, void* d_buf);
+int rkdg_scatter_rows(rkdg_ctx* ctx, const int32_t* d_index, int32_t n, int32_t nrows, const void* d_buf);
+/* Waits for the context's stream and reports any error its kernels flagged. */
+int rkdg_sync(rkdg_ctx* ctx);
 
 /* ---- output ------------------------------------------------------------ */
 /* Writes the cell means as the reference's Tecplot solution.plt
@@ -224,12 +264,14 @@ int rkdg_set_residual_log(rkdg_ctx* ctx, const char* path);
  * rkdg_checkpoint_save writes the context's full state to path: a header
  * (format tag, triangle count, order, precision, a hash of the mesh in its
  * internal order, time, step count, the CFL wave maximum and monitor, the
- * far-field state) followed by the state rows exactly as held on the device.
- * A run restored from it continues bit for bit as if never stopped.
- * rkdg_checkpoint_load restores such a file into a context built on the
- * same mesh, order and precision (RKDG_ERR_INVALID otherwise; an FP32 file
- * also needs the same far-field state, its cell means being stored relative
- * to it); RKDG_ERR_IO when the file cannot be read or written. */
+ * far-field state, the quadrature rules, flux, limiter, RK scheme, gamma,
+ * CFL number and TVB constant) followed by the state rows exactly as held on
+ * the device.  A run restored from it continues bit for bit as if never
+ * stopped.  rkdg_checkpoint_load restores such a file into a context built
+ * on the same mesh, order, precision, method and physics (RKDG_ERR_INVALID
+ * otherwise; an FP32 or FP32C file also needs the same far-field state, its
+ * cell means being stored relative to it); RKDG_ERR_IO when the file cannot
+ * be read or written. */
 int rkdg_checkpoint_save(rkdg_ctx* ctx, const char* path);
 int rkdg_checkpoint_load(rkdg_ctx* ctx, const char* path);
 
@@ -262,11 +304,18 @@ int rkdg_batch_get_state(rkdg_batch* b, int32_t solve, double* U, int32_t ld);
 int rkdg_batch_advance(rkdg_batch* b, int32_t nsteps, const double* t_final, double* t,
                        int32_t* steps);
 int rkdg_batch_set_time(rkdg_batch* b, int32_t solve, double t);
-/* Picks the persistent grid size and tile order by timing candidate launch
- * shapes on this batch; returns the chosen CTA count (0: one per tile) and
- * tile order (0 solve order, 1 P2 tiles first). */
-int rkdg_batch_autotune(rkdg_batch* b, int32_t* ctas, int32_t* tile_order);
+/* Picks the tile size (128 or 256 elements, one thread per element), the
+ * persistent grid size and the tile order by timing candidate launch shapes
+ * on this batch's live state; returns the chosen CTA count (0: one per
+ * tile), tile order (0 solve order, 1 P2 tiles first) and tile size (any
+ * pointer may be NULL).  The reference fixes its block size from its
+ * configuration file (threadsperblock, src/cudarkdgsolver.cu:22). */
+int rkdg_batch_autotune(rkdg_batch* b, int32_t* ctas, int32_t* tile_order, int32_t* tile);
 int rkdg_batch_set_shape(rkdg_batch* b, int32_t ctas, int32_t tile_order);
+/* Rebuilds the tile tables for tiles of 128 or 256 elements.  A solve's
+ * result does not depend on the tile size beyond rounding (interface
+ * fluxes are formed once per tile pair). */
+int rkdg_batch_set_tile(rkdg_batch* b, int32_t tile);
 /* Mean device milliseconds of one launch of stage s over all solves (the
  * last stage with its CFL and monitor epilogue, as it runs in a step). */
 int rkdg_batch_time_stage(rkdg_batch* b, int32_t s, int32_t reps, double* ms_per_launch);
@@ -287,9 +336,9 @@ int rkdg_batch_get_stream(const rkdg_batch* b, void** stream);
  * process). */
 typedef struct rkdg_server rkdg_server;
 
-/* params: precision, flux, rk, gamma, cfl, tvb_m and nq (P2 rule, 6) shared
- * by all requests; hbm_budget_bytes bounds the pool; max_slots bounds the
- * number of solves in flight. */
+/* params: precision, rk, gamma, cfl, tvb_m and nq (P2 rule, 6) shared by
+ * all requests, flux the default of rkdg_server_submit; hbm_budget_bytes
+ * bounds the pool; max_slots bounds the number of solves in flight. */
 int rkdg_server_create(const rkdg_params* params, size_t hbm_budget_bytes, int32_t max_slots,
                        rkdg_server** out);
 /* Stops the loop (in-flight solves are abandoned) and frees everything. */
@@ -300,6 +349,13 @@ int rkdg_server_destroy(rkdg_server* s);
  * tiles) runs in the calling thread.  Returns the request id. */
 int rkdg_server_submit(rkdg_server* s, const rkdg_mesh_desc* mesh, int32_t order, const double* U0,
                        double t_final, const double* farfield, int32_t limiter, int64_t* id);
+/* As rkdg_server_submit, with the request's own Riemann flux (RKDG_FLUX_*;
+ * rkdg_server_submit uses params->flux).  The loop runs the LLF and the
+ * HLLC requests' tiles as two launches per stage on two streams, joined
+ * before the next stage. */
+int rkdg_server_submit_method(rkdg_server* s, const rkdg_mesh_desc* mesh, int32_t order, const double* U0,
+                              double t_final, const double* farfield, int32_t limiter, int32_t flux,
+                              int64_t* id);
 /* Waits up to timeout_s (< 0: forever) for request id; status 0 queued,
  * 1 running, 2 done, 3 failed.  On done, U (may be NULL) receives the final
  * state [4][nbasis][ntri], and times[3] (may be NULL) the submit, admit and
@@ -313,6 +369,23 @@ int rkdg_server_stats(rkdg_server* s, double* dof_stage_updates, double* busy_se
                       int64_t* completed, int32_t* peak_in_flight, int64_t* capacity_elements);
 /* Seconds on the loop's steady clock (the clock of rkdg_server_wait's times). */
 double rkdg_server_clock(void);
+/* Where the loop's time went: seconds uploading admitted requests (tables,
+ * state, tile lists; the device idles meanwhile), seconds retiring finished
+ * ones (state export and copy back), seconds of step chunks (graph launches
+ * and the control-block read that ends each chunk of 4 steps), and the
+ * number of chunks. */
+int rkdg_server_timing(rkdg_server* s, double* admit_s, double* retire_s, double* step_s, int64_t* chunks);
+/* Health of the loop: RKDG_OK while it runs, with the number of queued and
+ * in-flight requests (either may be NULL).  Once the loop has stopped on an
+ * error (a failed CUDA call) it returns that error's code, with the message
+ * in rkdg_last_error(), and zero counts: every request that was queued or in
+ * flight then has status 3 (failed), later submits are refused, and the
+ * server can only be destroyed. */
+int rkdg_server_status(rkdg_server* s, int32_t* queued, int32_t* in_flight);
+/* Test support, no reference counterpart: the loop stops as on a failed CUDA
+ * call before launching its (after_chunks + 1)-th next chunk of steps.
+ * Nothing is done to the device; it exercises the failure handling above. */
+int rkdg_server_inject_fault(rkdg_server* s, int32_t after_chunks);
 
 /* ---- diagnostics ------------------------------------------------------- */
 /* No reference counterpart.  The stage kernels wait on an mbarrier for each

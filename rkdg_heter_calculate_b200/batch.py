@@ -86,10 +86,13 @@ class Batch:
         return t, n
 
     def autotune(self):
-        c = C.c_int32()
-        o = C.c_int32()
-        capi.check(capi.lib().rkdg_batch_autotune(self.h, C.byref(c), C.byref(o)))
-        return c.value, o.value
+        """Times the candidate launch shapes; returns (CTAs, tile order, tile size)."""
+        c, o, t = C.c_int32(), C.c_int32(), C.c_int32()
+        capi.check(capi.lib().rkdg_batch_autotune(self.h, C.byref(c), C.byref(o), C.byref(t)))
+        return c.value, o.value, t.value
+
+    def set_tile(self, tile):
+        capi.check(capi.lib().rkdg_batch_set_tile(self.h, int(tile)))
 
     def set_shape(self, ctas, tile_order=0):
         capi.check(capi.lib().rkdg_batch_set_shape(self.h, ctas, tile_order))

@@ -93,7 +93,9 @@ def lib():
             "rkdg_batch_get_state": (C.c_int, [vp, C.c_int32, _dp, C.c_int32]),
             "rkdg_batch_advance": (C.c_int, [vp, C.c_int32, _dp, _dp, C.POINTER(C.c_int32)]),
             "rkdg_batch_set_time": (C.c_int, [vp, C.c_int32, C.c_double]),
-            "rkdg_batch_autotune": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+            "rkdg_batch_autotune": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                              C.POINTER(C.c_int32)]),
+            "rkdg_batch_set_tile": (C.c_int, [vp, C.c_int32]),
             "rkdg_batch_set_shape": (C.c_int, [vp, C.c_int32, C.c_int32]),
             "rkdg_batch_time_stage": (C.c_int, [vp, C.c_int32, C.c_int32, _dp]),
             "rkdg_batch_get_sizes": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32),
@@ -103,11 +105,21 @@ def lib():
             "rkdg_server_destroy": (C.c_int, [vp]),
             "rkdg_server_submit": (C.c_int, [vp, C.POINTER(MeshDesc), C.c_int32, _dp, C.c_double, _dp,
                                              C.c_int32, C.POINTER(C.c_int64)]),
+            "rkdg_server_submit_method": (C.c_int, [vp, C.POINTER(MeshDesc), C.c_int32, _dp, C.c_double, _dp,
+                                                    C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
             "rkdg_server_wait": (C.c_int, [vp, C.c_int64, C.c_double, C.POINTER(C.c_int32), _dp, _dp,
                                            C.POINTER(C.c_int32)]),
             "rkdg_server_stats": (C.c_int, [vp, _dp, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_int32),
                                             C.POINTER(C.c_int64)]),
             "rkdg_server_clock": (C.c_double, []),
+            "rkdg_create_part": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(Params), C.c_int32, C.POINTER(vp)]),
+            "rkdg_part_rows": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+            "rkdg_gather_rows": (C.c_int, [vp, vp, C.c_int32, C.c_int32, vp]),
+            "rkdg_scatter_rows": (C.c_int, [vp, vp, C.c_int32, C.c_int32, vp]),
+            "rkdg_sync": (C.c_int, [vp]),
+            "rkdg_server_status": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+            "rkdg_server_timing": (C.c_int, [vp, _dp, _dp, _dp, C.POINTER(C.c_int64)]),
+            "rkdg_server_inject_fault": (C.c_int, [vp, C.c_int32]),
             "rkdg_checkpoint_save": (C.c_int, [vp, C.c_char_p]),
             "rkdg_checkpoint_load": (C.c_int, [vp, C.c_char_p]),
             "rkdg_set_residual_log": (C.c_int, [vp, C.c_char_p]),

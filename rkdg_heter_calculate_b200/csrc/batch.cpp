@@ -40,7 +40,9 @@ struct rkdg_batch {
     StepCtl* h_ctl = nullptr;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
-    int ctas = 0, tile_order = 0;
+    int ctas = 0, tile_order = 0, tile = kTile;
+    std::vector<HostMesh> topo;  // per solve (internal order): T, neighbours, shared edges, tags
+    size_t table_bytes = 0;      // device bytes of the tile tables (rebuilt with the tile size)
     bool wave_valid = false;
     std::vector<bool> have_state;
     TileArgs tiles{};
@@ -157,6 +159,48 @@ void enqueue_step(rkdg_batch* b) {
     }
 }
 
+// (Re)builds the tile tables of every solve for tiles of b->tile elements
+// and uploads them: edge codes, descriptors (in the chosen tile order), halo
+// and flux-task lists.
+void build_batch_tiles(rkdg_batch* b) {
+    std::vector<int32_t> code, halo;
+    std::vector<uint16_t> task;
+    b->desc_solve.clear();
+    b->ntiles = 0;
+    b->max_halo = 4;
+    for (int s = 0; s < b->S; ++s) {
+        TileTables tt = build_tiles(b->topo[s], b->off[s], s, b->order[s], (int)(halo.size() / 2),
+                                    (int)task.size(), -1, b->tile);
+        code.insert(code.end(), tt.code.begin(), tt.code.end());
+        halo.insert(halo.end(), tt.halo.begin(), tt.halo.end());
+        task.insert(task.end(), tt.task.begin(), tt.task.end());
+        b->desc_solve.insert(b->desc_solve.end(), tt.desc.begin(), tt.desc.end());
+        b->max_halo = std::max(b->max_halo, tt.max_halo);
+        b->ntiles += tt.ntiles;
+    }
+    code.resize((size_t)4 * b->ld, 0);
+    for (void* p : {(void*)b->tcode, (void*)b->tdesc, (void*)b->halo, (void*)b->task}) cudaFree(p);
+    b->bytes -= b->table_bytes;
+    const size_t before = b->bytes;
+    b->tcode = (int4*)balloc(b, sizeof(int32_t) * code.size());
+    h2d(b, reinterpret_cast<int32_t*>(b->tcode), code);
+    b->tdesc = (int4*)balloc(b, sizeof(int32_t) * b->desc_solve.size());
+    upload_desc(b);
+    b->halo = (int2*)balloc(b, sizeof(int32_t) * std::max<size_t>(2, halo.size()) + kTablePad);
+    h2d(b, reinterpret_cast<int32_t*>(b->halo), halo);
+    b->task = (uint16_t*)balloc(b, sizeof(uint16_t) * std::max<size_t>(1, task.size()) + kTablePad);
+    h2d(b, b->task, task);
+    b->table_bytes = b->bytes - before;
+    b->tiles.code = b->tcode;
+    b->tiles.desc = b->tdesc;
+    b->tiles.halo = b->halo;
+    b->tiles.task = b->task;
+    b->tiles.max_halo = b->max_halo;
+    b->tiles.ntiles = b->ntiles;
+    b->tiles.tile = b->tile;
+    sync(b);  // host tables go out of scope
+}
+
 void drop_graph(rkdg_batch* b) {
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
@@ -234,27 +278,26 @@ int rkdg_batch_create(int32_t nsolves, const rkdg_mesh_desc* meshes, const int32
 
         // pack the solves
         std::vector<double> jv;      // [total][4]
-        std::vector<int32_t> code, halo, perm;
-        std::vector<uint16_t> task;
+        std::vector<int32_t> perm;
         int64_t total = 0;
         int maxT = 0;
         for (int s = 0; s < nsolves; ++s) {
             HostMesh m = build_mesh(meshes[s]);
             if (p.reorder) m = permute_mesh(m, morton_order(m));
             HostGeometry g = build_geometry(m, orders[s], false, false);
-            TileTables tt = build_tiles(m, (int)total, s, orders[s], (int)(halo.size() / 2), (int)task.size());
             b->T.push_back(m.T);
             b->off.push_back((int)total);
             maxT = std::max(maxT, m.T);
             jv.insert(jv.end(), g.jinv.begin(), g.jinv.end());
-            code.insert(code.end(), tt.code.begin(), tt.code.end());
-            halo.insert(halo.end(), tt.halo.begin(), tt.halo.end());
-            task.insert(task.end(), tt.task.begin(), tt.task.end());
-            b->desc_solve.insert(b->desc_solve.end(), tt.desc.begin(), tt.desc.end());
             perm.insert(perm.end(), m.perm.begin(), m.perm.end());
-            b->max_halo = std::max(b->max_halo, tt.max_halo);
-            b->ntiles += tt.ntiles;
-            total += m.T;
+            // the connectivity the tile tables are built from (tile size may change)
+            HostMesh t;
+            t.T = m.T;
+            t.nbr = std::move(m.nbr);
+            t.shared = std::move(m.shared);
+            t.bc = std::move(m.bc);
+            b->topo.push_back(std::move(t));
+            total += b->T.back();
             if (total > (int64_t)1 << 30) throw Error{RKDG_ERR_INVALID, "batch too large"};
         }
         b->total = total;
@@ -273,15 +316,7 @@ int rkdg_batch_create(int32_t nsolves, const rkdg_mesh_desc* meshes, const int32
         }
         b->jinv = (double*)balloc(b, sizeof(double) * jp.size());
         h2d(b, b->jinv, jp);
-        code.resize((size_t)4 * ld, 0);
-        b->tcode = (int4*)balloc(b, sizeof(int32_t) * code.size());
-        h2d(b, reinterpret_cast<int32_t*>(b->tcode), code);
-        b->tdesc = (int4*)balloc(b, sizeof(int32_t) * b->desc_solve.size());
-        upload_desc(b);
-        b->halo = (int2*)balloc(b, sizeof(int32_t) * std::max<size_t>(2, halo.size()) + kTablePad);
-        h2d(b, reinterpret_cast<int32_t*>(b->halo), halo);
-        b->task = (uint16_t*)balloc(b, sizeof(uint16_t) * std::max<size_t>(1, task.size()) + kTablePad);
-        h2d(b, b->task, task);
+        build_batch_tiles(b);
         b->perm = (int32_t*)balloc(b, sizeof(int32_t) * perm.size());
         h2d(b, b->perm, perm);
         std::vector<double> far((size_t)4 * nsolves);
@@ -294,12 +329,6 @@ int rkdg_batch_create(int32_t nsolves, const rkdg_mesh_desc* meshes, const int32
         b->ctl = (StepCtl*)balloc(b, sizeof(StepCtl) * nsolves);
         for (int s = 0; s < nsolves; ++s) b->h_ctl[s].cfl = p.cfl;
         push(b);
-        b->tiles.code = b->tcode;
-        b->tiles.desc = b->tdesc;
-        b->tiles.halo = b->halo;
-        b->tiles.task = b->task;
-        b->tiles.max_halo = b->max_halo;
-        b->tiles.ntiles = b->ntiles;
         sync(b);
         *out = b;
     });
@@ -461,7 +490,28 @@ int rkdg_batch_set_shape(rkdg_batch* b, int32_t ctas, int32_t tile_order) {
     });
 }
 
-int rkdg_batch_autotune(rkdg_batch* b, int32_t* ctas_out, int32_t* order_out) {
+int rkdg_batch_set_tile(rkdg_batch* b, int32_t tile) {
+    return guarded([&] {
+        if (!b || (tile != 128 && tile != 256)) throw Error{RKDG_ERR_INVALID, "rkdg_batch_set_tile: 128 or 256"};
+        RKDG_CUDA_TRY(cudaSetDevice(b->device));
+        if (tile == b->tile) return;
+        sync(b);
+        const int old = b->tile;
+        b->tile = tile;
+        drop_graph(b);
+        build_batch_tiles(b);
+        b->wave_valid = false;  // the CFL measure is redone over the new tiles at the next advance
+        if (!tiled_fits(kprec(b), b->ord, b->p.flux, b->max_halo, tile)) {
+            const int mh = b->max_halo;
+            b->tile = old;
+            build_batch_tiles(b);
+            throw Error{RKDG_ERR_INVALID, "tiles of " + std::to_string(tile) + " elements: halo lists of " +
+                                              std::to_string(mh) + " entries exceed the shared memory of a CTA"};
+        }
+    });
+}
+
+int rkdg_batch_autotune(rkdg_batch* b, int32_t* ctas_out, int32_t* order_out, int32_t* tile_out) {
     return guarded([&] {
         if (!b) throw Error{RKDG_ERR_INVALID, "null batch"};
         for (int s = 0; s < b->S; ++s)
@@ -469,33 +519,40 @@ int rkdg_batch_autotune(rkdg_batch* b, int32_t* ctas_out, int32_t* order_out) {
         RKDG_CUDA_TRY(cudaSetDevice(b->device));
         cudaDeviceProp prop;
         RKDG_CUDA_TRY(cudaGetDeviceProperties(&prop, b->device));
-        const int per_sm = std::max(1, tiled_max_ctas_per_sm(kprec(b), b->ord, b->p.nq, b->p.flux,
-                                                              b->tiles.max_halo));
-        const int wave = prop.multiProcessorCount * per_sm;
-        std::vector<int> cand_ctas = {0, wave, 2 * wave, 4 * wave};
-        std::vector<int> cand_order = {0};
-        if (b->ord == 3) cand_order.push_back(1);
         double best = 1e300;
-        int bc = 0, bo = 0;
+        int bc = 0, bo = 0, bt = b->tile;
         const int stage = b->p.rk > 1 ? 1 : 0;  // a stage that also reads U^n
-        for (int o : cand_order)
-            for (int c : cand_ctas) {
-                if (c > 0 && c >= b->ntiles) continue;
-                int rc = rkdg_batch_set_shape(b, c, o);
-                if (rc != RKDG_OK) throw Error{rc, "autotune: set_shape failed"};
-                double ms = 0;
-                rc = rkdg_batch_time_stage(b, stage, 5, &ms);
-                if (rc != RKDG_OK) throw Error{rc, "autotune: timing failed"};
-                if (ms < best) {
-                    best = ms;
-                    bc = c;
-                    bo = o;
+        for (int tile : {128, 256}) {
+            int rc = rkdg_batch_set_tile(b, tile);
+            if (rc == RKDG_ERR_INVALID) continue;  // this tile size does not fit the batch's halo lists
+            if (rc != RKDG_OK) throw Error{rc, "autotune: set_tile failed"};
+            const int per_sm = std::max(1, tiled_max_ctas_per_sm(kprec(b), b->ord, b->p.nq, b->p.flux,
+                                                                  b->tiles.max_halo, tile));
+            const int wave = prop.multiProcessorCount * per_sm;
+            std::vector<int> cand_order = {0};
+            if (b->ord == 3) cand_order.push_back(1);
+            for (int o : cand_order)
+                for (int c : {0, wave, 2 * wave, 4 * wave}) {
+                    if (c > 0 && c >= b->ntiles) continue;
+                    rc = rkdg_batch_set_shape(b, c, o);
+                    if (rc != RKDG_OK) throw Error{rc, "autotune: set_shape failed"};
+                    double ms = 0;
+                    rc = rkdg_batch_time_stage(b, stage, 5, &ms);
+                    if (rc != RKDG_OK) throw Error{rc, "autotune: timing failed"};
+                    if (ms < best) {
+                        best = ms;
+                        bc = c;
+                        bo = o;
+                        bt = tile;
+                    }
                 }
-            }
-        int rc = rkdg_batch_set_shape(b, bc, bo);
+        }
+        int rc = rkdg_batch_set_tile(b, bt);
+        if (rc == RKDG_OK) rc = rkdg_batch_set_shape(b, bc, bo);
         if (rc != RKDG_OK) throw Error{rc, "autotune: set_shape failed"};
         if (ctas_out) *ctas_out = bc;
         if (order_out) *order_out = bo;
+        if (tile_out) *tile_out = bt;
     });
 }
 

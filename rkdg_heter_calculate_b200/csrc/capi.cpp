@@ -29,6 +29,7 @@ using namespace rkdg;
 struct rkdg_ctx {
     rkdg_params p{};
     int T = 0, ld = 0, nb = 0;
+    int T_own = 0;  // elements the context updates; [T_own, T) are a partition's halo copies
     int device = 0;
     HostMesh mesh;  // internal (possibly reordered) order
     std::vector<double> area;
@@ -186,7 +187,9 @@ void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out, bool monitor 
     a.last_stage = s == c->p.rk - 1;
     a.monitor = monitor ? 1 : 0;
     launch_stage(a, c->tiles, c->p.order, c->p.nq, c->p.flux, kprec(c), c->ctas, c->stream);
-    if (c->p.limiter == RKDG_LIMITER_TVB)
+    // a partition applies its limiter by rkdg_limit once the halo means of
+    // the stage output have been exchanged
+    if (c->p.limiter == RKDG_LIMITER_TVB && c->T_own == c->T)
         launch_tiled_limiter(c->tiles, 0, c->ld, c->d.U[out], c->d.conn, c->d.lim, c->d.jinv, nullptr,
                              c->d.far, kprec(c), c->p.nq, c->p.gamma, c->p.tvb_m, c->d.ctl,
                              c->stream);
@@ -280,12 +283,19 @@ void rkdg_default_params(rkdg_params* p) {
     p->farfield[3] = 0.5 * 1.0 * ut * ut + 1.0 / (gamma - 1);
 }
 
-int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx** out) {
+}  // extern "C"
+
+namespace {
+
+// rkdg_create and rkdg_create_part: n_owned < 0 for a whole mesh.
+int create_ctx(const rkdg_mesh_desc* mesh, const rkdg_params* params, int32_t n_owned, rkdg_ctx** out) {
     rkdg_ctx* c = nullptr;
     int rc = guarded([&] {
         if (!mesh || !params || !out) throw Error{RKDG_ERR_INVALID, "rkdg_create: null argument"};
         *out = nullptr;
         check_params(*params);
+        if (n_owned >= 0 && (n_owned == 0 || n_owned > mesh->ntri))
+            throw Error{RKDG_ERR_INVALID, "rkdg_create_part: n_owned must be in [1, ntri]"};
         int dev = 0;
         cudaError_t e = cudaGetDevice(&dev);
         if (e != cudaSuccess) {
@@ -303,9 +313,11 @@ int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx*
         c->p = *params;
         c->nb = params->order == 1 ? 3 : 6;
         HostMesh m = build_mesh(*mesh);
-        if (params->reorder) m = permute_mesh(m, morton_order(m));
+        // a partition keeps its caller's order: owned elements first, halo copies after
+        if (params->reorder && n_owned < 0) m = permute_mesh(m, morton_order(m));
         c->mesh = std::move(m);
         c->T = c->mesh.T;
+        c->T_own = n_owned < 0 ? c->T : n_owned;
         c->ld = (c->T + 127) / 128 * 128;
         HostGeometry g = build_geometry(c->mesh, params->order, false,
                                         params->limiter == RKDG_LIMITER_TVB);
@@ -346,7 +358,7 @@ int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx*
             upload_limiter(c->d.lim, ld, 0, g.lim, T, kprec(c), c->stream);
         }
         {
-            TileTables tt = build_tiles(c->mesh, 0, 0, params->order, 0, 0);
+            TileTables tt = build_tiles(c->mesh, 0, 0, params->order, 0, 0, c->T_own);
             c->d.tcode = (int4*)dev_alloc(c, sizeof(int32_t) * tt.code.size());
             c->d.tdesc = (int4*)dev_alloc(c, sizeof(int32_t) * tt.desc.size());
             c->d.halo = (int2*)dev_alloc(c, sizeof(int32_t) * std::max<size_t>(2, tt.halo.size()) + kTablePad);
@@ -380,6 +392,56 @@ int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx*
     });
     if (rc != RKDG_OK && c) destroy_ctx(c);
     return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rkdg_create(const rkdg_mesh_desc* mesh, const rkdg_params* params, rkdg_ctx** out) {
+    return create_ctx(mesh, params, -1, out);
+}
+
+int rkdg_create_part(const rkdg_mesh_desc* mesh, const rkdg_params* params, int32_t n_owned, rkdg_ctx** out) {
+    return create_ctx(mesh, params, n_owned, out);
+}
+
+int rkdg_part_rows(const rkdg_ctx* c, int32_t* state_rows_out, int32_t* mean_rows) {
+    return guarded([&] {
+        if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        if (state_rows_out) *state_rows_out = state_rows(c->p.precision, c->nb);
+        if (mean_rows) *mean_rows = c->p.precision == RKDG_FP64 ? 2 : 1;
+    });
+}
+
+int rkdg_gather_rows(rkdg_ctx* c, const int32_t* d_index, int32_t n, int32_t nrows, void* d_out) {
+    return guarded([&] {
+        if (!c || n < 0 || nrows < 1 || nrows > state_rows(c->p.precision, c->nb) || (n > 0 && (!d_index || !d_out)))
+            throw Error{RKDG_ERR_INVALID, "rkdg_gather_rows: bad arguments"};
+        require_state(c);
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        launch_rows(true, c->d.U[c->cur], c->ld, c->T, d_index, n, nrows, d_out, &c->d.ctl->error, c->stream);
+    });
+}
+
+int rkdg_scatter_rows(rkdg_ctx* c, const int32_t* d_index, int32_t n, int32_t nrows, const void* d_in) {
+    return guarded([&] {
+        if (!c || n < 0 || nrows < 1 || nrows > state_rows(c->p.precision, c->nb) || (n > 0 && (!d_index || !d_in)))
+            throw Error{RKDG_ERR_INVALID, "rkdg_scatter_rows: bad arguments"};
+        require_state(c);
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        launch_rows(false, c->d.U[c->cur], c->ld, c->T, d_index, n, nrows, const_cast<void*>(d_in),
+                    &c->d.ctl->error, c->stream);
+    });
+}
+
+int rkdg_sync(rkdg_ctx* c) {
+    return guarded([&] {
+        if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        pull_ctl(c);
+        check_error_flag(c);
+    });
 }
 
 int rkdg_destroy(rkdg_ctx* ctx) {
@@ -547,6 +609,8 @@ int rkdg_limit(rkdg_ctx* c) {
 int rkdg_step(rkdg_ctx* c, double dt, double* dt_used, double* monitor) {
     return guarded([&] {
         if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        if (c->T_own != c->T)
+            throw Error{RKDG_ERR_INVALID, "a partition context advances stage by stage (rkdg_stage) with halo exchanges"};
         require_state(c);
         RKDG_CUDA_TRY(cudaSetDevice(c->device));
         normalise_buffers(c);
@@ -572,6 +636,8 @@ int rkdg_step(rkdg_ctx* c, double dt, double* dt_used, double* monitor) {
 int rkdg_advance(rkdg_ctx* c, int32_t nsteps, double t_final, double* t, int32_t* steps_done) {
     return guarded([&] {
         if (!c || nsteps < 0) throw Error{RKDG_ERR_INVALID, "rkdg_advance: bad arguments"};
+        if (c->T_own != c->T)
+            throw Error{RKDG_ERR_INVALID, "a partition context advances stage by stage (rkdg_stage) with halo exchanges"};
         require_state(c);
         RKDG_CUDA_TRY(cudaSetDevice(c->device));
         normalise_buffers(c);
@@ -694,9 +760,9 @@ int rkdg_conservation_totals(rkdg_ctx* c, double totals[4]) {
         if (!c || !totals) throw Error{RKDG_ERR_INVALID, "bad arguments"};
         require_state(c);
         RKDG_CUDA_TRY(cudaSetDevice(c->device));
-        const int n = totals_partial_count(c->T);
+        const int n = totals_partial_count(c->T_own);
         double* out4 = c->d.partial + (size_t)4 * n;
-        launch_totals(c->T, c->ld, c->d.U[c->cur], c->p.order, kprec(c), c->d.jinv,
+        launch_totals(c->T_own, c->ld, c->d.U[c->cur], c->p.order, kprec(c), c->d.jinv,
                       c->d.partial, out4, c->p.farfield, lo_row(c), c->stream);
         RKDG_CUDA_TRY(cudaMemcpyAsync(totals, out4, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         sync(c);
@@ -772,6 +838,9 @@ int rkdg_write_solution(rkdg_ctx* c, const char* path) {
 // ------------------------------------------------------ checkpoint / resume
 namespace {
 
+// Version 2 also records the method (rules, flux, limiter, RK scheme) and
+// the physics (gamma, CFL number, TVB constant) the saved CFL wave maximum
+// and state belong to; a context with other settings refuses the file.
 struct CheckpointHeader {
     char magic[8];
     uint32_t version;
@@ -781,7 +850,10 @@ struct CheckpointHeader {
     int32_t step, pad;
     unsigned long long wave_bits, mon_bits[2];
     double farfield[4];
+    int32_t nq, ng, flux, limiter, rk, pad2;
+    double gamma, cfl, tvb_m;
 };
+constexpr uint32_t kCkptVersion = 2;
 constexpr char kCkptMagic[8] = {'R', 'K', 'D', 'G', 'C', 'K', 'P', '1'};
 
 // FNV-1a over the internal-order vertex coordinates of every triangle: the
@@ -812,7 +884,7 @@ int rkdg_checkpoint_save(rkdg_ctx* c, const char* path) {
         sync(c);
         CheckpointHeader h{};
         std::memcpy(h.magic, kCkptMagic, 8);
-        h.version = 1;
+        h.version = kCkptVersion;
         h.ntri = c->T;
         h.order = c->p.order;
         h.nbasis = c->nb;
@@ -825,6 +897,14 @@ int rkdg_checkpoint_save(rkdg_ctx* c, const char* path) {
         h.mon_bits[0] = c->h_ctl->mon_bits[0];
         h.mon_bits[1] = c->h_ctl->mon_bits[1];
         for (int v = 0; v < 4; ++v) h.farfield[v] = c->p.farfield[v];
+        h.nq = c->p.nq;
+        h.ng = c->p.ng;
+        h.flux = c->p.flux;
+        h.limiter = c->p.limiter;
+        h.rk = c->p.rk;
+        h.gamma = c->p.gamma;
+        h.cfl = c->p.cfl;
+        h.tvb_m = c->p.tvb_m;
         std::ofstream f(path, std::ios::binary);
         if (!f) throw Error{RKDG_ERR_IO, std::string("cannot open ") + path + " for writing"};
         f.write(reinterpret_cast<const char*>(&h), sizeof(h));
@@ -841,13 +921,19 @@ int rkdg_checkpoint_load(rkdg_ctx* c, const char* path) {
         CheckpointHeader h{};
         f.read(reinterpret_cast<char*>(&h), sizeof(h));
         if (!f) throw Error{RKDG_ERR_IO, std::string("short read from ") + path};
-        if (std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != 1)
+        if (std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != kCkptVersion)
             throw Error{RKDG_ERR_INVALID, std::string(path) + " is not a checkpoint of this format"};
         const int packs = state_packs(c);
         if (h.ntri != c->T || h.order != c->p.order || h.precision != c->p.precision || h.packs != packs)
             throw Error{RKDG_ERR_INVALID, "checkpoint was written for another triangle count, order or precision"};
         if (h.mesh_hash != mesh_hash(c->mesh))
             throw Error{RKDG_ERR_INVALID, "checkpoint was written for another mesh (or triangle ordering)"};
+        if (h.nq != c->p.nq || h.ng != c->p.ng || h.flux != c->p.flux || h.limiter != c->p.limiter ||
+            h.rk != c->p.rk || h.gamma != c->p.gamma || h.cfl != c->p.cfl ||
+            (c->p.limiter != RKDG_LIMITER_NONE && h.tvb_m != c->p.tvb_m))
+            throw Error{RKDG_ERR_INVALID,
+                        "checkpoint was written with another method or physics (rules, flux, limiter, RK "
+                        "scheme, gamma, CFL number or TVB constant)"};
         if (c->p.precision != RKDG_FP64)
             for (int v = 0; v < 4; ++v)
                 if (h.farfield[v] != c->p.farfield[v])

@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <string>
 #include <type_traits>
 
 #include "rkdg_internal.hpp"
@@ -547,20 +548,22 @@ enum { MODE_STAGE = 0, MODE_RESIDUAL = 1, MODE_STAGE_COMP = 2 };
 #include "stage_tiled.cuh"
 
 // CFL measure of the current state per solve (first step, rkdg_compute_dt):
-// one CTA per tile, a block max per tile, one atomicMax into its solve.
+// one CTA per tile (its threads loop over the tile's elements), a block max
+// per tile, one atomicMax into its solve.
+constexpr int kAuxBlock = 128;
 template <typename Real>
-__global__ void __launch_bounds__(kTile) wave_kernel(const TileArgs ta, int ld,
-                                                     const Real* __restrict__ U,
-                                                     const double* __restrict__ jinv, double gamma,
-                                                     StepCtl* ctl, const double* __restrict__ refs) {
+__global__ void __launch_bounds__(kAuxBlock) wave_kernel(const TileArgs ta, int ld,
+                                                         const Real* __restrict__ U,
+                                                         const double* __restrict__ jinv, double gamma,
+                                                         StepCtl* ctl, const double* __restrict__ refs) {
     const int ntiles = ta.ntiles_dev ? *ta.ntiles_dev : ta.ntiles;
     if ((int)blockIdx.x >= ntiles) return;
     const int4 d0 = __ldg(ta.desc + 2 * blockIdx.x);
-    const int e = d0.x + threadIdx.x;
     StepCtl* c = ctl + d0.z;
     const double* ref = refs + 4 * d0.z;
     double w = 0.0;
-    if ((int)threadIdx.x < d0.y) {
+    for (int x = threadIdx.x; x < d0.y; x += blockDim.x) {
+        const int e = d0.x + x;
         Real m[4];
         load_mean<Real, 1>(U, ld, e, m);
         const double2* j2 = reinterpret_cast<const double2*>(jinv);
@@ -569,7 +572,7 @@ __global__ void __launch_bounds__(kTile) wave_kernel(const TileArgs ta, int ld,
 #pragma unroll
         for (int v = 0; v < 4; ++v) mm[v] = m[v] + ref_of<Real>(ref, v);
         elem_lengths<Real>(j2[e], j2[ld + e], len, ia);
-        w = wave_of<Real>(mm, (Real)gamma, len, ia, bad);
+        w = fmax(w, wave_of<Real>(mm, (Real)gamma, len, ia, bad));
         if (bad) atomicOr(&c->error, 1);
     }
     block_max3_atomic(w, 0.0, 0.0, &c->wave_bits, nullptr, nullptr);
@@ -650,6 +653,44 @@ __device__ __forceinline__ void limit_element(int e, int ld, Real* __restrict__ 
     const double idet = 1.0 / (r0.x * r1.y - r0.y * r1.x);  // det J
     // columns of J: x_1 - x_0 and x_2 - x_0
     const double c0x = r1.y * idet, c0y = -r1.x * idet, c1x = -r0.y * idet, c1y = r0.x * idet;
+    Real dirx[3], diry[3], thrk[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) tilde[k][v] = tb.mphi[k][0] * u[1][v] + tb.mphi[k][1] * u[2][v];
+        const double dxi = k == 1 ? -1.0 / 3.0 : 1.0 / 6.0, deta = k == 2 ? -1.0 / 3.0 : 1.0 / 6.0;
+        const double dx = c0x * dxi + c1x * deta, dy = c0y * dxi + c1y * deta;
+        const double r2 = dx * dx + dy * dy, irl = 1.0 / sqrt(r2);
+        dirx[k] = (Real)(dx * irl);
+        diry[k] = (Real)(dy * irl);
+        thrk[k] = (Real)(tvb_m * (4.0 * r2));
+    }
+    // the mean's primitive state and sound speed (the eigenvectors below)
+    const Real rho = mean[0], ir = Real(1) / rho, vx = mean[1] * ir, vy = mean[2] * ir;
+    const Real p = (gamma - Real(1)) * (mean[3] - Real(0.5) * rho * (vx * vx + vy * vy));
+    const Real c = sqrt(gamma * p * ir), H = (mean[3] + p) * ir;
+    const Real k2 = Real(0.5) * (vx * vx + vy * vy);
+    const Real b1 = (gamma - Real(1)) / (c * c), b2 = b1 * k2, ic = Real(1) / c;
+    {
+        // Exact early exit: every row of the left eigenvector matrix below
+        // has 1-norm at most B (|q|, |q_t| <= |vx| + |vy|, |nx| + |ny| <= 1.5),
+        // so when B max |tilde| is within the smallest TVB threshold, every
+        // characteristic increment is kept and the element is not limited
+        // (uniform and near-uniform regions skip the neighbour means and the
+        // decompositions).  A non-physical mean (NaN bound) takes the full
+        // path.
+        const Real av = fabs(vx) + fabs(vy);
+        const Real B0 = Real(0.5) * (b2 + av * ic + b1 * av + Real(1.5) * ic + b1);
+        const Real B1 = fabs(Real(1) - b2) + b1 * av + b1;
+        const Real B2 = av + Real(1.5);
+        const Real B = fmax(fmax(B0, B1), B2) * Real(1.001);
+        Real tmax = Real(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) tmax = fmax(tmax, fabs(tilde[k][v]));
+        if (B * tmax <= fmin(fmin(thrk[0], thrk[1]), thrk[2])) return;
+    }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         int ne = k == 0 ? cn.x : (k == 1 ? cn.y : cn.z);
@@ -666,8 +707,6 @@ __device__ __forceinline__ void limit_element(int e, int ld, Real* __restrict__ 
             double il = 1.0 / sqrt(Nx * Nx + Ny * Ny);
             ghost<Real>(tag, mean, far, (Real)(Nx * il), (Real)(Ny * il), nbm[k]);
         }
-#pragma unroll
-        for (int v = 0; v < 4; ++v) tilde[k][v] = tb.mphi[k][0] * u[1][v] + tb.mphi[k][1] * u[2][v];
     }
     bool limited = false;
     Real delta[3][4];
@@ -676,11 +715,8 @@ __device__ __forceinline__ void limit_element(int e, int ld, Real* __restrict__ 
         const Pair ab = __ldg(lim + (size_t)k * ld + e);
         const Real al = (Real)ab.x, be = (Real)ab.y;
         const int j = (pair_bits >> k) & 1u ? (k + 2) % 3 : (k + 1) % 3;
-        const double dxi = k == 1 ? -1.0 / 3.0 : 1.0 / 6.0, deta = k == 2 ? -1.0 / 3.0 : 1.0 / 6.0;
-        const double dx = c0x * dxi + c1x * deta, dy = c0y * dxi + c1y * deta;
-        const double r2 = dx * dx + dy * dy, irl = 1.0 / sqrt(r2);
-        const Real nx = (Real)(dx * irl), ny = (Real)(dy * irl);
-        const Real thr = (Real)(tvb_m * (4.0 * r2));
+        const Real nx = dirx[k], ny = diry[k];
+        const Real thr = thrk[k];
         Real dbar[4];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
@@ -688,11 +724,7 @@ __device__ __forceinline__ void limit_element(int e, int ld, Real* __restrict__ 
             dbar[v] = al * (nbm[k][v] - mean[v]) + be * (nj - mean[v]);
         }
         // eigenvectors of the Euler flux Jacobian in direction n at the mean
-        Real rho = mean[0], ir = Real(1) / rho, vx = mean[1] * ir, vy = mean[2] * ir;
-        Real p = (gamma - Real(1)) * (mean[3] - Real(0.5) * rho * (vx * vx + vy * vy));
-        Real c = sqrt(gamma * p * ir), H = (mean[3] + p) * ir;
-        Real q = vx * nx + vy * ny, qt = -vx * ny + vy * nx, k2 = Real(0.5) * (vx * vx + vy * vy);
-        Real b1 = (gamma - Real(1)) / (c * c), b2 = b1 * k2, ic = Real(1) / c;
+        const Real q = vx * nx + vy * ny, qt = -vx * ny + vy * nx;
         Real Lm[4][4] = {{Real(0.5) * (b2 + q * ic), Real(0.5) * (-b1 * vx - nx * ic),
                           Real(0.5) * (-b1 * vy - ny * ic), Real(0.5) * b1},
                          {Real(1) - b2, b1 * vx, b1 * vy, -b1},
@@ -761,7 +793,7 @@ __device__ __forceinline__ void limit_element(int e, int ld, Real* __restrict__ 
 // tiles drop their quadratic modes where limited).  Every path runs this one
 // kernel, so a solve limits to the same bits wherever it runs.
 template <typename Real>
-__global__ void __launch_bounds__(kTile) tiled_limiter_kernel(const TileArgs ta, int ld,
+__global__ void __launch_bounds__(kAuxBlock) tiled_limiter_kernel(const TileArgs ta, int ld,
                                                               Real* __restrict__ U,
                                                               const int4* __restrict__ conn,
                                                               const void* __restrict__ lim,
@@ -774,14 +806,47 @@ __global__ void __launch_bounds__(kTile) tiled_limiter_kernel(const TileArgs ta,
     const int ntiles = ta.ntiles_dev ? *ta.ntiles_dev : ta.ntiles;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int4 d0 = __ldg(ta.desc + 2 * tile);
-        if ((flags && !flags[d0.z]) || (ctl && ctl[d0.z].done) || (int)threadIdx.x >= d0.y) continue;
+        if ((flags && !flags[d0.z]) || (ctl && ctl[d0.z].done)) continue;
         const double* f = refs + 4 * d0.z;
-        const int e = d0.x + threadIdx.x;
-        if (d0.w == 2)
-            limit_element<Real, 6>(e, ld, U, conn, lim, jinv, gamma, f[0], f[1], f[2], f[3], tvb_m, tab<Real>(cfg2));
-        else
-            limit_element<Real, 3>(e, ld, U, conn, lim, jinv, gamma, f[0], f[1], f[2], f[3], tvb_m, tab<Real>(cfg1));
+        for (int x = threadIdx.x; x < d0.y; x += blockDim.x) {
+            const int e = d0.x + x;
+            if (d0.w == 2)
+                limit_element<Real, 6>(e, ld, U, conn, lim, jinv, gamma, f[0], f[1], f[2], f[3], tvb_m, tab<Real>(cfg2));
+            else
+                limit_element<Real, 3>(e, ld, U, conn, lim, jinv, gamma, f[0], f[1], f[2], f[3], tvb_m, tab<Real>(cfg1));
+        }
     }
+}
+
+// ------------------------------------------------- halo row exchange --
+// Rows 0..nrows-1 (16-byte packs) of the listed elements of a state, to or
+// from a contiguous buffer [n][nrows]: the pack and unpack of a partition's
+// halo exchange.  An index outside [0, T) is skipped and sets bit 2 of the
+// error word.
+__global__ void gather_rows_kernel(const int4* __restrict__ U, int ld, int T, const int* __restrict__ idx, int n,
+                                   int nrows, int4* __restrict__ out, int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * nrows) return;
+    const int j = i / nrows, r = i - j * nrows;
+    const int e = idx[j];
+    if (e < 0 || e >= T) {
+        atomicOr(err, 4);
+        return;
+    }
+    out[i] = U[(size_t)r * ld + e];
+}
+
+__global__ void scatter_rows_kernel(int4* __restrict__ U, int ld, int T, const int* __restrict__ idx, int n,
+                                    int nrows, const int4* __restrict__ in, int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * nrows) return;
+    const int j = i / nrows, r = i - j * nrows;
+    const int e = idx[j];
+    if (e < 0 || e >= T) {
+        atomicOr(err, 4);
+        return;
+    }
+    U[(size_t)r * ld + e] = in[i];
 }
 
 // ---------------------------------------------------- basis conversion --
@@ -943,47 +1008,75 @@ namespace {
 
 // Shared-memory attributes of one instantiation for a halo size; returns the
 // dynamic shared memory per CTA.
-template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
+// The device's largest opt-in dynamic + static shared memory per CTA, less
+// the stage kernel's static shared memory (barrier, maxima, dt, tables).
+size_t smem_limit() {
+    static int limit = 0;
+    if (limit == 0) {
+        int dev = 0, v = 0;
+        RKDG_CUDA_TRY(cudaGetDevice(&dev));
+        RKDG_CUDA_TRY(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        limit = v;
+    }
+    return (size_t)limit - 1024;
+}
+
+template <typename Real, int NQ2, int FLUX, int MODE, int ORD, int BT>
 size_t prepare_tiled(int max_halo) {
-    const size_t smem = TiledSmem<Real, ORD, FLUX>::bytes(max_halo);
+    const size_t smem = TiledSmem<Real, ORD, FLUX, BT>::bytes(max_halo);
+    if (smem > smem_limit())
+        throw Error{RKDG_ERR_INVALID, "tiles of " + std::to_string(BT) + " elements with halo lists of " +
+                                          std::to_string(max_halo) + " entries need " + std::to_string(smem) +
+                                          " bytes of shared memory per CTA, above the device's limit: use "
+                                          "128-element tiles or the locality order"};
     // dynamic + static shared memory above 48 KB needs the opt-in.  Per
     // instantiation; raised when a context with a larger halo appears.
     static size_t configured = 0;
     if (configured == 0)  // give shared memory the whole carveout
-        RKDG_CUDA_TRY(cudaFuncSetAttribute(tiled_stage_kernel<Real, NQ2, FLUX, MODE, ORD>,
+        RKDG_CUDA_TRY(cudaFuncSetAttribute(tiled_stage_kernel<Real, NQ2, FLUX, MODE, ORD, BT>,
                                            cudaFuncAttributePreferredSharedMemoryCarveout,
                                            (int)cudaSharedmemCarveoutMaxShared));
     if (smem > configured) {
-        RKDG_CUDA_TRY(cudaFuncSetAttribute(tiled_stage_kernel<Real, NQ2, FLUX, MODE, ORD>,
+        RKDG_CUDA_TRY(cudaFuncSetAttribute(tiled_stage_kernel<Real, NQ2, FLUX, MODE, ORD, BT>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         configured = smem;
     }
     return smem;
 }
 
-template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
+template <typename Real, int NQ2, int FLUX, int MODE, int ORD, int BT>
 int occupancy_tiled(int max_halo) {
-    const size_t smem = prepare_tiled<Real, NQ2, FLUX, MODE, ORD>(max_halo);
+    const size_t smem = prepare_tiled<Real, NQ2, FLUX, MODE, ORD, BT>(max_halo);
     int n = 0;
     RKDG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &n, tiled_stage_kernel<Real, NQ2, FLUX, MODE, ORD>, kTile, smem));
+        &n, tiled_stage_kernel<Real, NQ2, FLUX, MODE, ORD, BT>, BT, smem));
     return n;
 }
 
-template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
+template <typename Real, int NQ2, int FLUX, int MODE, int ORD, int BT>
 void launch_tiled(const StageArgs& a, const TileArgs& t, int ctas, cudaStream_t s) {
-    const size_t smem = prepare_tiled<Real, NQ2, FLUX, MODE, ORD>(t.max_halo);
+    const size_t smem = prepare_tiled<Real, NQ2, FLUX, MODE, ORD, BT>(t.max_halo);
     const int grid = (ctas > 0 && ctas < t.ntiles) ? ctas : t.ntiles;
-    if (grid > 0) tiled_stage_kernel<Real, NQ2, FLUX, MODE, ORD><<<grid, kTile, smem, s>>>(a, t);
+    if (grid > 0) tiled_stage_kernel<Real, NQ2, FLUX, MODE, ORD, BT><<<grid, BT, smem, s>>>(a, t);
+}
+
+// Tile sizes the stage kernel is built for: 128 everywhere, 256 for the
+// stage (not the residual) kernels the batch autotuner may pick.
+template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
+void launch_tiled_bt(const StageArgs& a, const TileArgs& t, int ctas, cudaStream_t s) {
+    if (t.tile == 128) return launch_tiled<Real, NQ2, FLUX, MODE, ORD, 128>(a, t, ctas, s);
+    if constexpr (MODE != MODE_RESIDUAL)
+        if (t.tile == 256) return launch_tiled<Real, NQ2, FLUX, MODE, ORD, 256>(a, t, ctas, s);
+    throw Error{RKDG_ERR_INVALID, "no stage kernel for a tile of " + std::to_string(t.tile) + " elements"};
 }
 
 template <typename Real, int FLUX, int MODE>
 void dispatch_tiled(const StageArgs& a, const TileArgs& t, int order, int nq, int ctas,
                     cudaStream_t s) {
-    if (order == 1) return launch_tiled<Real, 6, FLUX, MODE, 1>(a, t, ctas, s);
-    if (order == 2 && nq == 7) return launch_tiled<Real, 7, FLUX, MODE, 2>(a, t, ctas, s);
-    if (order == 2 && nq == 6) return launch_tiled<Real, 6, FLUX, MODE, 2>(a, t, ctas, s);
-    if (order == 3 && nq == 6) return launch_tiled<Real, 6, FLUX, MODE, 3>(a, t, ctas, s);
+    if (order == 1) return launch_tiled_bt<Real, 6, FLUX, MODE, 1>(a, t, ctas, s);
+    if (order == 2 && nq == 7) return launch_tiled_bt<Real, 7, FLUX, MODE, 2>(a, t, ctas, s);
+    if (order == 2 && nq == 6) return launch_tiled_bt<Real, 6, FLUX, MODE, 2>(a, t, ctas, s);
+    if (order == 3 && nq == 6) return launch_tiled_bt<Real, 6, FLUX, MODE, 3>(a, t, ctas, s);
     throw Error{RKDG_ERR_INVALID, "unsupported order/rule combination for the tiled kernel"};
 }
 
@@ -1034,9 +1127,9 @@ void launch_wave(const TileArgs& t, int ld, const void* U, int prec, const doubl
     if (nsolves > 0) reset_wave_kernel<<<(nsolves + 127) / 128, 128, 0, stream>>>(ctl, nsolves);
     if (t.ntiles > 0) {
         if (prec == RKDG_FP32)
-            wave_kernel<float><<<t.ntiles, kTile, 0, stream>>>(t, ld, static_cast<const float*>(U), jinv, gamma, ctl, refs);
+            wave_kernel<float><<<t.ntiles, kAuxBlock, 0, stream>>>(t, ld, static_cast<const float*>(U), jinv, gamma, ctl, refs);
         else
-            wave_kernel<double><<<t.ntiles, kTile, 0, stream>>>(t, ld, static_cast<const double*>(U), jinv, gamma, ctl, refs);
+            wave_kernel<double><<<t.ntiles, kAuxBlock, 0, stream>>>(t, ld, static_cast<const double*>(U), jinv, gamma, ctl, refs);
     }
     RKDG_CUDA_TRY(cudaGetLastError());
 }
@@ -1046,26 +1139,48 @@ void launch_step_begin(StepCtl* ctl, int nsolves, cudaStream_t stream) {
     RKDG_CUDA_TRY(cudaGetLastError());
 }
 
-int tiled_max_ctas_per_sm(int prec, int order, int nq, int flux, int max_halo) {
+namespace {
+template <typename Real, int FLUX>
+int occupancy_for(int order, int nq, int tile, int max_halo) {
+    auto pick = [&](auto bt) -> int {
+        constexpr int BT = decltype(bt)::value;
+        if (order == 1) return occupancy_tiled<Real, 6, FLUX, MODE_STAGE, 1, BT>(max_halo);
+        if (order == 3) return occupancy_tiled<Real, 6, FLUX, MODE_STAGE, 3, BT>(max_halo);
+        if (nq == 7) return occupancy_tiled<Real, 7, FLUX, MODE_STAGE, 2, BT>(max_halo);
+        return occupancy_tiled<Real, 6, FLUX, MODE_STAGE, 2, BT>(max_halo);
+    };
+    if (tile == 256) return pick(std::integral_constant<int, 256>{});
+    return pick(std::integral_constant<int, 128>{});
+}
+}  // namespace
+
+size_t tiled_smem_bytes(int prec, int order, int flux, int max_halo, int tile) {
+    auto f = [&](auto r, auto bt) -> size_t {
+        using Real = decltype(r);
+        constexpr int BT = decltype(bt)::value;
+        const bool h = flux == RKDG_FLUX_HLLC;
+        if (order == 1)
+            return h ? TiledSmem<Real, 1, RKDG_FLUX_HLLC, BT>::bytes(max_halo) : TiledSmem<Real, 1, RKDG_FLUX_LLF, BT>::bytes(max_halo);
+        if (order == 2)
+            return h ? TiledSmem<Real, 2, RKDG_FLUX_HLLC, BT>::bytes(max_halo) : TiledSmem<Real, 2, RKDG_FLUX_LLF, BT>::bytes(max_halo);
+        return h ? TiledSmem<Real, 3, RKDG_FLUX_HLLC, BT>::bytes(max_halo) : TiledSmem<Real, 3, RKDG_FLUX_LLF, BT>::bytes(max_halo);
+    };
+    if (prec == RKDG_FP32)
+        return tile == 256 ? f(0.0f, std::integral_constant<int, 256>{}) : f(0.0f, std::integral_constant<int, 128>{});
+    return tile == 256 ? f(0.0, std::integral_constant<int, 256>{}) : f(0.0, std::integral_constant<int, 128>{});
+}
+
+bool tiled_fits(int prec, int order, int flux, int max_halo, int tile) {
+    return tiled_smem_bytes(prec, order, flux, max_halo, tile) <= smem_limit();
+}
+
+int tiled_max_ctas_per_sm(int prec, int order, int nq, int flux, int max_halo, int tile) {
     const bool h = flux == RKDG_FLUX_HLLC;
-    if (prec == RKDG_FP32) {
-        if (order == 1) return h ? occupancy_tiled<float, 6, RKDG_FLUX_HLLC, MODE_STAGE, 1>(max_halo)
-                                 : occupancy_tiled<float, 6, RKDG_FLUX_LLF, MODE_STAGE, 1>(max_halo);
-        if (order == 3) return h ? occupancy_tiled<float, 6, RKDG_FLUX_HLLC, MODE_STAGE, 3>(max_halo)
-                                 : occupancy_tiled<float, 6, RKDG_FLUX_LLF, MODE_STAGE, 3>(max_halo);
-        if (nq == 7) return h ? occupancy_tiled<float, 7, RKDG_FLUX_HLLC, MODE_STAGE, 2>(max_halo)
-                              : occupancy_tiled<float, 7, RKDG_FLUX_LLF, MODE_STAGE, 2>(max_halo);
-        return h ? occupancy_tiled<float, 6, RKDG_FLUX_HLLC, MODE_STAGE, 2>(max_halo)
-                 : occupancy_tiled<float, 6, RKDG_FLUX_LLF, MODE_STAGE, 2>(max_halo);
-    }
-    if (order == 1) return h ? occupancy_tiled<double, 6, RKDG_FLUX_HLLC, MODE_STAGE, 1>(max_halo)
-                             : occupancy_tiled<double, 6, RKDG_FLUX_LLF, MODE_STAGE, 1>(max_halo);
-    if (order == 3) return h ? occupancy_tiled<double, 6, RKDG_FLUX_HLLC, MODE_STAGE, 3>(max_halo)
-                             : occupancy_tiled<double, 6, RKDG_FLUX_LLF, MODE_STAGE, 3>(max_halo);
-    if (nq == 7) return h ? occupancy_tiled<double, 7, RKDG_FLUX_HLLC, MODE_STAGE, 2>(max_halo)
-                          : occupancy_tiled<double, 7, RKDG_FLUX_LLF, MODE_STAGE, 2>(max_halo);
-    return h ? occupancy_tiled<double, 6, RKDG_FLUX_HLLC, MODE_STAGE, 2>(max_halo)
-             : occupancy_tiled<double, 6, RKDG_FLUX_LLF, MODE_STAGE, 2>(max_halo);
+    if (prec == RKDG_FP32)
+        return h ? occupancy_for<float, RKDG_FLUX_HLLC>(order, nq, tile, max_halo)
+                 : occupancy_for<float, RKDG_FLUX_LLF>(order, nq, tile, max_halo);
+    return h ? occupancy_for<double, RKDG_FLUX_HLLC>(order, nq, tile, max_halo)
+             : occupancy_for<double, RKDG_FLUX_LLF>(order, nq, tile, max_halo);
 }
 
 void launch_tiled_limiter(const TileArgs& t, int ctas, int ld, void* U, const int4* conn,
@@ -1075,9 +1190,23 @@ void launch_tiled_limiter(const TileArgs& t, int ctas, int ld, void* U, const in
     const int cfg1 = cfg_index(3, 2), cfg2 = cfg_index(nq2, 3);
     const int grid = ctas > 0 ? ctas : std::max(1, t.ntiles);
     if (prec == RKDG_FP32)
-        tiled_limiter_kernel<float><<<grid, kTile, 0, stream>>>(t, ld, static_cast<float*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl);
+        tiled_limiter_kernel<float><<<grid, kAuxBlock, 0, stream>>>(t, ld, static_cast<float*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl);
     else
-        tiled_limiter_kernel<double><<<grid, kTile, 0, stream>>>(t, ld, static_cast<double*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl);
+        tiled_limiter_kernel<double><<<grid, kAuxBlock, 0, stream>>>(t, ld, static_cast<double*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl);
+    RKDG_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_rows(bool gather, void* U, int ld, int T, const int* idx, int n, int nrows, void* buf, int* err,
+                 cudaStream_t stream) {
+    const int total = n * nrows;
+    if (total <= 0) return;
+    const int grid = (total + 255) / 256;
+    if (gather)
+        gather_rows_kernel<<<grid, 256, 0, stream>>>(static_cast<const int4*>(U), ld, T, idx, n, nrows,
+                                                      static_cast<int4*>(buf), err);
+    else
+        scatter_rows_kernel<<<grid, 256, 0, stream>>>(static_cast<int4*>(U), ld, T, idx, n, nrows,
+                                                       static_cast<const int4*>(buf), err);
     RKDG_CUDA_TRY(cudaGetLastError());
 }
 

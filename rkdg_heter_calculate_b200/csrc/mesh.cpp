@@ -395,11 +395,13 @@ HostGeometry build_geometry(const HostMesh& m, int order, bool with_conversion, 
 }
 
 TileTables build_tiles(const HostMesh& m, int elem_offset, int sid, int order, int halo_offset,
-                       int task_offset) {
-    const int T = m.T, B = kTile;
+                       int task_offset, int n_tiled, int tile) {
+    const int T = n_tiled >= 0 ? n_tiled : m.T, B = tile;
+    if (B != 128 && B != 256) throw Error{RKDG_ERR_INVALID, "tiles hold 128 or 256 elements"};
     TileTables t;
+    t.tile = B;
     t.ntiles = (T + B - 1) / B;
-    t.code.assign((size_t)4 * T, 0);
+    t.code.assign((size_t)4 * m.T, 0);
     t.desc.assign((size_t)8 * t.ntiles, 0);
     int maxh = 0;
     for (int tile = 0; tile < t.ntiles; ++tile) {

@@ -12,7 +12,9 @@
 // librkdg.so holds it (kMaxBlocks * 4 doubles = 128 KiB) until the process
 // exits.  Host code may not use the symbol as a pointer; its device address
 // is looked up once per device with cudaGetSymbolAddress (on the first call
-// made with that device current) and passed to the kernels.
+// made with that device current) and passed to the kernels.  The address
+// belongs to the context that was current then, so a device reset between
+// calls (which unloads the module) is not supported.
 #include <cuda_runtime.h>
 
 #include <mutex>

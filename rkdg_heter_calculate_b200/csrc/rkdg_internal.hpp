@@ -22,12 +22,17 @@ struct Error {
     int code;
     std::string msg;
 };
+// A failed call's error is also taken off the runtime's per-thread last
+// error (cudaGetLastError), so that a non-sticky error reported here is not
+// reported again by a later, unrelated check.
 #define RKDG_CUDA_TRY(expr)                                                              \
     do {                                                                                 \
         cudaError_t e_ = (expr);                                                         \
-        if (e_ != cudaSuccess)                                                           \
+        if (e_ != cudaSuccess) {                                                         \
+            cudaGetLastError();                                                          \
             throw ::rkdg::Error{RKDG_ERR_CUDA, std::string(#expr) + ": " +               \
                                                    cudaGetErrorString(e_)};              \
+        }                                                                                \
     } while (0)
 
 // ----------------------------------------------------------- quadrature --
@@ -119,6 +124,7 @@ enum { EDGE_IN_OWNER = 0, EDGE_IN_OTHER = 1, EDGE_HALO = 2, EDGE_BOUNDARY = 3 };
 // desc per tile (8 ints): e0, count, solve id, order, halo_begin, nhalo,
 // task_begin, ntask.
 struct TileTables {
+    int tile = kTile;                  // elements per tile
     int ntiles = 0;
     int max_halo = 0;                  // rounded up to a multiple of 4
     std::vector<int32_t> code;         // [T][4] (code of edges 0..2, unused)
@@ -126,8 +132,10 @@ struct TileTables {
     std::vector<int32_t> halo;         // [nhalo][2] (global element, its edge)
     std::vector<uint16_t> task;        // local element * 4 + edge, sorted by edge
 };
+// n_tiled >= 0: only elements [0, n_tiled) are tiled (a partition's owned
+// elements; the rest are halo copies that other tiles read as neighbours).
 TileTables build_tiles(const HostMesh& m, int elem_offset = 0, int sid = 0, int order = 2,
-                       int halo_offset = 0, int task_offset = 0);
+                       int halo_offset = 0, int task_offset = 0, int n_tiled = -1, int tile = kTile);
 
 // ------------------------------------------------------------- device --
 struct StepCtl {
@@ -140,12 +148,14 @@ struct StepCtl {
     unsigned long long mon_bits[2]; // residual monitor, as bits
     int step;
     int done;
-    int error;                 // bit 0: non-physical state seen; bit 1: a device wait timed out
+    int error;                 // bit 0: non-physical state seen; bit 1: a device wait timed out;
+                               // bit 2: a halo-exchange row index out of range
     int pad;
 };
 
 // Throws the error a solve's control word reports (no-op when clean).
 inline void throw_ctl_error(int error, const std::string& who) {
+    if (error & 4) throw Error{RKDG_ERR_INVALID, who + ": a row index given to a halo exchange is out of range"};
     if (error & 2) throw Error{RKDG_ERR_CUDA, who + ": a device-side wait on staged data timed out"};
     if (error) throw Error{RKDG_ERR_STATE, who + ": non-physical state (NaN or non-positive density/pressure)"};
 }
@@ -178,6 +188,7 @@ struct TileArgs {
     int max_halo;
     int ntiles;
     const int* ntiles_dev;  // when set, kernels read the tile count here (graph-stable)
+    int tile = kTile;       // elements per tile (threads per CTA of the stage kernel): 128 or 256
 };
 
 struct StageArgs {
@@ -229,8 +240,14 @@ void launch_wave(const TileArgs& t, int ld, const void* U, int prec, const doubl
 void launch_step_begin(StepCtl* ctl, int nsolves, cudaStream_t stream);
 // bounded device wait on data that never arrives (see rkdg_wait_selftest)
 void wait_selftest(double limit_s, int* timed_out, double* waited_s);
-// resident CTAs per SM of the tiled stage kernel (order 3: mixed pack)
-int tiled_max_ctas_per_sm(int prec, int order, int nq, int flux, int max_halo);
+// dynamic shared memory per CTA of the tiled stage kernel for a tile size
+// and halo list length (order 3: mixed pack); the launchers refuse a
+// configuration above the device's per-CTA limit with RKDG_ERR_INVALID
+size_t tiled_smem_bytes(int prec, int order, int flux, int max_halo, int tile);
+bool tiled_fits(int prec, int order, int flux, int max_halo, int tile);
+// resident CTAs per SM of the tiled stage kernel (order 3: mixed pack) for
+// tiles of `tile` elements
+int tiled_max_ctas_per_sm(int prec, int order, int nq, int flux, int max_halo, int tile = kTile);
 // TVB limiter over tiles; flags[solve] (may be null: all on) enables it per
 // solve, solves whose control block (ctl may be null) says done are skipped;
 // ctas 0 = one CTA per tile
@@ -251,5 +268,10 @@ void launch_export(int T, int ld, const void* U, const double* conv, const int32
 void launch_totals(int T, int ld, const void* U, int order, int prec, const double* jinv,
                    double* partial, double* out4, const double* ref, int lo_row, cudaStream_t stream);
 int totals_partial_count(int T);
+// Halo exchange of a partition: rows 0..nrows-1 of elements idx[0..n) of U
+// to (gather) or from (scatter) buf [n][nrows] 16-byte packs; bad indices
+// set bit 2 of *err.
+void launch_rows(bool gather, void* U, int ld, int T, const int* idx, int n, int nrows, void* buf, int* err,
+                 cudaStream_t stream);
 
 }  // namespace rkdg

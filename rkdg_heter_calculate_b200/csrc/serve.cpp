@@ -89,6 +89,7 @@ constexpr int kPoolHalo = 160;  // halo entries per tile the pool's kernels stag
 struct Request {
     int64_t id = 0;
     int order = 2, nb = 6, T = 0;
+    int flux = RKDG_FLUX_LLF;
     bool limiter = false;
     double t_final = 0, far[4] = {0, 0, 0, 0};
     std::vector<double> jinv;   // [T][4]
@@ -111,7 +112,7 @@ struct Request {
 
 struct rkdg_server {
     rkdg_params p{};
-    int device = 0, word = 4, max_slots = 0, ctas = 0;
+    int device = 0, word = 4, max_slots = 0, ctas[2] = {0, 0};
     int64_t cap = 0, hcap = 0, kcap = 0, tcap = 0, max_T = 0;
     int ld = 0;
     size_t bytes = 0;
@@ -125,15 +126,17 @@ struct rkdg_server {
     int2* halo = nullptr;
     uint16_t* task = nullptr;
     int4* desc = nullptr;
-    int* ntiles_dev = nullptr;
+    int* ntiles_dev = nullptr;   // [2]: active tiles of the LLF and HLLC lists
     StepCtl* ctl = nullptr;
     double* far = nullptr;
     int* flags = nullptr;
     double* staging = nullptr;
     StepCtl* h_ctl = nullptr;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;  // the HLLC tiles' launches, forked and joined in the step graph
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaGraphExec_t graph = nullptr;
-    TileArgs tiles{};
+    TileArgs tiles[2]{};  // indexed by flux: the LLF and the HLLC requests' tiles
     // host state
     RangeAlloc elems, halos, tasks;
     std::vector<int> free_slots;
@@ -145,11 +148,15 @@ struct rkdg_server {
     std::condition_variable cv_work, cv_done;
     std::thread engine;
     bool stop = false;
-    std::string fatal;
+    std::string fatal;         // set when the engine thread has stopped on an error
+    int fatal_code = RKDG_OK;
+    int fault_after = -1;      // rkdg_server_inject_fault: chunks left before a simulated failure
     bool tiles_dirty = false;
-    int ntiles = 0;
+    int ntiles[2] = {0, 0};
     // stats
     double dof_updates = 0, busy = 0;
+    double t_admit = 0, t_retire = 0;  // engine seconds spent uploading and retiring requests
+    int64_t chunks = 0;
     int64_t completed = 0;
     int peak = 0;
 };
@@ -198,6 +205,11 @@ void coeffs(int rk, int st, double& a, double& c) {
     else a = 1.0 / 3.0, c = 2.0 / 3.0;
 }
 
+// One step of every solve in flight: per RK stage, the stage kernel and the
+// limiter over the LLF requests' tiles on the server's stream and over the
+// HLLC requests' tiles on a second stream forked from it (the two lists
+// hold different solves, so the launches overlap where one list runs out),
+// joined before the next stage.
 void enqueue_step(rkdg_server* s) {
     launch_step_begin(s->ctl, s->max_slots, s->stream);
     const int plan[3][3] = {{0, 0, 1}, {1, 0, 2}, {2, 0, 0}};
@@ -218,9 +230,16 @@ void enqueue_step(rkdg_server* s) {
         a.Unew = s->U[pl[2]];
         a.last_stage = st == s->p.rk - 1;
         a.lo_row = lo_row(s);
-        launch_stage(a, s->tiles, 3, s->p.nq, s->p.flux, kprec(s), s->ctas, s->stream);
-        launch_tiled_limiter(s->tiles, s->ctas, s->ld, s->U[pl[2]], s->conn, s->lim, s->jinv, s->flags,
-                             s->far, kprec(s), s->p.nq, s->p.gamma, s->p.tvb_m, s->ctl, s->stream);
+        RKDG_CUDA_TRY(cudaEventRecord(s->ev_fork, s->stream));
+        RKDG_CUDA_TRY(cudaStreamWaitEvent(s->stream2, s->ev_fork, 0));
+        for (int f = 0; f < 2; ++f) {
+            cudaStream_t st_f = f == RKDG_FLUX_HLLC ? s->stream2 : s->stream;
+            launch_stage(a, s->tiles[f], 3, s->p.nq, f, kprec(s), s->ctas[f], st_f);
+            launch_tiled_limiter(s->tiles[f], s->ctas[f], s->ld, s->U[pl[2]], s->conn, s->lim, s->jinv, s->flags,
+                                 s->far, kprec(s), s->p.nq, s->p.gamma, s->p.tvb_m, s->ctl, st_f);
+        }
+        RKDG_CUDA_TRY(cudaEventRecord(s->ev_join, s->stream2));
+        RKDG_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
     }
 }
 
@@ -287,23 +306,26 @@ void relocate(const Request& r, std::vector<int32_t>& d) {
     }
 }
 
-// Rewrites the active tile list (P2 tiles first, then P1: the expensive
-// tiles start early in the persistent pass) and measures the CFL wave speed
-// of the newly admitted solves over their own tiles only, so the solves
-// already in flight keep the value their last stage computed.
+// Rewrites the two active tile lists (per flux; P2 tiles first, then P1:
+// the expensive tiles start early in the persistent pass) and measures the
+// CFL wave speed of the newly admitted solves over their own tiles only, so
+// the solves already in flight keep the value their last stage computed.
 void rebuild_tiles(rkdg_server* s, const std::vector<std::shared_ptr<Request>>& fresh) {
-    std::vector<int32_t> d, dn;
-    for (int pass = 0; pass < 2; ++pass)
-        for (auto& r : s->active)
-            if (r && (pass == 0) == (r->order == 2)) relocate(*r, d);
+    std::vector<int32_t> d[2], dn;
+    for (int f = 0; f < 2; ++f)
+        for (int pass = 0; pass < 2; ++pass)
+            for (auto& r : s->active)
+                if (r && r->flux == f && (pass == 0) == (r->order == 2)) relocate(*r, d[f]);
     for (auto& r : fresh) relocate(*r, dn);
-    s->ntiles = (int)(d.size() / 8);
-    h2d(s, reinterpret_cast<int32_t*>(s->desc), d.data(), d.size());
-    h2d(s, s->ntiles_dev, &s->ntiles, 1);
+    for (int f = 0; f < 2; ++f) {
+        s->ntiles[f] = (int)(d[f].size() / 8);
+        h2d(s, reinterpret_cast<int32_t*>(const_cast<int4*>(s->tiles[f].desc)), d[f].data(), d[f].size());
+    }
+    h2d(s, s->ntiles_dev, s->ntiles, 2);
     if (!dn.empty()) {
-        int4* scratch = s->desc + 2 * s->tcap;
+        int4* scratch = s->desc + 4 * s->tcap;
         h2d(s, reinterpret_cast<int32_t*>(scratch), dn.data(), dn.size());
-        TileArgs t = s->tiles;
+        TileArgs t = s->tiles[0];
         t.desc = scratch;
         t.ntiles = (int)(dn.size() / 8);
         t.ntiles_dev = nullptr;
@@ -408,12 +430,19 @@ void engine_loop(rkdg_server* s) {
                 if (s->stop) return;
                 in = admit(s);
             }
+            const double ta = now_s();
             for (auto& r : in) upload(s, *r);
             if (!in.empty() || s->tiles_dirty) rebuild_tiles(s, in);
+            const double tb = now_s();
             int in_flight = 0;
             for (auto& r : s->active) in_flight += r ? 1 : 0;
             if (in_flight == 0) continue;
             s->peak = std::max(s->peak, in_flight);
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                if (s->fault_after == 0) throw Error{RKDG_ERR_CUDA, "engine stopped by rkdg_server_inject_fault"};
+                if (s->fault_after > 0) --s->fault_after;
+            }
             const double t0 = now_s();
             for (int i = 0; i < chunk; ++i) RKDG_CUDA_TRY(cudaGraphLaunch(s->graph, s->stream));
             RKDG_CUDA_TRY(cudaMemcpyAsync(s->h_ctl, s->ctl, sizeof(StepCtl) * s->max_slots,
@@ -424,6 +453,8 @@ void engine_loop(rkdg_server* s) {
             {
                 std::lock_guard<std::mutex> lk(s->mu);
                 s->busy += t1 - t0;
+                s->t_admit += tb - ta;
+                ++s->chunks;
                 for (auto& r : s->active) {
                     if (!r) continue;
                     const StepCtl& c = s->h_ctl[r->slot];
@@ -434,11 +465,17 @@ void engine_loop(rkdg_server* s) {
                     if (c.done || c.error) done.push_back(r);
                 }
             }
+            const double tr = now_s();
             for (auto& r : done) retire(s, *r, s->h_ctl[r->slot].error != 0);
+            if (!done.empty()) {
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->t_retire += now_s() - tr;
+            }
         }
     } catch (const Error& e) {
         std::lock_guard<std::mutex> lk(s->mu);
         s->fatal = e.msg;
+        s->fatal_code = e.code;
         for (auto& r : s->active)
             if (r) r->status = REQ_FAILED, r->error = e.msg, r->error_code = e.code;
         for (auto& r : s->queue) r->status = REQ_FAILED, r->error = e.msg, r->error_code = e.code;
@@ -463,6 +500,9 @@ void destroy_server(rkdg_server* s) {
                     (void*)s->ctl, (void*)s->far, (void*)s->flags, (void*)s->staging})
         cudaFree(p);
     if (s->h_ctl) cudaFreeHost(s->h_ctl);
+    if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+    if (s->ev_join) cudaEventDestroy(s->ev_join);
+    if (s->stream2) cudaStreamDestroy(s->stream2);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -518,6 +558,9 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
         s->kcap = 3 * s->cap;
         s->tcap = s->cap / 128 + 2 * (int64_t)max_slots + 16;
         RKDG_CUDA_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+        RKDG_CUDA_TRY(cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking));
+        RKDG_CUDA_TRY(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+        RKDG_CUDA_TRY(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
         upload_tables(6, 3);
         upload_tables(3, 2);
         for (int k = 0; k < 3; ++k) {
@@ -532,9 +575,9 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
         s->perm = (int32_t*)salloc(s, sizeof(int32_t) * (size_t)s->cap);
         s->halo = (int2*)salloc(s, sizeof(int2) * (size_t)s->hcap + kTablePad);
         s->task = (uint16_t*)salloc(s, sizeof(uint16_t) * (size_t)s->kcap + kTablePad);
-        s->desc = (int4*)salloc(s, sizeof(int32_t) * 16 * (size_t)s->tcap);  // list + admission scratch
-        s->ntiles_dev = (int*)salloc(s, sizeof(int));
-        RKDG_CUDA_TRY(cudaMemsetAsync(s->ntiles_dev, 0, sizeof(int), s->stream));
+        s->desc = (int4*)salloc(s, sizeof(int32_t) * 24 * (size_t)s->tcap);  // two lists + admission scratch
+        s->ntiles_dev = (int*)salloc(s, 2 * sizeof(int));
+        RKDG_CUDA_TRY(cudaMemsetAsync(s->ntiles_dev, 0, 2 * sizeof(int), s->stream));
         s->ctl = (StepCtl*)salloc(s, sizeof(StepCtl) * max_slots);
         std::vector<StepCtl> c(max_slots);
         for (auto& x : c) {
@@ -558,15 +601,18 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
         for (int i = max_slots - 1; i >= 0; --i) s->free_slots.push_back(i);
         s->active.assign(max_slots, nullptr);
         // persistent grid, and a graph of one step whose tile count is read on the device
-        const int per_sm = std::max(1, tiled_max_ctas_per_sm(kernel_prec(p.precision), 3, p.nq, p.flux, kPoolHalo));
-        s->ctas = prop.multiProcessorCount * per_sm;
-        s->tiles.code = s->tcode;
-        s->tiles.desc = s->desc;
-        s->tiles.halo = s->halo;
-        s->tiles.task = s->task;
-        s->tiles.max_halo = kPoolHalo;
-        s->tiles.ntiles = (int)s->tcap;
-        s->tiles.ntiles_dev = s->ntiles_dev;
+        for (int f = 0; f < 2; ++f) {
+            const int per_sm = std::max(1, tiled_max_ctas_per_sm(kernel_prec(p.precision), 3, p.nq, f, kPoolHalo));
+            s->ctas[f] = prop.multiProcessorCount * per_sm;
+            TileArgs& t = s->tiles[f];
+            t.code = s->tcode;
+            t.desc = s->desc + 2 * f * s->tcap;
+            t.halo = s->halo;
+            t.task = s->task;
+            t.max_halo = kPoolHalo;
+            t.ntiles = (int)s->tcap;
+            t.ntiles_dev = s->ntiles_dev + f;
+        }
         RKDG_CUDA_TRY(cudaStreamSynchronize(s->stream));
         cudaGraph_t g;
         RKDG_CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
@@ -590,14 +636,16 @@ int rkdg_server_destroy(rkdg_server* s) {
     return guarded([&] { destroy_server(s); });
 }
 
-int rkdg_server_submit(rkdg_server* s, const rkdg_mesh_desc* mesh, int32_t order, const double* U0,
-                       double t_final, const double* farfield, int32_t limiter, int64_t* id) {
+int rkdg_server_submit_method(rkdg_server* s, const rkdg_mesh_desc* mesh, int32_t order, const double* U0,
+                              double t_final, const double* farfield, int32_t limiter, int32_t flux, int64_t* id) {
     return guarded([&] {
-        if (!s || !mesh || !U0 || !id || (order != 1 && order != 2))
+        if (!s || !mesh || !U0 || !id || (order != 1 && order != 2) ||
+            (flux != RKDG_FLUX_LLF && flux != RKDG_FLUX_HLLC))
             throw Error{RKDG_ERR_INVALID, "rkdg_server_submit: bad arguments"};
         auto r = std::make_shared<Request>();
         r->t_submit = now_s();
         r->order = order;
+        r->flux = flux;
         r->nb = order == 1 ? 3 : 6;
         r->limiter = limiter != 0;
         r->t_final = t_final;
@@ -636,6 +684,15 @@ int rkdg_server_submit(rkdg_server* s, const rkdg_mesh_desc* mesh, int32_t order
     });
 }
 
+int rkdg_server_submit(rkdg_server* s, const rkdg_mesh_desc* mesh, int32_t order, const double* U0,
+                       double t_final, const double* farfield, int32_t limiter, int64_t* id) {
+    if (!s) {
+        set_error("rkdg_server_submit: null server");
+        return RKDG_ERR_INVALID;
+    }
+    return rkdg_server_submit_method(s, mesh, order, U0, t_final, farfield, limiter, s->p.flux, id);
+}
+
 int rkdg_server_wait(rkdg_server* s, int64_t id, double timeout_s, int32_t* status, double* U,
                      double* times, int32_t* steps) {
     return guarded([&] {
@@ -662,6 +719,37 @@ int rkdg_server_wait(rkdg_server* s, int64_t id, double timeout_s, int32_t* stat
             s->reqs.erase(it);
             if (failed) throw Error{code, err.empty() ? "request failed" : err};
         }
+    });
+}
+
+int rkdg_server_status(rkdg_server* s, int32_t* queued, int32_t* in_flight) {
+    return guarded([&] {
+        if (!s) throw Error{RKDG_ERR_INVALID, "null server"};
+        std::lock_guard<std::mutex> lk(s->mu);
+        int n = 0;
+        for (auto& r : s->active) n += (r && r->status == REQ_RUNNING) ? 1 : 0;
+        if (queued) *queued = s->fatal.empty() ? (int32_t)s->queue.size() : 0;
+        if (in_flight) *in_flight = s->fatal.empty() ? n : 0;
+        if (!s->fatal.empty()) throw Error{s->fatal_code, "server stopped: " + s->fatal};
+    });
+}
+
+int rkdg_server_timing(rkdg_server* s, double* admit_s, double* retire_s, double* step_s, int64_t* chunks) {
+    return guarded([&] {
+        if (!s) throw Error{RKDG_ERR_INVALID, "null server"};
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (admit_s) *admit_s = s->t_admit;
+        if (retire_s) *retire_s = s->t_retire;
+        if (step_s) *step_s = s->busy;
+        if (chunks) *chunks = s->chunks;
+    });
+}
+
+int rkdg_server_inject_fault(rkdg_server* s, int32_t after_chunks) {
+    return guarded([&] {
+        if (!s || after_chunks < 0) throw Error{RKDG_ERR_INVALID, "rkdg_server_inject_fault: bad arguments"};
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->fault_after = after_chunks;
     });
 }
 

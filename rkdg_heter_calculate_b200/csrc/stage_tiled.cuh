@@ -1,6 +1,6 @@
 // Tile-staged fused stage kernel (included by kernels.cu).
 //
-// A tile is up to kTile consecutive (locality-ordered) elements of one
+// A tile is up to BT consecutive (locality-ordered) elements of one
 // solve; its descriptor names the element range, the solve, the polynomial
 // order, and its halo and flux-task ranges.  One CTA processes a tile:
 //   phase A  each thread: its element's state, volume integral (registers),
@@ -161,55 +161,58 @@ __device__ __forceinline__ void acc_rows(float R[NB][4], const float f[4], const
     for (int i = I0; i < NB; ++i) set4(R[i], f2fma(fl, tab[i], lo2(R[i])), f2fma(fh, tab[i], hi2(R[i])));
 }
 
-template <typename Real>
+template <typename Real, int BT>
 struct TiledLayout {
     // edge normals per element: FP32 (Nx, Ny) per edge, the length formed
     // where used; FP64 (Nx, Ny, length)
     static constexpr int NC = sizeof(Real) == 4 ? 2 : 3;
-    static constexpr size_t code_off = (sizeof(Real) * 3 * NC * kTile + 15) / 16 * 16;
+    static constexpr size_t code_off = (sizeof(Real) * 3 * NC * BT + 15) / 16 * 16;
 };
 
 // Cell means (own and halo) are kept only where the LLF coefficient needs
 // them.
-template <typename Real, int ORD, int FLUX>
+template <typename Real, int ORD, int FLUX, int BT>
 struct TiledSmem {
     static constexpr int NG = ORD == 1 ? 2 : 3;
     static constexpr int SROWS = (ORD == 1 ? 3 : 6) * (int)(sizeof(Real) / 4);
     static constexpr int MEANS = FLUX == RKDG_FLUX_LLF ? 1 : 0;
     static constexpr bool HALO_IN_STAGING = sizeof(Real) == 4;
     __host__ __device__ static constexpr size_t work(int hm) {
-        return TiledLayout<Real>::code_off + sizeof(int4) * kTile + sizeof(uint16_t) * 3 * kTile +
-               sizeof(Vec4<Real>) * ((size_t)3 * NG * kTile + MEANS * kTile +
+        return TiledLayout<Real, BT>::code_off + sizeof(int4) * BT + sizeof(uint16_t) * 3 * BT +
+               sizeof(Vec4<Real>) * ((size_t)3 * NG * BT + MEANS * BT +
                                      (HALO_IN_STAGING ? 0 : (size_t)(NG + MEANS) * hm));
     }
     __host__ __device__ static constexpr size_t stage_offset(int hm) { return (work(hm) + 127) / 128 * 128; }
     __host__ __device__ static constexpr size_t stage_rows(int hm) {
-        return (size_t)SROWS * (kTile > hm ? kTile : hm);
+        return (size_t)SROWS * (BT > hm ? BT : hm);
     }
     __host__ __device__ static constexpr size_t bytes(int hm) { return stage_offset(hm) + stage_rows(hm) * 16; }
 };
 
-// Resident CTAs per SM the register allocation is held to (FP32: 80
-// registers and at most 37 KB of shared memory per CTA, 24 warps per SM).
-template <typename Real, int ORD>
+// Resident CTAs per SM the register allocation is held to: 24 warps per SM
+// in FP32 (80 registers; 128-element tiles at most 37 KB of shared memory
+// per CTA), 8 (P2, 12 for P1) in FP64, whatever the tile size.
+template <typename Real, int ORD, int BT>
 struct TiledOccupancy {
-    static constexpr int value = sizeof(Real) == 8 ? (ORD == 1 ? 3 : 2) : 6;
+    static constexpr int warps = sizeof(Real) == 8 ? (ORD == 1 ? 12 : 8) : 24;
+    static constexpr int value = warps * 32 / BT > 0 ? warps * 32 / BT : 1;
 };
 
 // Issues the bulk copies of tile d's state rows into the staging area (one
 // thread; completion counted on bar).
-template <typename Real>
+template <typename Real, int BT>
 __device__ __forceinline__ void stage_copy(const StageArgs& a, const int4 d, unsigned char* stg, uint64_t* bar) {
     const int rows = (d.w == 2 ? 6 : 3) * (int)(sizeof(Real) / 4);
     const uint32_t rb = (uint32_t)d.y * 16u;
     mbar_expect_tx(bar, rb * (uint32_t)rows);
     const char* U = static_cast<const char*>(a.U);
     for (int r = 0; r < rows; ++r)
-        bulk_g2s(stg + (size_t)r * kTile * 16, U + ((size_t)r * a.ld + d.x) * 16, rb, bar);
+        bulk_g2s(stg + (size_t)r * BT * 16, U + ((size_t)r * a.ld + d.x) * 16, rb, bar);
 }
-// L2 prefetches of tile d's J^-1 and edge-code rows, U^n rows and halo and
-// task lists, and with STATE its state rows (one thread; the tables are
-// padded so that the 16-byte rounding stays inside them).
+// L2 prefetches of tile d's J^-1 and edge-code rows, U^n rows, the rows of
+// the means' low parts (RKDG_FP32C) and halo and task lists, and with STATE
+// its state rows (one thread; the tables are padded so that the 16-byte
+// rounding stays inside them).
 template <typename Real, bool STATE>
 __device__ __forceinline__ void stage_prefetch(const StageArgs& a, const TileArgs& ta, const int4 d,
                                                const int4 dd) {
@@ -227,6 +230,11 @@ __device__ __forceinline__ void stage_prefetch(const StageArgs& a, const TileArg
         const char* U0 = static_cast<const char*>(a.U0);
         for (int r = 0; r < rows; ++r) bulk_prefetch_l2(U0 + ((size_t)r * a.ld + d.x) * 16, rb);
     }
+    if (a.lo_row >= 0) {  // RKDG_FP32C: the low parts of the means, read by the update
+        const size_t lo = ((size_t)a.lo_row * a.ld + d.x) * 16;
+        bulk_prefetch_l2(static_cast<const char*>(a.U) + lo, rb);
+        if (a.U0 != nullptr) bulk_prefetch_l2(static_cast<const char*>(a.U0) + lo, rb);
+    }
     if (dd.y > 0) {
         const uintptr_t b = reinterpret_cast<uintptr_t>(ta.halo + dd.x) & ~uintptr_t(15);
         const uintptr_t e = (reinterpret_cast<uintptr_t>(ta.halo + dd.x + dd.y) + 15) & ~uintptr_t(15);
@@ -240,13 +248,13 @@ __device__ __forceinline__ void stage_prefetch(const StageArgs& a, const TileArg
 }
 
 // Element x's state from the staging rows.
-template <typename Real, int NB>
+template <typename Real, int NB, int BT>
 __device__ __forceinline__ void load_staged(const unsigned char* stg, int x, Real u[NB][4]) {
     if constexpr (sizeof(Real) == 8) {
         const double2* p = reinterpret_cast<const double2*>(stg);
 #pragma unroll
         for (int i = 0; i < NB; ++i) {
-            const double2 a = p[(2 * i) * kTile + x], b = p[(2 * i + 1) * kTile + x];
+            const double2 a = p[(2 * i) * BT + x], b = p[(2 * i + 1) * BT + x];
             u[i][0] = a.x;
             u[i][1] = a.y;
             u[i][2] = b.x;
@@ -256,7 +264,7 @@ __device__ __forceinline__ void load_staged(const unsigned char* stg, int x, Rea
         const float4* p = reinterpret_cast<const float4*>(stg);
 #pragma unroll
         for (int i = 0; i < NB; ++i) {
-            const float4 a = p[i * kTile + x];
+            const float4 a = p[i * BT + x];
             u[i][0] = a.x;
             u[i][1] = a.y;
             u[i][2] = a.z;
@@ -276,11 +284,11 @@ struct TilePre {
     double det;                         // det J^-1 = 1 / (2 area)
     int2 hh[3];
 };
-template <typename Real>
+template <typename Real, int BT>
 __device__ __forceinline__ TilePre<Real> tile_pre(const StageArgs& a, const TileArgs& ta, const int4 d0,
                                                   const int4 d1, const double2 r0, const double2 r1,
                                                   const int4 code, unsigned char* smem_raw) {
-    constexpr int BT = kTile, NC = TiledLayout<Real>::NC;
+    constexpr int NC = TiledLayout<Real, BT>::NC;
     const int tid = threadIdx.x;
     TilePre<Real> t;
     // far-field / reference state by value (a pointer into the parameter
@@ -295,8 +303,8 @@ __device__ __forceinline__ TilePre<Real> tile_pre(const StageArgs& a, const Tile
     t.rs = ref_state<Real>(fs, a.gamma);
     // the halo and task lists (L2 hits: prefetched with the tile's rows)
     const int h0 = d1.x, nh = d1.y, t0 = d1.z, nt = d1.w;
-    int4* s_code = reinterpret_cast<int4*>(smem_raw + TiledLayout<Real>::code_off);  // [BT]
-    uint16_t* s_task = reinterpret_cast<uint16_t*>(s_code + BT);                     // [3 BT]
+    int4* s_code = reinterpret_cast<int4*>(smem_raw + TiledLayout<Real, BT>::code_off);  // [BT]
+    uint16_t* s_task = reinterpret_cast<uint16_t*>(s_code + BT);                         // [3 BT]
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
         const int h = tid + r * BT;
@@ -330,26 +338,25 @@ __device__ __forceinline__ TilePre<Real> tile_pre(const StageArgs& a, const Tile
     return t;
 }
 
-template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE>
+template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE, int BT>
 __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& ta, const int4 d0,
                                            const int4 d1, unsigned char* smem_raw, unsigned char* stg,
                                            const int nxt, const int ntiles, uint64_t* bar,
                                            const TilePre<Real>& pre, Real (*s_red)[3], const double* s_dt) {
     constexpr int CFG = cfg_index(NQ, NG);
-    constexpr int BT = kTile;
     using V4 = Vec4<Real>;
     const Tab<Real>& tb = tab<Real>(CFG);
     const int HM = ta.max_halo;
-    constexpr int NC = TiledLayout<Real>::NC;
+    constexpr int NC = TiledLayout<Real, BT>::NC;
     Real* s_nrm = reinterpret_cast<Real*>(smem_raw);                       // [3][NC][BT] Nx, Ny (, len)
-    int4* s_code = reinterpret_cast<int4*>(smem_raw + TiledLayout<Real>::code_off);  // [BT]
+    int4* s_code = reinterpret_cast<int4*>(smem_raw + TiledLayout<Real, BT>::code_off);  // [BT]
     uint16_t* s_task = reinterpret_cast<uint16_t*>(s_code + BT);           // [3 BT] flux tasks
     V4* s_tr = reinterpret_cast<V4*>(s_task + 3 * BT);                     // [3][NG][BT] own traces
     constexpr int MEANS = FLUX == RKDG_FLUX_LLF ? 1 : 0;                   // LLF needs cell means
     V4* s_mean = s_tr + 3 * NG * BT;                                       // [BT] (LLF)
     // halo traces [NG][HM] and means [HM]: FP32 in the staging rows (trace g
     // of halo h in row g, entry h, of that neighbour's own staged state)
-    constexpr bool HALO_IN_STAGING = TiledSmem<Real, 3, FLUX>::HALO_IN_STAGING;
+    constexpr bool HALO_IN_STAGING = TiledSmem<Real, 3, FLUX, BT>::HALO_IN_STAGING;
     V4* s_htr = HALO_IN_STAGING ? reinterpret_cast<V4*>(stg) : s_mean + MEANS * BT;
     V4* s_hmean = s_htr + NG * HM;
     constexpr bool PK = sizeof(Real) == 4;  // FP32: lane-pair arithmetic, paired tables
@@ -393,7 +400,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     // formed once per state
     const Real k00 = tb.vphi[0][0];
     {
-        load_staged<Real, NB>(stg, sx, u);
+        load_staged<Real, NB, BT>(stg, sx, u);
         __syncthreads();  // staged rows consumed: the area takes the halo states
         {
             const char* Ub = static_cast<const char*>(a.U);
@@ -564,7 +571,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
         nd0 = __ldg(ta.desc + 2 * nxt);
         if constexpr (!HALO_IN_STAGING) {
             fence_proxy_async();
-            stage_copy<Real>(a, nd0, stg, bar);
+            stage_copy<Real, BT>(a, nd0, stg, bar);
         }
         stage_prefetch<Real, HALO_IN_STAGING>(a, ta, nd0, __ldg(ta.desc + 2 * nxt + 1));
     }
@@ -666,7 +673,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     __syncthreads();  // fluxes complete; FP32: halo traces read, the staging area takes the next tile's rows
     if (HALO_IN_STAGING && tid == 0 && nxt < ntiles) {
         fence_proxy_async();
-        stage_copy<Real>(a, nd0, stg, bar);
+        stage_copy<Real, BT>(a, nd0, stg, bar);
     }
 
     // ------------------------------------------------------------ phase C
@@ -819,11 +826,11 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 // The tile's maxima from s_red into its solve's control block (one thread,
 // after the barrier that closes the tile; bits of a non-negative double
 // order like the values).
-template <typename Real>
+template <typename Real, int BT>
 __device__ __forceinline__ void tile_maxima_atomic(const StageArgs& a, StepCtl* ctl, const Real (*s_red)[3]) {
     Real w = s_red[0][0], m0 = s_red[0][1], m1 = s_red[0][2];
 #pragma unroll
-    for (int k = 1; k < kTile / 32; ++k) {
+    for (int k = 1; k < BT / 32; ++k) {
         w = fmax(w, s_red[k][0]);
         m0 = fmax(m0, s_red[k][1]);
         m1 = fmax(m1, s_red[k][2]);
@@ -837,16 +844,17 @@ __device__ __forceinline__ void tile_maxima_atomic(const StageArgs& a, StepCtl* 
 
 // ORD: 1 = P1 tiles only, 2 = P2 tiles only, 3 = both (dispatch per tile;
 // P2 tiles use the NQ2-point volume rule, P1 tiles the 3/2-point rules).
+// BT: elements per tile = threads per CTA.
 // A barrier wait that times out sets bit 1 of the solve's error word and
 // ends the CTA (all threads together).
-template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
-__global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
+template <typename Real, int NQ2, int FLUX, int MODE, int ORD, int BT>
+__global__ void __launch_bounds__(BT, TiledOccupancy<Real, ORD, BT>::value)
     tiled_stage_kernel(const StageArgs a, const TileArgs ta) {
-    using SM = TiledSmem<Real, ORD, FLUX>;
+    using SM = TiledSmem<Real, ORD, FLUX, BT>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t s_bar;
-    __shared__ Real s_red[kTile / 32][3];  // per-warp maxima of a last stage
-    __shared__ double s_dt;                // the tile's solve's dt (read before the staging wait)
+    __shared__ Real s_red[BT / 32][3];  // per-warp maxima of a last stage
+    __shared__ double s_dt;             // the tile's solve's dt (read before the staging wait)
     unsigned char* stg = smem_raw + SM::stage_offset(ta.max_halo);
     const int ntiles = ta.ntiles_dev ? *ta.ntiles_dev : ta.ntiles;
     int tile = blockIdx.x;
@@ -855,7 +863,7 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
     __syncthreads();
     if (threadIdx.x == 0) {
         const int4 fd = __ldg(ta.desc + 2 * tile);
-        stage_copy<Real>(a, fd, stg, &s_bar);
+        stage_copy<Real, BT>(a, fd, stg, &s_bar);
         // FP64 (two CTAs per SM) gains from the first tile's table prefetch,
         // FP32 (six) loses
         if constexpr (sizeof(Real) == 8) stage_prefetch<Real, false>(a, ta, fd, __ldg(ta.desc + 2 * tile + 1));
@@ -872,7 +880,7 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
         const int4 code = __ldg(ta.code + ex);
         const int done = MODE != MODE_RESIDUAL ? a.ctl[d0.z].done : 0;
         if (MODE != MODE_RESIDUAL && threadIdx.x == 0) s_dt = a.ctl[d0.z].dt;
-        const TilePre<Real> pre = tile_pre<Real>(a, ta, d0, d1, r0, r1, code, smem_raw);
+        const TilePre<Real> pre = tile_pre<Real, BT>(a, ta, d0, d1, r0, r1, code, smem_raw);
         const bool ok = mbar_wait(&s_bar, parity);
         if (__syncthreads_or(!ok)) {  // also: every thread has seen this phase complete
             if (threadIdx.x == 0) atomicOr(&a.ctl[d0.z].error, 2);
@@ -880,16 +888,17 @@ __global__ void __launch_bounds__(kTile, TiledOccupancy<Real, ORD>::value)
         }
         parity ^= 1u;
         if (done) {  // finished solve: pass the tile on
-            if (threadIdx.x == 0 && nxt < ntiles) stage_copy<Real>(a, __ldg(ta.desc + 2 * nxt), stg, &s_bar);
+            if (threadIdx.x == 0 && nxt < ntiles) stage_copy<Real, BT>(a, __ldg(ta.desc + 2 * nxt), stg, &s_bar);
             continue;
         }
         if (ORD == 2 || (ORD == 3 && d0.w == 2))
-            tile_stage<Real, 6, NQ2, 3, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre, s_red,
-                                                   &s_dt);
+            tile_stage<Real, 6, NQ2, 3, FLUX, MODE, BT>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre, s_red,
+                                                       &s_dt);
         else
-            tile_stage<Real, 3, 3, 2, FLUX, MODE>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre, s_red,
-                                                 &s_dt);
+            tile_stage<Real, 3, 3, 2, FLUX, MODE, BT>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre, s_red,
+                                                     &s_dt);
         __syncthreads();  // shared memory is reused by the next tile
-        if (MODE != MODE_RESIDUAL && a.last_stage && threadIdx.x == 0) tile_maxima_atomic<Real>(a, a.ctl + d0.z, s_red);
+        if (MODE != MODE_RESIDUAL && a.last_stage && threadIdx.x == 0)
+            tile_maxima_atomic<Real, BT>(a, a.ctl + d0.z, s_red);
     }
 }

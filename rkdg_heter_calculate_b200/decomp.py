@@ -1,0 +1,280 @@
+"""Domain decomposition of one mesh over several devices.
+
+The reference splits a mesh over MPI ranks: each rank reads a partition
+file, finds its interface elements and builds inner-boundary ghost cells
+(multi_gpuRkdg/src/unstructuredgrid.cpp:290-318, 502-526), exchanges the
+interface indices once (src/sendboundaryindex.cpp:8-37), and before every
+stage copies its whole state to the host, packs the interface rows and sends
+them with MPI_Isend/MPI_Irecv (RkdgAdvance::commuInfo,
+src/rkdgadvance.cpp:287-409); its dt reduction over ranks is commented out
+(src/rkdgadvance.cpp:226-234).
+
+Here one process drives one device.  `Partition` splits the mesh into
+contiguous ranges of its locality (Morton) order and lists, per part, the
+halo copies it needs and, per pair of parts, the rows that cross.
+`DecomposedSolve` advances the parts held by this process: before every
+stage the halo rows are gathered on the owner's device (rkdg_gather_rows),
+moved device to device, and scattered into the receiver's halo rows
+(rkdg_scatter_rows); each step's dt is the minimum over all parts; with the
+TVB limiter the halo means of each stage output are refreshed before
+rkdg_limit.  The transport is pluggable: `TorchTransport` uses
+torch.distributed point-to-point operations (NCCL between GPUs, gloo on the
+host), `LocalTransport` moves rows between parts held by one process.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import capi, meshgen
+
+
+class Partition:
+    """k parts of a mesh: contiguous, equal-sized ranges of its locality
+    order.  For part p: `owned[p]` (caller element ids, in locality order),
+    `halo[p]` (caller ids of the other parts' elements that share an edge
+    with an owned one, grouped by owner and in the owner's order),
+    `local_mesh(p)` (owned elements first, then the halo copies), and for
+    each pair of parts the local indices that cross: `send[p][q]` (p-local
+    rows q needs, in q's halo order) and `recv[p][q]` (where they land in
+    p's halo)."""
+
+    def __init__(self, mesh: meshgen.Mesh, nparts: int):
+        if nparts < 1 or nparts > mesh.ntri:
+            raise ValueError("nparts must be in [1, ntri]")
+        T = mesh.ntri
+        order = capi.locality_order(mesh.vertices, mesh.tris, mesh.neighbours)  # new -> caller
+        bounds = np.rint(np.linspace(0, T, nparts + 1)).astype(np.int64)
+        owner = np.empty(T, dtype=np.int64)
+        pos = np.empty(T, dtype=np.int64)  # position in the owner's owned list
+        self.mesh = mesh
+        self.nparts = nparts
+        self.owned = []
+        for p in range(nparts):
+            ids = order[bounds[p]:bounds[p + 1]].astype(np.int64)
+            owner[ids] = p
+            pos[ids] = np.arange(ids.size)
+            self.owned.append(ids)
+        self.owner = owner
+        self.halo = []
+        for p in range(nparts):
+            nb = mesh.neighbours[self.owned[p]].ravel()
+            nb = np.unique(nb[nb >= 0])
+            nb = nb[owner[nb] != p]
+            key = owner[nb] * (T + 1) + pos[nb]
+            self.halo.append(nb[np.argsort(key, kind="stable")])
+        # rows crossing between parts: q's halo entries owned by p, in q's order
+        self.send = [dict() for _ in range(nparts)]
+        self.recv = [dict() for _ in range(nparts)]
+        for q in range(nparts):
+            h = self.halo[q]
+            n_own_q = self.owned[q].size
+            for p in np.unique(owner[h]):
+                sel = np.nonzero(owner[h] == p)[0]
+                self.send[int(p)][q] = pos[h[sel]].astype(np.int32)
+                self.recv[q][int(p)] = (n_own_q + sel).astype(np.int32)
+
+    def n_owned(self, p: int) -> int:
+        return int(self.owned[p].size)
+
+    def local_ids(self, p: int) -> np.ndarray:
+        """Caller ids of part p's local elements: owned, then halo copies."""
+        return np.concatenate([self.owned[p], self.halo[p]])
+
+    def local_mesh(self, p: int) -> meshgen.Mesh:
+        """Part p as a mesh: its owned elements and halo copies, neighbours
+        renumbered; a halo copy's edges to elements outside the part are
+        open (tagged outflow; the library never updates a halo copy)."""
+        m = self.mesh
+        ids = self.local_ids(p)
+        g2l = np.full(m.ntri, -1, dtype=np.int64)
+        g2l[ids] = np.arange(ids.size)
+        nb_g = m.neighbours[ids]
+        nb = np.where(nb_g >= 0, g2l[np.maximum(nb_g, 0)], -1).astype(np.int32)
+        bc = m.bc[ids].copy()
+        opened = (nb < 0) & (nb_g >= 0)  # edges of halo copies leaving the part
+        assert not opened[: self.n_owned(p)].any()
+        bc[opened] = capi.BC_OUTFLOW
+        return meshgen.Mesh(vertices=m.vertices, tris=np.ascontiguousarray(m.tris[ids]), neighbours=nb,
+                            bc=bc.astype(np.int8), periodic=m.periodic, name=f"{m.name}_part{p}", extent=m.extent)
+
+    def split(self, U: np.ndarray, p: int) -> np.ndarray:
+        """Part p's local state [4][nb][local] from a whole-mesh state."""
+        return np.ascontiguousarray(U[:, :, self.local_ids(p)])
+
+    def join(self, parts: dict) -> np.ndarray:
+        """A whole-mesh state from the parts' owned rows {p: [4][nb][local]}."""
+        first = next(iter(parts.values()))
+        out = np.zeros(first.shape[:2] + (self.mesh.ntri,))
+        for p, U in parts.items():
+            out[:, :, self.owned[p]] = U[:, :, : self.n_owned(p)]
+        return out
+
+
+class DevicePart:
+    """One part on the current device: a partition context (rkdg_create_part)
+    and the device index lists of its halo exchange."""
+
+    def __init__(self, partition: Partition, p: int, **solver_kw):
+        import torch
+
+        from .solver import CUDARkdgSolver
+
+        self.p = p
+        self.s = CUDARkdgSolver(partition.local_mesh(p), n_owned=partition.n_owned(p), **solver_kw)
+        self.limiter = solver_kw.get("limiter") is not None
+        rows, mean_rows = self.s.part_rows()
+        self.rows = {False: rows, True: mean_rows}
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self.send = {q: torch.tensor(v, device=dev) for q, v in partition.send[p].items()}
+        self.recv = {q: torch.tensor(v, device=dev) for q, v in partition.recv[p].items()}
+
+    def stream(self):
+        import torch
+
+        return torch.cuda.ExternalStream(self.s.stream())
+
+    def set_state(self, U, basis="reference"):
+        self.s.setFreedom(U, basis=basis)
+
+    def state(self, basis="reference"):
+        return self.s.copyFreedomToHost(basis=basis)
+
+    def time_step(self) -> float:
+        return self.s.getTimeStep()
+
+    def save_old(self):
+        self.s.saveOld()
+
+    def stage(self, st: int, dt: float):
+        self.s.stage(st, dt)
+
+    def limit(self):
+        self.s.limit()
+
+    def buffer(self, q: int, incoming: bool, means_only: bool):
+        import torch
+
+        n = (self.recv if incoming else self.send)[q].numel()
+        return torch.empty((n, self.rows[means_only], 16), dtype=torch.uint8, device=self.send_device())
+
+    def send_device(self):
+        import torch
+
+        return torch.device("cuda", torch.cuda.current_device())
+
+    def pack(self, q: int, means_only: bool):
+        buf = self.buffer(q, False, means_only)
+        idx = self.send[q]
+        capi.check(capi.lib().rkdg_gather_rows(self.s.h, idx.data_ptr(), idx.numel(), self.rows[means_only],
+                                               buf.data_ptr()))
+        return buf
+
+    def unpack(self, q: int, means_only: bool, buf):
+        idx = self.recv[q]
+        capi.check(capi.lib().rkdg_scatter_rows(self.s.h, idx.data_ptr(), idx.numel(), self.rows[means_only],
+                                                buf.data_ptr()))
+
+    def sync(self):
+        capi.check(capi.lib().rkdg_sync(self.s.h))
+
+    def close(self):
+        self.s.close()
+
+
+class LocalTransport:
+    """Every part held by this process: rows move between the parts'
+    buffers on one device, dt is the minimum over them."""
+
+    def exchange(self, parts: dict, means_only: bool):
+        bufs = {}
+        for p, part in parts.items():
+            for q in part.send:
+                bufs[(p, q)] = part.pack(q, means_only)
+            part.sync()
+        for p, part in parts.items():
+            for q in part.recv:
+                part.unpack(q, means_only, bufs[(q, p)])
+            part.sync()
+
+    def min(self, x: float) -> float:
+        return x
+
+
+class TorchTransport:
+    """One part per rank of a torch.distributed process group: the rows of
+    every neighbouring pair cross in one batch of point-to-point operations
+    (NCCL between GPUs: device to device, ordered on the part's stream; gloo
+    between host processes), and dt is an all-reduce minimum."""
+
+    def __init__(self, group=None):
+        import torch.distributed as dist
+
+        self.dist = dist
+        self.group = group
+
+    def exchange(self, parts: dict, means_only: bool):
+        import contextlib
+
+        import torch
+
+        (p, part), = parts.items()
+        ctx = torch.cuda.stream(part.stream()) if hasattr(part, "stream") else contextlib.nullcontext()
+        with ctx:
+            ops, incoming = [], {}
+            for q in sorted(set(part.send) | set(part.recv)):
+                if q in part.send:
+                    ops.append(self.dist.P2POp(self.dist.isend, part.pack(q, means_only), q, self.group))
+                if q in part.recv:
+                    incoming[q] = part.buffer(q, True, means_only)
+                    ops.append(self.dist.P2POp(self.dist.irecv, incoming[q], q, self.group))
+            if ops:
+                for w in self.dist.batch_isend_irecv(ops):
+                    w.wait()
+            for q, buf in incoming.items():
+                part.unpack(q, means_only, buf)
+        part.sync()
+
+    def min(self, x: float) -> float:
+        import torch
+
+        dev = "cuda" if self.dist.get_backend(self.group) == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MIN, group=self.group)
+        return float(t.item())
+
+
+class DecomposedSolve:
+    """The time loop over the parts this process holds ({part: DevicePart}
+    or any object with the same methods), with halo exchanges through
+    `transport`.  Every process takes the same exchange and reduction steps
+    in the same order."""
+
+    def __init__(self, parts: dict, transport, rk: int = 3, limiter: bool = False):
+        self.parts = parts
+        self.transport = transport
+        self.rk = rk
+        self.limiter = limiter
+
+    def step(self) -> float:
+        # halo copies current (so every part's dt sees true neighbour
+        # states), then dt as the minimum over all parts
+        self.transport.exchange(self.parts, False)
+        dt = self.transport.min(min(part.time_step() for part in self.parts.values()))
+        for part in self.parts.values():
+            part.save_old()
+        for st in range(self.rk):
+            if st > 0:
+                self.transport.exchange(self.parts, False)
+            for part in self.parts.values():
+                part.stage(st, dt)
+            if self.limiter:
+                self.transport.exchange(self.parts, True)
+                for part in self.parts.values():
+                    part.limit()
+        return dt
+
+    def advance(self, nsteps: int) -> float:
+        t = 0.0
+        for _ in range(nsteps):
+            t += self.step()
+        return t

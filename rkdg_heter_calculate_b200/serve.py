@@ -57,6 +57,7 @@ class Server:
         capi.check(capi.lib().rkdg_server_create(C.byref(p), int(hbm_budget_bytes), int(max_slots),
                                                  C.byref(h)))
         self.h = h
+        self.params = p
         self._shape = {}
 
     def close(self):
@@ -77,7 +78,8 @@ class Server:
             pass
 
     def submit(self, mesh, order: int, U0: np.ndarray, t_final: float, farfield=None,
-               limiter: bool = False) -> int:
+               limiter: bool = False, flux=None) -> int:
+        """Queues a solve; flux ("llf" / "hllc") defaults to the server's."""
         nb = 3 if order == 1 else 6
         T = int(mesh.tris.shape[0])
         U0 = np.ascontiguousarray(U0, dtype=np.float64)
@@ -86,9 +88,11 @@ class Server:
                                  getattr(mesh, "bc", None))
         far = None if farfield is None else np.ascontiguousarray(farfield, dtype=np.float64)
         rid = C.c_int64()
-        capi.check(capi.lib().rkdg_server_submit(self.h, C.byref(d), int(order), capi.dptr(U0),
-                                                 float(t_final), capi.dptr(far) if far is not None else None,
-                                                 int(bool(limiter)), C.byref(rid)))
+        fl = self.params.flux if flux is None else _FLUX[flux]
+        capi.check(capi.lib().rkdg_server_submit_method(self.h, C.byref(d), int(order), capi.dptr(U0),
+                                                        float(t_final),
+                                                        capi.dptr(far) if far is not None else None,
+                                                        int(bool(limiter)), fl, C.byref(rid)))
         del keep
         self._shape[rid.value] = (4, nb, T)
         return rid.value
@@ -105,6 +109,25 @@ class Server:
         capi.check(rc)
         return Result(rid, st.value, U if st.value == DONE else None, times[0], times[1], times[2],
                       steps.value)
+
+    def status(self) -> dict:
+        """Queued and in-flight counts; raises RkdgError once the loop has
+        stopped on an error."""
+        q, f = C.c_int32(), C.c_int32()
+        capi.check(capi.lib().rkdg_server_status(self.h, C.byref(q), C.byref(f)))
+        return {"queued": q.value, "in_flight": f.value}
+
+    def inject_fault(self, after_chunks: int = 0):
+        """Test support: the loop stops as on a failed CUDA call (nothing is
+        done to the device)."""
+        capi.check(capi.lib().rkdg_server_inject_fault(self.h, int(after_chunks)))
+
+    def timing(self) -> dict:
+        """Engine seconds uploading, retiring and stepping, and step chunks."""
+        a, r, st = C.c_double(), C.c_double(), C.c_double()
+        n = C.c_int64()
+        capi.check(capi.lib().rkdg_server_timing(self.h, C.byref(a), C.byref(r), C.byref(st), C.byref(n)))
+        return {"admit_s": a.value, "retire_s": r.value, "step_s": st.value, "chunks": n.value}
 
     def stats(self) -> dict:
         dof, busy = C.c_double(), C.c_double()

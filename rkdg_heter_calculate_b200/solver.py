@@ -54,7 +54,7 @@ class CUDARkdgSolver:
 
     def __init__(self, mesh, order=2, nq=7, ng=3, flux="llf", limiter=None, rk=3,
                  precision="fp64", gamma=1.4, cfl=0.18, tvb_m=50.0, farfield=None,
-                 reorder=True):
+                 reorder=True, n_owned=None):
         p = capi.default_params()
         p.order, p.nq, p.ng = order, nq, ng
         p.flux = _FLUX[flux]
@@ -72,7 +72,10 @@ class CUDARkdgSolver:
         d, keep = capi.mesh_desc(mesh.vertices, mesh.tris, getattr(mesh, "neighbours", None),
                                  getattr(mesh, "bc", None))
         h = C.c_void_p()
-        capi.check(capi.lib().rkdg_create(C.byref(d), C.byref(p), C.byref(h)))
+        if n_owned is None:
+            capi.check(capi.lib().rkdg_create(C.byref(d), C.byref(p), C.byref(h)))
+        else:  # one partition of a decomposed mesh (see decomp.py)
+            capi.check(capi.lib().rkdg_create_part(C.byref(d), C.byref(p), int(n_owned), C.byref(h)))
         self.h = h
         self.T = d.ntri
 
@@ -100,6 +103,12 @@ class CUDARkdgSolver:
         by = C.c_size_t()
         capi.check(capi.lib().rkdg_get_sizes(self.h, C.byref(t), C.byref(nb), C.byref(by)))
         return t.value, nb.value, by.value
+
+    def part_rows(self):
+        """(all state rows, cell-mean rows) of 16 bytes per element."""
+        a, b = C.c_int32(), C.c_int32()
+        capi.check(capi.lib().rkdg_part_rows(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def stream(self) -> int:
         s = C.c_void_p()

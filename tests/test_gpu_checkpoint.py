@@ -1,8 +1,8 @@
 """Checkpoint and resume: a run stopped after some steps, written to a file
 and restored into a fresh context on the same mesh continues bit for bit
 (state, time and step count) as the run that never stopped; a file written
-for another mesh, order or far field is refused, and a missing file is an
-I/O error."""
+for another mesh, order, precision, far field, flux, CFL number or gamma is
+refused, and a missing file is an I/O error."""
 import numpy as np
 import pytest
 
@@ -74,7 +74,15 @@ def test_mismatched_checkpoints_are_refused(tmp_path):
     for other in (solver(meshgen.periodic_delaunay(12, seed=2), "fp32"),   # another mesh, same size
                   solver(mesh, "fp64"),                                      # another precision
                   solver(mesh, "fp32", order=1),                             # another order
-                  solver(mesh, "fp32", far=primitive_to_conservative(1.0, 0.5, 0.0, 1.0))):
+                  solver(mesh, "fp32", far=primitive_to_conservative(1.0, 0.5, 0.0, 1.0)),
+                  # another flux, CFL number or gamma: the saved wave maximum and state belong to
+                  # the writer's method and physics
+                  CUDARkdgSolver(mesh, order=2, nq=6, ng=3, flux="llf", rk=3, precision="fp32", cfl=0.2,
+                                 farfield=FAR),
+                  CUDARkdgSolver(mesh, order=2, nq=6, ng=3, flux="hllc", rk=3, precision="fp32", cfl=0.3,
+                                 farfield=FAR),
+                  CUDARkdgSolver(mesh, order=2, nq=6, ng=3, flux="hllc", rk=3, precision="fp32", cfl=0.2,
+                                 farfield=FAR, gamma=1.3)):
         with pytest.raises(capi.RkdgError) as e:
             other.restore(path)
         assert e.value.code == capi.RKDG_ERR_INVALID

@@ -6,7 +6,9 @@ against include/rkdg.h and librkdg.so and run on the reference's own
 NACA0012 mesh set (fixture tests/golden/naca0012_previous.npz, written back
 in the reference's file format): its final state equals the same sequence
 through the Python binding bit for bit, and matches the oracle and the
-reference's own CUDA kernels (oracle/_ref/gpu) to 1e-12.  Its solution.plt
+reference's own code built for the host (oracle/_ref) after twenty steps to
+1e-11; the reference's CUDA kernels (oracle/_ref/gpu) give the same
+residual on it.  Its solution.plt
 is byte-identical to the file the reference's own writer
 (CCUDARkdgSolver::outputSolution, src/cudarkdgsolver.cu:860-1001) makes
 from the same cell means.
@@ -19,7 +21,7 @@ import numpy as np
 import pytest
 
 from helpers import rel_err
-from oracle import oracle, ref_gpu
+from oracle import oracle, ref, ref_gpu
 from rkdg_heter_calculate_b200 import CUDARkdgSolver, meshgen
 from rkdg_heter_calculate_b200.solver import freestream_state
 
@@ -91,8 +93,26 @@ def test_cpp_caller_matches_oracle(cpp_run):
     for _ in range(NSTEPS):
         o.step()
     U = read_state(work, "state_reference.bin", T)
-    assert rel_err(U, o.state()) < 1e-12
+    # twenty steps: rounding accumulates over the stages (the host build of
+    # the reference and the oracle differ by 1e-12 here)
+    assert rel_err(U, o.state()) < 1e-11
     assert np.abs(U[:, 1:]).max() > 1e-6  # the airfoil has disturbed the free stream
+
+
+@pytest.mark.skipif(not ref.available(), reason="the reference's host build (oracle/_ref) is absent")
+def test_cpp_caller_matches_reference_host_build(cpp_run):
+    """The reference's own code compiled for the host (oracle/_ref), run the
+    same twenty steps from the same free stream on the same mesh files."""
+    work, mesh = cpp_run
+    T = mesh.ntri
+    far = freestream_state(1.4, 0.4, 5.0)
+    r = ref.RefCase(mesh, alpha_deg=5.0, mach=0.4, cfl=0.18)
+    U0 = np.zeros((4, 6, T))
+    U0[:, 0, :] = np.array(far)[:, None]
+    r.set_dofs(U0)
+    r.advance(NSTEPS)
+    assert rel_err(read_state(work, "state_reference.bin", T), r.dofs()) < 1e-11
+    r.close()
 
 
 @pytest.mark.skipif(not ref_gpu.available(), reason="the reference's GPU build (oracle/_ref/gpu) is absent")
@@ -100,12 +120,15 @@ def test_cpp_caller_matches_reference_kernels_and_writer(cpp_run):
     work, mesh = cpp_run
     T = mesh.ntri
     g = ref_gpu.RefGpuCase(mesh, alpha_deg=5.0, mach=0.4, cfl=0.18)
-    far = freestream_state(1.4, 0.4, 5.0)
-    U0 = np.zeros((4, 6, T))
-    U0[:, 0, :] = np.array(far)[:, None]
-    g.set_state(U0)
-    g.steps(NSTEPS)
-    assert rel_err(read_state(work, "state_reference.bin", T), g.state()) < 1e-12
+    # the reference's own kernels on the C++ caller's final state: the same
+    # residual (its multi-step runs are not compared: its block reductions of
+    # dt rely on implicit warp synchrony, which sm_100 does not give)
+    U = read_state(work, "state_reference.bin", T)
+    g.set_state(U)
+    s = CUDARkdgSolver(mesh)
+    s.setFreedom(U)
+    assert rel_err(s.residual(), g.residual()) < 1e-10
+    s.close()
     # the reference's writer on the C++ caller's cell means: the same bytes
     ref_plt = str(work / "output" / "solution_reference_writer.plt")
     g.write_solution(read_state(work, "state_native.bin", T)[:, 0, :], ref_plt)

@@ -41,12 +41,25 @@ def shuffled(mesh, seed):
                         extent=mesh.extent)
 
 
-def stages_against_oracle(s, o, U0, nsteps, rk):
-    """R(U0), then nsteps steps stage by stage: dt and every stage's state."""
+def where(a, b):
+    """Largest difference: (relative error, [var, basis, element], count of
+    elements off by more than 1e-12 of max |b|)."""
+    d = np.abs(a - b)
+    i = np.unravel_index(np.argmax(d), d.shape)
+    scale = np.abs(b).max()
+    return d[i] / scale, list(map(int, i)), int((d.max(axis=(0, 1)) > 1e-12 * scale).sum())
+
+
+def stages_against_oracle(s, o, U0, nsteps, rk, tol_r=TOL, tol_stage=TOL, max_off=0):
+    """R(U0), then nsteps steps stage by stage: dt and every stage's state
+    (at most max_off elements may differ by more than 1e-12, none by more
+    than tol_stage)."""
     s.setFreedom(U0)
     o.set_state(U0)
-    assert rel_err(s.residual(), o.residual()) < TOL
-    for _ in range(nsteps):
+    e_r = where(s.residual(), o.residual())
+    print(f"R(U): {e_r}")
+    assert e_r[0] < tol_r
+    for n in range(nsteps):
         dt_o = o.time_step()
         dt_g = s.getTimeStep()
         assert dt_g == pytest.approx(dt_o, rel=1e-13)
@@ -55,8 +68,9 @@ def stages_against_oracle(s, o, U0, nsteps, rk):
         for st in range(rk):
             o.stage(st, dt_o)
             s.stage(st, dt_o)
-            e = rel_err(s.copyFreedomToHost(), o.state())
-            assert e < TOL, f"stage {st}: {e:.2e}"
+            e = where(s.copyFreedomToHost(), o.state())
+            print(f"step {n} stage {st}: {e}")
+            assert e[0] < tol_stage and e[2] <= max_off, f"step {n} stage {st}: {e}"
 
 
 def test_unstructured_vortex_980k_p2_hllc():
@@ -69,7 +83,14 @@ def test_unstructured_vortex_980k_p2_hllc():
     o = oracle.Oracle(mesh, order=2, nq=6, ng=3, flux=oracle.HLLC, rk=3, farfield=far, cfl=0.2)
     U0 = vortex_state(mesh, o.basis()["coeff"], 6)
     s = CUDARkdgSolver(mesh, order=2, nq=6, ng=3, flux="hllc", rk=3, cfl=0.2, farfield=far)
-    stages_against_oracle(s, o, U0, 2, 3)
+    # R(U) is the small difference of volume and surface terms O(1/h) larger
+    # than itself: its relative rounding grows as the mesh is refined.  The
+    # states: the reference's basis (which the oracle restates) is evaluated
+    # as polynomials in (x - x_c)/sqrt(A) at physical points, whose rounding
+    # on triangles of 0.014 at coordinates up to 10 is eps |x|/h ~ 1e-13 and
+    # enters the quadratic modes squared; at this size the two codes agree to
+    # a few 1e-12 in the highest modes (1e-12 and below on coarser meshes)
+    stages_against_oracle(s, o, U0, 2, 3, tol_r=1e-10, tol_stage=1e-11, max_off=5000)
     s.close()
     o.close()
 
@@ -104,24 +125,30 @@ def test_step_with_walls_and_limiter(reorder):
     U0 = step_state(mesh, o.basis()["coeff"], far)
     s = CUDARkdgSolver(mesh, order=1, nq=3, ng=2, flux="llf", rk=3, limiter="tvb", tvb_m=50.0, cfl=0.3,
                        farfield=far, reorder=reorder)
-    stages_against_oracle(s, o, U0, 2, 3)
+    # the limiter's minmod and TVB threshold are switches: where two of their
+    # arguments agree to rounding, the two codes may take different sides and
+    # differ by that (tiny) gap; a handful of elements may do so
+    stages_against_oracle(s, o, U0, 2, 3, tol_stage=1e-10, max_off=20)
     s.close()
     o.close()
 
 
-def test_batch_persistent_loop_and_long_halo_lists():
-    """A pack of P1 and P2 solves (shuffled meshes, no locality order, so the
-    halo lists run to hundreds of entries per tile) advanced with 37 CTAs for
-    hundreds of tiles (each CTA loops over many tiles, the staging pipeline
-    crossing solves): every solve matches the oracle after two steps, and the
-    persistent run equals the one-CTA-per-tile run bit for bit."""
+@pytest.mark.parametrize("tile,shuffle", [(128, True), (256, False)])
+def test_batch_persistent_loop_and_long_halo_lists(tile, shuffle):
+    """A pack of P1 and P2 solves advanced with 37 CTAs for hundreds of tiles
+    (each CTA loops over many tiles, the staging pipeline crossing solves):
+    every solve matches the oracle after two steps, and the persistent run
+    equals the one-CTA-per-tile run bit for bit.  With 128-element tiles on
+    shuffled meshes (no locality order: halo lists of hundreds of entries per
+    tile), and with 256-element tiles in the locality order."""
     specs = [(meshgen.periodic_delaunay(90, seed=21), 2, 5.0, 0.4),
              (meshgen.periodic_delaunay(70, seed=22), 1, 3.0, 2.0),
              (meshgen.periodic_delaunay(60, seed=23), 2, 1.5, 4.0),
              (meshgen.periodic_structured(50, 50, jitter=0.2, seed=24), 1, 4.0, 5.5)]
     meshes, orders, states, fars, oracles = [], [], [], [], []
     for i, (m, order, beta, th) in enumerate(specs):
-        m = shuffled(m, 30 + i)
+        if shuffle:
+            m = shuffled(m, 30 + i)
         ui, vi = np.sqrt(2) * np.cos(th), np.sqrt(2) * np.sin(th)
         far = primitive_to_conservative(1.0, ui, vi, 1.0)
         kw = dict(order=2, nq=6, ng=3) if order == 2 else dict(order=1, nq=3, ng=2)
@@ -132,9 +159,10 @@ def test_batch_persistent_loop_and_long_halo_lists():
         states.append(U)
     results = []
     for ctas in (37, 0):
-        b = Batch(meshes, orders, precision="fp64", flux="hllc", cfl=0.2, farfields=fars, reorder=False)
+        b = Batch(meshes, orders, precision="fp64", flux="hllc", cfl=0.2, farfields=fars, reorder=not shuffle)
+        b.set_tile(tile)
         _, ntiles, _ = b.sizes()
-        assert ntiles > 4 * 37
+        assert ntiles > 2 * 37
         b.set_shape(ctas)
         for i, (m, U, o) in enumerate(zip(meshes, states, oracles)):
             b.set_state(i, native_of(m, U, o))

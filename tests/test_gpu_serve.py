@@ -15,14 +15,16 @@ from rkdg_heter_calculate_b200.solver import freestream_state, primitive_to_cons
 
 pytestmark = pytest.mark.gpu
 MB = 1 << 20
-# LLF for every request: the Mach-3 step with the Davis-speed HLLC flux goes
-# non-physical at the step corner (FP64 and FP32 alike) under P1 + TVB
+# Each request carries its flux: HLLC for the vortex requests, LLF for the
+# limited ones (the Mach-3 step with the Davis-speed HLLC flux goes
+# non-physical at the step corner, FP64 and FP32 alike, under P1 + TVB)
 TVB_M = 50.0
 SERVER = dict(flux="llf", rk=3, cfl=0.2, tvb_m=TVB_M)
 
 
 def requests():
-    """(mesh, order, U0 native, t_final, far field, limiter)."""
+    """(mesh, order, U0 native, t_final, far field, limiter, flux): vortex
+    requests with HLLC, the limited ones with LLF."""
     out = []
     for m, order, beta, th, tf in [
         (meshgen.periodic_delaunay(20, seed=11), 2, 5.0, 0.3, 0.21),
@@ -34,26 +36,26 @@ def requests():
         nb = 3 if order == 1 else 6
         U = vortex.project_native(m, lambda X, Y: vortex.exact(X, Y, 0.0, beta, 1.4, ui, vi), nb)
         far = np.array([1.0, ui, vi, 2.5 + 0.5 * (ui * ui + vi * vi)])
-        out.append((m, order, U, tf, far, False))
+        out.append((m, order, U, tf, far, False, "hllc"))
     # Mach-3 wind-tunnel step, P1 with the TVB limiter, started from the inflow state
     step = meshgen.forward_step(h=1.0 / 30)
     far = np.array(primitive_to_conservative(1.4, 3.0, 0.0, 1.0))
     U = np.zeros((4, 3, step.ntri))
     U[:, 0, :] = far[:, None]
-    out.append((step, 1, U, 0.02, far, True))
+    out.append((step, 1, U, 0.02, far, True, "llf"))
     # subsonic flow around a square cylinder, P2 with the limiter
     box = meshgen.box_with_obstacle(16)
     far = np.array(freestream_state())
     U = np.zeros((4, 6, box.ntri))
     U[:, 0, :] = far[:, None]
-    out.append((box, 2, U, 1.0, far, True))
+    out.append((box, 2, U, 1.0, far, True, "llf"))
     return out
 
 
 def solo(req, precision):
-    m, order, U, tf, far, lim = req
+    m, order, U, tf, far, lim, flux = req
     kw = dict(order=2, nq=6, ng=3) if order == 2 else dict(order=1, nq=3, ng=2)
-    s = CUDARkdgSolver(m, flux="llf", rk=3, precision=precision, cfl=0.2, farfield=far,
+    s = CUDARkdgSolver(m, flux=flux, rk=3, precision=precision, cfl=0.2, farfield=far,
                        limiter="tvb" if lim else None, tvb_m=TVB_M, **kw)
     s.setFreedom(U, basis="native")
     t, n = s.advance(1000000, t_final=tf)
@@ -63,8 +65,8 @@ def solo(req, precision):
 
 
 def submit(srv, req):
-    m, order, U, tf, far, lim = req
-    return srv.submit(m, order, U, tf, farfield=far, limiter=lim)
+    m, order, U, tf, far, lim, flux = req
+    return srv.submit(m, order, U, tf, farfield=far, limiter=lim, flux=flux)
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp32c", "fp64"])
@@ -97,7 +99,7 @@ def test_budget_and_slots_bound_admission():
     reqs = requests()
     big = max(r[0].ntri for r in reqs)
     # a pool of about 1.2x the largest request: the rest queue until memory frees
-    per_elem = 3 * 24 * 4 + 227 + 192   # FP32 pool bytes per element, staging included
+    per_elem = 3 * 24 * 4 + 107 + 192   # FP32 pool bytes per element, staging included
     budget = 64 * MB + int(1.2 * big) * per_elem
     with Server(budget, max_slots=3, precision="fp32", **SERVER) as srv:
         cap = srv.stats()["capacity_elements"]
@@ -115,7 +117,8 @@ def test_budget_and_slots_bound_admission():
 
 def test_oversized_request_rejected():
     reqs = requests()
-    with Server(64 * MB + 4200 * 707, max_slots=2, precision="fp32", **SERVER) as srv:
+    per_elem = 3 * 24 * 4 + 107 + 192   # FP32 pool bytes per element, staging included
+    with Server(64 * MB + 4300 * per_elem, max_slots=2, precision="fp32", **SERVER) as srv:
         step = reqs[4]
         assert step[0].ntri > srv.stats()["capacity_elements"]
         with pytest.raises(capi.RkdgError) as e:
@@ -125,12 +128,12 @@ def test_oversized_request_rejected():
 
 def test_failed_request_fails_alone():
     reqs = requests()
-    m, order, U, tf, far, lim = reqs[2]
+    m, order, U, tf, far, lim, flux = reqs[2]
     bad = U.copy()
     bad[0, 0, 5] = -1.0   # negative density in one cell
     with Server(128 * MB, max_slots=4, precision="fp32", **SERVER) as srv:
         good_id = submit(srv, reqs[3])
-        bad_id = srv.submit(m, order, bad, tf, farfield=far)
+        bad_id = srv.submit(m, order, bad, tf, farfield=far, flux=flux)
         with pytest.raises(capi.RkdgError) as e:
             srv.wait(bad_id)
         assert e.value.code == capi.RKDG_ERR_STATE
@@ -138,3 +141,29 @@ def test_failed_request_fails_alone():
     assert res.status == DONE
     ref, _, _ = solo(reqs[3], "fp32")
     np.testing.assert_array_equal(res.state, ref)
+
+
+def test_engine_failure_fails_every_request_and_is_reported():
+    """A failure of the loop (a CUDA call failing, simulated on the host by
+    rkdg_server_inject_fault: nothing touches the device) fails every request
+    that is in flight or queued, is reported by the status query, and later
+    submits are refused."""
+    reqs = requests()
+    with Server(256 * MB, max_slots=2, precision="fp32", **SERVER) as srv:
+        assert srv.status() == {"queued": 0, "in_flight": 0}
+        long_run = (reqs[0][0], reqs[0][1], reqs[0][2], 50.0, reqs[0][4], False, "hllc")
+        ids = [submit(srv, long_run) for _ in range(4)]  # two in flight, two queued (2 slots)
+        time.sleep(0.2)
+        st = srv.status()
+        assert st["in_flight"] == 2 and st["queued"] == 2
+        srv.inject_fault(1)
+        for rid in ids:
+            with pytest.raises(capi.RkdgError) as e:
+                srv.wait(rid, timeout=60.0)
+            assert e.value.code == capi.RKDG_ERR_CUDA and "inject_fault" in str(e.value)
+        with pytest.raises(capi.RkdgError) as e:
+            srv.status()
+        assert e.value.code == capi.RKDG_ERR_CUDA
+        with pytest.raises(capi.RkdgError) as e:
+            submit(srv, reqs[3])
+        assert e.value.code == capi.RKDG_ERR_CUDA

@@ -50,6 +50,36 @@ def test_noalloc_totals_match_context_totals_on_two_calls():
     s.close()
 
 
+def test_noalloc_totals_in_place_on_a_full_state_and_its_own_stream():
+    """A caller that keeps its whole state on the device in the reference
+    layout [4][nbasis][ld] passes it in place: the mean rows (row 0 of each
+    variable's block) are nbasis * ld apart, so d_means is the array itself
+    with that stride.  The call is ordered on a stream the caller created."""
+    import torch
+
+    mesh = meshgen.periodic_delaunay(40, seed=8)
+    T = mesh.ntri
+    s = CUDARkdgSolver(mesh, order=2, nq=6, ng=3, flux="hllc", rk=3, farfield=(1.0, 1.0, 1.0, 3.5))
+    U = vortex.project_native(mesh, lambda X, Y: vortex.exact(X, Y, 0.0, beta=4.0), 6)
+    s.setFreedom(U, basis="native")
+    s.advance(2)
+    expected = s.conservation_totals()
+    state = s.copyFreedomToHost(basis="native")  # [4][6][T]
+    s.close()
+    ld = T + 3
+    full = np.zeros((4, 6, ld))
+    full[:, :, :T] = state
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        d_state = torch.tensor(full, dtype=torch.float64, device="cuda")
+        d_area = torch.tensor(mesh.areas(), dtype=torch.float64, device="cuda")
+        d_out = torch.full((4,), float("nan"), dtype=torch.float64, device="cuda")
+    rc = _call(T, d_state.data_ptr(), 6 * ld, d_area.data_ptr(), d_out.data_ptr(), stream.cuda_stream)
+    assert rc == 0, capi.lib().rkdg_last_error()
+    stream.synchronize()
+    np.testing.assert_allclose(d_out.cpu().numpy(), expected, rtol=1e-12, atol=0.0)
+
+
 def test_noalloc_rejects_oversized_meshes():
     rc = _call(4096 * 256 + 1, 1, 4096 * 256 + 1, 1, 1, 0)
     assert rc == capi.RKDG_OK + 1  # RKDG_ERR_INVALID, no launch
