@@ -5,7 +5,7 @@
 // solve id and order, and one tile-staged launch per RK stage covers all of
 // them.  Per-solve control blocks hold dt, time, final time, the CFL measure
 // and the monitor, so solves advance with their own time steps inside one
-// CUDA graph of the whole step.
+// CUDA graph of whole steps (one, and eight for long runs).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -39,7 +39,8 @@ struct rkdg_batch {
     StepCtl* ctl = nullptr;
     StepCtl* h_ctl = nullptr;
     cudaStream_t stream = nullptr;
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph = nullptr;   // one step
+    cudaGraphExec_t graph_n = nullptr; // kGraphSteps steps (fewer graph launches and boundaries)
     int ctas = 0, tile_order = 0, tile = kTile;
     std::vector<HostMesh> topo;  // per solve (internal order): T, neighbours, shared edges, tags
     size_t table_bytes = 0;      // device bytes of the tile tables (rebuilt with the tile size)
@@ -201,10 +202,34 @@ void build_batch_tiles(rkdg_batch* b) {
     sync(b);  // host tables go out of scope
 }
 
+constexpr int kGraphSteps = 8;
+
+// A graph of `steps` whole steps on the batch's stream.
+cudaGraphExec_t capture_steps(rkdg_batch* b, int steps) {
+    cudaGraph_t g;
+    RKDG_CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        for (int i = 0; i < steps; ++i) enqueue_step(b);
+    } catch (...) {
+        cudaStreamEndCapture(b->stream, &g);
+        throw;
+    }
+    RKDG_CUDA_TRY(cudaStreamEndCapture(b->stream, &g));
+    cudaGraphExec_t e = nullptr;
+    cudaError_t err = cudaGraphInstantiate(&e, g, 0);
+    cudaGraphDestroy(g);
+    RKDG_CUDA_TRY(err);
+    return e;
+}
+
 void drop_graph(rkdg_batch* b) {
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
+    }
+    if (b->graph_n) {
+        cudaGraphExecDestroy(b->graph_n);
+        b->graph_n = nullptr;
     }
 }
 
@@ -406,24 +431,14 @@ int rkdg_batch_advance(rkdg_batch* b, int32_t nsteps, const double* t_final, dou
             b->h_ctl[s].done = 0;
         }
         push(b);
-        if (!b->graph) {
-            cudaGraph_t g;
-            RKDG_CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-            try {
-                enqueue_step(b);
-            } catch (...) {
-                cudaStreamEndCapture(b->stream, &g);
-                throw;
-            }
-            RKDG_CUDA_TRY(cudaStreamEndCapture(b->stream, &g));
-            RKDG_CUDA_TRY(cudaGraphInstantiate(&b->graph, g, 0));
-            cudaGraphDestroy(g);
-        }
+        if (!b->graph) b->graph = capture_steps(b, 1);
+        if (!b->graph_n && nsteps >= kGraphSteps) b->graph_n = capture_steps(b, kGraphSteps);
         int left = nsteps;
         const int chunk = any_final ? 32 : std::max(1, nsteps);
         while (left > 0) {
             const int n = std::min(left, chunk);
-            for (int i = 0; i < n; ++i) RKDG_CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
+            for (int i = 0; i < n / kGraphSteps; ++i) RKDG_CUDA_TRY(cudaGraphLaunch(b->graph_n, b->stream));
+            for (int i = 0; i < n % kGraphSteps; ++i) RKDG_CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
             left -= n;
             if (any_final && left > 0) {
                 pull(b);

@@ -40,7 +40,8 @@ struct rkdg_ctx {
     bool conv_ready = false;
     bool wave_valid = false;
     bool have_state = false;
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph = nullptr;    // one step
+    cudaGraphExec_t graph_n = nullptr;  // kGraphSteps steps (fewer graph launches and boundaries)
     StepCtl* h_ctl = nullptr;  // pinned mirror of the device control block
     TileArgs tiles{};
     int ctas = 0;     // tiled grid size (0: one CTA per tile)
@@ -163,6 +164,7 @@ StageArgs base_args(const rkdg_ctx* c) {
     a.gamma = c->p.gamma;
     for (int v = 0; v < 4; ++v) a.far[v] = c->p.farfield[v];
     a.lo_row = lo_row(c);
+    a.tvb_m = c->p.tvb_m;
     return a;
 }
 
@@ -186,12 +188,14 @@ void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out, bool monitor 
     a.Unew = c->d.U[out];
     a.last_stage = s == c->p.rk - 1;
     a.monitor = monitor ? 1 : 0;
-    launch_stage(a, c->tiles, c->p.order, c->p.nq, c->p.flux, kprec(c), c->ctas, c->stream);
     // a partition applies its limiter by rkdg_limit once the halo means of
     // the stage output have been exchanged
-    if (c->p.limiter == RKDG_LIMITER_TVB && c->T_own == c->T)
+    const bool limit = c->p.limiter == RKDG_LIMITER_TVB && c->T_own == c->T;
+    a.tile_flags = limit ? c->d.tile_flags : nullptr;  // the stage's per-tile limiter test
+    launch_stage(a, c->tiles, c->p.order, c->p.nq, c->p.flux, kprec(c), c->ctas, c->stream);
+    if (limit)
         launch_tiled_limiter(c->tiles, 0, c->ld, c->d.U[out], c->d.conn, c->d.lim, c->d.jinv, nullptr,
-                             c->d.far, kprec(c), c->p.nq, c->p.gamma, c->p.tvb_m, c->d.ctl,
+                             c->d.far, kprec(c), c->p.nq, c->p.gamma, c->p.tvb_m, c->d.ctl, c->d.tile_flags,
                              c->stream);
 }
 
@@ -207,6 +211,26 @@ void enqueue_step(rkdg_ctx* c, bool monitor) {
         launch_one_stage(c, 0, 0, 0, 1, monitor);
         launch_one_stage(c, 1, 1, 0, 0, monitor);
     }
+}
+
+constexpr int kGraphSteps = 8;
+
+// A graph of `steps` whole steps on the context's stream.
+cudaGraphExec_t capture_steps(rkdg_ctx* c, int steps, bool monitor) {
+    cudaGraph_t g;
+    RKDG_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        for (int i = 0; i < steps; ++i) enqueue_step(c, monitor);
+    } catch (...) {
+        cudaStreamEndCapture(c->stream, &g);
+        throw;
+    }
+    RKDG_CUDA_TRY(cudaStreamEndCapture(c->stream, &g));
+    cudaGraphExec_t e = nullptr;
+    cudaError_t err = cudaGraphInstantiate(&e, g, 0);
+    cudaGraphDestroy(g);
+    RKDG_CUDA_TRY(err);
+    return e;
 }
 
 void check_error_flag(rkdg_ctx* c) {
@@ -229,11 +253,13 @@ void destroy_ctx(rkdg_ctx* c) {
     cudaGetDevice(&prev);
     cudaSetDevice(c->device);
     if (c->graph) cudaGraphExecDestroy(c->graph);
+    if (c->graph_n) cudaGraphExecDestroy(c->graph_n);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (void* p : {c->d.U[0], c->d.U[1], c->d.U[2]}) cudaFree(p);
     cudaFree(c->d.jinv);
     cudaFree(c->d.conn);
     cudaFree(c->d.lim);
+    cudaFree(c->d.tile_flags);
     cudaFree(c->d.perm);
     cudaFree(c->d.conv_in);
     cudaFree(c->d.conv_out);
@@ -378,6 +404,8 @@ int create_ctx(const rkdg_mesh_desc* mesh, const rkdg_params* params, int32_t n_
             c->tiles.task = c->d.task;
             c->tiles.max_halo = tt.max_halo;
             c->tiles.ntiles = tt.ntiles;
+            if (params->limiter == RKDG_LIMITER_TVB)
+                c->d.tile_flags = (int*)dev_alloc(c, sizeof(int) * std::max(1, tt.ntiles));
             sync(c);  // host tables go out of scope
         }
         c->d.partial = (double*)dev_alloc(c, sizeof(double) * 4 * (totals_partial_count(T) + 1));
@@ -601,7 +629,7 @@ int rkdg_limit(rkdg_ctx* c) {
         RKDG_CUDA_TRY(cudaSetDevice(c->device));
         launch_tiled_limiter(c->tiles, 0, c->ld, c->d.U[c->cur], c->d.conn, c->d.lim, c->d.jinv,
                              nullptr, c->d.far, kprec(c), c->p.nq, c->p.gamma, c->p.tvb_m,
-                             nullptr, c->stream);
+                             nullptr, nullptr, c->stream);
         sync(c);
     });
 }
@@ -654,18 +682,9 @@ int rkdg_advance(rkdg_ctx* c, int32_t nsteps, double t_final, double* t, int32_t
         }
         if (!c->graph) {
             c->graph_monitor = (bool)c->reslog;
-            cudaGraph_t g;
-            RKDG_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-            try {
-                enqueue_step(c, c->graph_monitor);
-            } catch (...) {
-                cudaStreamEndCapture(c->stream, &g);
-                throw;
-            }
-            RKDG_CUDA_TRY(cudaStreamEndCapture(c->stream, &g));
-            RKDG_CUDA_TRY(cudaGraphInstantiate(&c->graph, g, 0));
-            cudaGraphDestroy(g);
+            c->graph = capture_steps(c, 1, c->graph_monitor);
         }
+        if (!c->graph_n && !c->reslog && nsteps >= kGraphSteps) c->graph_n = capture_steps(c, kGraphSteps, false);
         if (c->reslog) {  // the history needs every step's monitor: one step per launch
             for (int i = 0; i < nsteps; ++i) {
                 const int before = c->h_ctl->step;
@@ -682,7 +701,10 @@ int rkdg_advance(rkdg_ctx* c, int32_t nsteps, double t_final, double* t, int32_t
         const int chunk = t_final > 0 ? 64 : nsteps;
         while (left > 0) {
             int n = std::min(left, chunk > 0 ? chunk : 1);
-            for (int i = 0; i < n; ++i) RKDG_CUDA_TRY(cudaGraphLaunch(c->graph, c->stream));
+            for (int i = 0; i < n / kGraphSteps && c->graph_n; ++i)
+                RKDG_CUDA_TRY(cudaGraphLaunch(c->graph_n, c->stream));
+            for (int i = c->graph_n ? n / kGraphSteps * kGraphSteps : 0; i < n; ++i)
+                RKDG_CUDA_TRY(cudaGraphLaunch(c->graph, c->stream));
             left -= n;
             if (t_final > 0 && left > 0) {
                 pull_ctl(c);

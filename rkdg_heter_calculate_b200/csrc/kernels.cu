@@ -542,9 +542,50 @@ __device__ __forceinline__ double wave_of(const Real m[4], Real gamma, const Rea
 
 // ------------------------------------------------------------ the stage --
 // MODE_STAGE_COMP: the FP32 stage of RKDG_FP32C (cell means updated in FP64
-// from their high and low parts)
-enum { MODE_STAGE = 0, MODE_RESIDUAL = 1, MODE_STAGE_COMP = 2 };
+// from their high and low parts); MODE_LIMITED (added to a stage mode): the
+// stage is followed by the TVB limiter and writes its per-tile test
+// (tvb_keeps) for it.  Kernels without MODE_LIMITED carry none of that code.
+enum { MODE_STAGE = 0, MODE_RESIDUAL = 1, MODE_STAGE_COMP = 2, MODE_LIMITED = 4 };
 
+// Exact test that the TVB limiter (limit_element) leaves an element unchanged: every
+// row of its left eigenvector matrix has 1-norm at most B (|q|, |q_t| <=
+// |vx| + |vy|, |nx| + |ny| <= 1.5; 1.001 covers rounding), so when B times
+// the largest |P1 midpoint increment| (tilde) is within the smallest TVB
+// threshold, every characteristic increment is kept.  A non-physical mean
+// (NaN bound) fails the test.  The stage kernel applies it to each stage's
+// output per tile, so the limiter can skip whole tiles.
+template <typename Real>
+__device__ __forceinline__ bool tvb_keeps(const Real mean[4], Real gamma, Real tmax, Real thr_min) {
+    const Real rho = mean[0], ir = Real(1) / rho, vx = mean[1] * ir, vy = mean[2] * ir;
+    const Real p = (gamma - Real(1)) * (mean[3] - Real(0.5) * rho * (vx * vx + vy * vy));
+    const Real c = sqrt(gamma * p * ir);
+    const Real k2 = Real(0.5) * (vx * vx + vy * vy);
+    const Real b1 = (gamma - Real(1)) / (c * c), b2 = b1 * k2, ic = Real(1) / c;
+    const Real av = fabs(vx) + fabs(vy);
+    const Real B0 = Real(0.5) * (b2 + av * ic + b1 * av + Real(1.5) * ic + b1);
+    const Real B1 = fabs(Real(1) - b2) + b1 * av + b1;
+    const Real B2 = av + Real(1.5);
+    const Real B = fmax(fmax(B0, B1), B2) * Real(1.001);
+    return B * tmax <= thr_min;
+}
+// The TVB thresholds M (2 |m_k - b0|)^2 of an element's three edges (m_k
+// the edge midpoint, b0 the centroid): m_k - b0 = J d_k with the
+// reference-element offsets d_0 = (1/6, 1/6), d_1 = (-1/3, 1/6),
+// d_2 = (1/6, -1/3) and the columns of J, x_1 - x_0 = (c0x, c0y) and
+// x_2 - x_0 = (c1x, c1y); also the unit directions (m_k - b0)/|m_k - b0|.
+template <typename Real>
+__device__ __forceinline__ void tvb_geometry(Real c0x, Real c0y, Real c1x, Real c1y, Real tvb_m, Real dirx[3],
+                                             Real diry[3], Real thr[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const Real dxi = k == 1 ? Real(-1.0 / 3.0) : Real(1.0 / 6.0), deta = k == 2 ? Real(-1.0 / 3.0) : Real(1.0 / 6.0);
+        const Real dx = c0x * dxi + c1x * deta, dy = c0y * dxi + c1y * deta;
+        const Real r2 = dx * dx + dy * dy, irl = Real(1) / sqrt(r2);
+        dirx[k] = dx * irl;
+        diry[k] = dy * irl;
+        thr[k] = tvb_m * (Real(4) * r2);
+    }
+}
 #include "stage_tiled.cuh"
 
 // CFL measure of the current state per solve (first step, rkdg_compute_dt):
@@ -650,21 +691,17 @@ __device__ __forceinline__ void limit_element(int e, int ld, Real* __restrict__ 
     }
     Real nbm[3][4], tilde[3][4];
     const unsigned pair_bits = ((unsigned)cn.w >> 12) & 7u;
-    const double idet = 1.0 / (r0.x * r1.y - r0.y * r1.x);  // det J
+    // the directions and threshold scales in the working precision: FP64
+    // for the parity path, FP32 (from the FP64 J^-1 rows) for the FP32 forms
+    const Real idet = Real(1) / (Real)(r0.x * r1.y - r0.y * r1.x);  // det J
     // columns of J: x_1 - x_0 and x_2 - x_0
-    const double c0x = r1.y * idet, c0y = -r1.x * idet, c1x = -r0.y * idet, c1y = r0.x * idet;
     Real dirx[3], diry[3], thrk[3];
+    tvb_geometry<Real>((Real)r1.y * idet, -(Real)r1.x * idet, -(Real)r0.y * idet, (Real)r0.x * idet, (Real)tvb_m,
+                       dirx, diry, thrk);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 3; ++k)
 #pragma unroll
         for (int v = 0; v < 4; ++v) tilde[k][v] = tb.mphi[k][0] * u[1][v] + tb.mphi[k][1] * u[2][v];
-        const double dxi = k == 1 ? -1.0 / 3.0 : 1.0 / 6.0, deta = k == 2 ? -1.0 / 3.0 : 1.0 / 6.0;
-        const double dx = c0x * dxi + c1x * deta, dy = c0y * dxi + c1y * deta;
-        const double r2 = dx * dx + dy * dy, irl = 1.0 / sqrt(r2);
-        dirx[k] = (Real)(dx * irl);
-        diry[k] = (Real)(dy * irl);
-        thrk[k] = (Real)(tvb_m * (4.0 * r2));
-    }
     // the mean's primitive state and sound speed (the eigenvectors below)
     const Real rho = mean[0], ir = Real(1) / rho, vx = mean[1] * ir, vy = mean[2] * ir;
     const Real p = (gamma - Real(1)) * (mean[3] - Real(0.5) * rho * (vx * vx + vy * vy));
@@ -672,24 +709,14 @@ __device__ __forceinline__ void limit_element(int e, int ld, Real* __restrict__ 
     const Real k2 = Real(0.5) * (vx * vx + vy * vy);
     const Real b1 = (gamma - Real(1)) / (c * c), b2 = b1 * k2, ic = Real(1) / c;
     {
-        // Exact early exit: every row of the left eigenvector matrix below
-        // has 1-norm at most B (|q|, |q_t| <= |vx| + |vy|, |nx| + |ny| <= 1.5),
-        // so when B max |tilde| is within the smallest TVB threshold, every
-        // characteristic increment is kept and the element is not limited
-        // (uniform and near-uniform regions skip the neighbour means and the
-        // decompositions).  A non-physical mean (NaN bound) takes the full
-        // path.
-        const Real av = fabs(vx) + fabs(vy);
-        const Real B0 = Real(0.5) * (b2 + av * ic + b1 * av + Real(1.5) * ic + b1);
-        const Real B1 = fabs(Real(1) - b2) + b1 * av + b1;
-        const Real B2 = av + Real(1.5);
-        const Real B = fmax(fmax(B0, B1), B2) * Real(1.001);
+        // exact early exit (tvb_keeps): uniform and near-uniform regions skip
+        // the neighbour means and the decompositions
         Real tmax = Real(0);
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
             for (int v = 0; v < 4; ++v) tmax = fmax(tmax, fabs(tilde[k][v]));
-        if (B * tmax <= fmin(fmin(thrk[0], thrk[1]), thrk[2])) return;
+        if (tvb_keeps<Real>(mean, gamma, tmax, fmin(fmin(thrk[0], thrk[1]), thrk[2]))) return;
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -802,9 +829,13 @@ __global__ void __launch_bounds__(kAuxBlock) tiled_limiter_kernel(const TileArgs
                                                               const double* __restrict__ refs,
                                                               double gamma, double tvb_m,
                                                               int cfg1, int cfg2,
-                                                              const StepCtl* __restrict__ ctl) {
+                                                              const StepCtl* __restrict__ ctl,
+                                                              const int* __restrict__ tile_flags) {
     const int ntiles = ta.ntiles_dev ? *ta.ntiles_dev : ta.ntiles;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        // a tile the stage kernel found unchanged by the limiter (tvb_keeps
+        // for every element) is skipped
+        if (tile_flags && !tile_flags[tile]) continue;
         const int4 d0 = __ldg(ta.desc + 2 * tile);
         if ((flags && !flags[d0.z]) || (ctl && ctl[d0.z].done)) continue;
         const double* f = refs + 4 * d0.z;
@@ -1065,7 +1096,7 @@ void launch_tiled(const StageArgs& a, const TileArgs& t, int ctas, cudaStream_t 
 template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
 void launch_tiled_bt(const StageArgs& a, const TileArgs& t, int ctas, cudaStream_t s) {
     if (t.tile == 128) return launch_tiled<Real, NQ2, FLUX, MODE, ORD, 128>(a, t, ctas, s);
-    if constexpr (MODE != MODE_RESIDUAL)
+    if constexpr (MODE != MODE_RESIDUAL && !(MODE & MODE_LIMITED))
         if (t.tile == 256) return launch_tiled<Real, NQ2, FLUX, MODE, ORD, 256>(a, t, ctas, s);
     throw Error{RKDG_ERR_INVALID, "no stage kernel for a tile of " + std::to_string(t.tile) + " elements"};
 }
@@ -1087,7 +1118,7 @@ void dispatch(const StageArgs& a, const TileArgs& t, int order, int nq, int flux
     if (prec == RKDG_FP32) {
         if (hllc) dispatch_tiled<float, RKDG_FLUX_HLLC, MODE>(a, t, order, nq, ctas, s);
         else dispatch_tiled<float, RKDG_FLUX_LLF, MODE>(a, t, order, nq, ctas, s);
-    } else if constexpr (MODE != MODE_STAGE_COMP) {
+    } else if constexpr (!(MODE & MODE_STAGE_COMP)) {
         if (hllc) dispatch_tiled<double, RKDG_FLUX_HLLC, MODE>(a, t, order, nq, ctas, s);
         else dispatch_tiled<double, RKDG_FLUX_LLF, MODE>(a, t, order, nq, ctas, s);
     } else {
@@ -1100,8 +1131,13 @@ void dispatch(const StageArgs& a, const TileArgs& t, int order, int nq, int flux
 
 void launch_stage(const StageArgs& a, const TileArgs& t, int order, int nq, int flux, int prec, int ctas,
                   cudaStream_t stream) {
-    if (a.lo_row >= 0) dispatch<MODE_STAGE_COMP>(a, t, order, nq, flux, prec, ctas, stream);
-    else dispatch<MODE_STAGE>(a, t, order, nq, flux, prec, ctas, stream);
+    if (a.tile_flags != nullptr) {
+        if (a.lo_row >= 0) dispatch<MODE_STAGE_COMP | MODE_LIMITED>(a, t, order, nq, flux, prec, ctas, stream);
+        else dispatch<MODE_STAGE | MODE_LIMITED>(a, t, order, nq, flux, prec, ctas, stream);
+    } else {
+        if (a.lo_row >= 0) dispatch<MODE_STAGE_COMP>(a, t, order, nq, flux, prec, ctas, stream);
+        else dispatch<MODE_STAGE>(a, t, order, nq, flux, prec, ctas, stream);
+    }
 }
 
 void launch_residual(const StageArgs& a, const TileArgs& t, int order, int nq, int flux, int prec, int ctas,
@@ -1186,13 +1222,13 @@ int tiled_max_ctas_per_sm(int prec, int order, int nq, int flux, int max_halo, i
 void launch_tiled_limiter(const TileArgs& t, int ctas, int ld, void* U, const int4* conn,
                           const void* lim, const double* jinv, const int* flags,
                           const double* refs, int prec, int nq2, double gamma, double tvb_m,
-                          const StepCtl* ctl, cudaStream_t stream) {
+                          const StepCtl* ctl, const int* tile_flags, cudaStream_t stream) {
     const int cfg1 = cfg_index(3, 2), cfg2 = cfg_index(nq2, 3);
     const int grid = ctas > 0 ? ctas : std::max(1, t.ntiles);
     if (prec == RKDG_FP32)
-        tiled_limiter_kernel<float><<<grid, kAuxBlock, 0, stream>>>(t, ld, static_cast<float*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl);
+        tiled_limiter_kernel<float><<<grid, kAuxBlock, 0, stream>>>(t, ld, static_cast<float*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl, tile_flags);
     else
-        tiled_limiter_kernel<double><<<grid, kAuxBlock, 0, stream>>>(t, ld, static_cast<double*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl);
+        tiled_limiter_kernel<double><<<grid, kAuxBlock, 0, stream>>>(t, ld, static_cast<double*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl, tile_flags);
     RKDG_CUDA_TRY(cudaGetLastError());
 }
 

@@ -165,6 +165,7 @@ struct DeviceArrays {
     double* jinv = nullptr;     // [2][ld][2]
     int4* conn = nullptr;       // [ld]
     void* lim = nullptr;        // [3][ld] (alpha, beta) of the limiter (when enabled)
+    int* tile_flags = nullptr;  // [ntiles] the stage kernel's per-tile limiter test (when enabled)
     int32_t* perm = nullptr;    // [T]
     double* conv_in = nullptr;  // [T][36]
     double* conv_out = nullptr; // [T][36]
@@ -206,6 +207,9 @@ struct StageArgs {
     int last_stage;      // compute wave max / error (and the monitor when asked) in the epilogue
     int monitor;         // last stage: also form the residual monitor max |d mean| (rho, rhoE)
     int lo_row;          // RKDG_FP32C: state row of the cell means' low parts (in U, U0, Unew), else -1
+    int* tile_flags;     // with the TVB limiter: per tile of the launch, 1 if the limiter may change an element
+    const int* limiter_on;  // per solve: the test is made only for solves with the limiter (null: all)
+    double tvb_m;        // the TVB constant of that test
 };
 
 // Arithmetic type of the kernels for a precision setting: RKDG_FP32C runs
@@ -249,12 +253,14 @@ bool tiled_fits(int prec, int order, int flux, int max_halo, int tile);
 // tiles of `tile` elements
 int tiled_max_ctas_per_sm(int prec, int order, int nq, int flux, int max_halo, int tile = kTile);
 // TVB limiter over tiles; flags[solve] (may be null: all on) enables it per
-// solve, solves whose control block (ctl may be null) says done are skipped;
-// ctas 0 = one CTA per tile
+// solve, solves whose control block (ctl may be null) says done are skipped,
+// and tiles whose tile_flags entry (may be null) is 0 -- the stage kernel
+// that wrote the state found the limiter would change none of their
+// elements -- are skipped; ctas 0 = one CTA per tile
 void launch_tiled_limiter(const TileArgs& t, int ctas, int ld, void* U, const int4* conn,
                           const void* lim, const double* jinv, const int* flags,
                           const double* refs, int prec, int nq2, double gamma, double tvb_m,
-                          const StepCtl* ctl, cudaStream_t stream);
+                          const StepCtl* ctl, const int* tile_flags, cudaStream_t stream);
 // Caller layout [4][nb][ldh] FP64 <-> HBM state packs.  lo_row >= 0: the
 // state is RKDG_FP32C and row lo_row holds the low part of each cell mean
 // (import splits the FP64 mean into high and low floats, export and the

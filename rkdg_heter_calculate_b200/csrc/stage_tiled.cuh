@@ -338,8 +338,10 @@ __device__ __forceinline__ TilePre<Real> tile_pre(const StageArgs& a, const Tile
     return t;
 }
 
+// Returns, when the stage is followed by the TVB limiter (a.tile_flags set),
+// whether the limiter may change this thread's element (tvb_keeps fails).
 template <typename Real, int NB, int NQ, int NG, int FLUX, int MODE, int BT>
-__device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& ta, const int4 d0,
+__device__ __forceinline__ bool tile_stage(const StageArgs& a, const TileArgs& ta, const int4 d0,
                                            const int4 d1, unsigned char* smem_raw, unsigned char* stg,
                                            const int nxt, const int ntiles, uint64_t* bar,
                                            const TilePre<Real>& pre, Real (*s_red)[3], const double* s_dt) {
@@ -702,7 +704,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
 #pragma unroll
             for (int v = 0; v < 4; ++v) R[i][v] *= sc;
         if (active) store_state<Real, NB>(Uout, a.ld, e, R);
-        return;
+        return false;
     }
     const double dtd = *s_dt;
     // a U^n + b (U + dt L) as U^n + b ((U - U^n) + dt L): a + b = 1 holds
@@ -711,7 +713,7 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
     const Real dt = (Real)(dtd * det), cb = (Real)a.b;
     Real u0m[4] = {Real(0), Real(0), Real(0), Real(0)};
     // RKDG_FP32C (comp): row 0 is updated in FP64 below, not here
-    constexpr bool comp = PK && MODE == MODE_STAGE_COMP;
+    constexpr bool comp = PK && (MODE & MODE_STAGE_COMP);
     {
         load_state<Real, NB>(U, a.ld, ee, u);  // stored values (L2 hit)
         if (a.U0 != nullptr) {
@@ -759,13 +761,13 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
         // accumulate over the stages.
         if (active) store_rows<Real, 1, NB>(Uout, a.ld, e, R);
         const size_t lr = (size_t)a.lo_row * a.ld;
-        const float4 h = __ldg(reinterpret_cast<const float4*>(a.U) + ee);
+        // the high parts: the stage input's and U^n's row 0 as loaded for
+        // the update above (U^n's is zero in a first stage)
+        const float4 h = make_float4(u[0][0], u[0][1], u[0][2], u[0][3]);
+        const float4 h0 = make_float4(u0m[0], u0m[1], u0m[2], u0m[3]);
         const float4 l = __ldg(reinterpret_cast<const float4*>(a.U) + lr + ee);
-        float4 h0 = make_float4(0.f, 0.f, 0.f, 0.f), l0 = h0;
-        if (a.U0 != nullptr) {
-            h0 = __ldg(reinterpret_cast<const float4*>(a.U0) + ee);
-            l0 = __ldg(reinterpret_cast<const float4*>(a.U0) + lr + ee);
-        }
+        float4 l0 = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (a.U0 != nullptr) l0 = __ldg(reinterpret_cast<const float4*>(a.U0) + lr + ee);
         const double dtdet = dtd * det;
         const float hv[4] = {h.x, h.y, h.z, h.w}, lv[4] = {l.x, l.y, l.z, l.w};
         const float h0v[4] = {h0.x, h0.y, h0.z, h0.w}, l0v[4] = {l0.x, l0.y, l0.z, l0.w};
@@ -821,6 +823,25 @@ __device__ __forceinline__ void tile_stage(const StageArgs& a, const TileArgs& t
             s_red[tid >> 5][2] = m1;
         }
     }
+    bool need = false;
+    if constexpr (MODE & MODE_LIMITED) {
+      if (active && (a.limiter_on == nullptr || a.limiter_on[sid])) {
+        // the limiter's exact test on the new state (its P1 part at the edge
+        // midpoints, the mean, the TVB thresholds from the rows of 2 area
+        // J^-1: the columns of J are (j11, -j10) and (-j01, j00))
+        Real mean[4], tmax = Real(0);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) mean[v] = R[0][v] + refv[v];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) tmax = fmax(tmax, fabs(tb.mphi[k][0] * R[1][v] + tb.mphi[k][1] * R[2][v]));
+        Real dirx[3], diry[3], thr[3];
+        tvb_geometry<Real>(j11, -j10, -j01, j00, (Real)a.tvb_m, dirx, diry, thr);
+        need = !tvb_keeps<Real>(mean, gamma, tmax, fmin(fmin(thr[0], thr[1]), thr[2]));
+      }
+    }
+    return need;
 }
 
 // The tile's maxima from s_red into its solve's control block (one thread,
@@ -889,15 +910,24 @@ __global__ void __launch_bounds__(BT, TiledOccupancy<Real, ORD, BT>::value)
         parity ^= 1u;
         if (done) {  // finished solve: pass the tile on
             if (threadIdx.x == 0 && nxt < ntiles) stage_copy<Real, BT>(a, __ldg(ta.desc + 2 * nxt), stg, &s_bar);
+            if ((MODE & MODE_LIMITED) && threadIdx.x == 0) a.tile_flags[tile] = 0;
             continue;
         }
+        bool need;
         if (ORD == 2 || (ORD == 3 && d0.w == 2))
-            tile_stage<Real, 6, NQ2, 3, FLUX, MODE, BT>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre, s_red,
-                                                       &s_dt);
+            need = tile_stage<Real, 6, NQ2, 3, FLUX, MODE, BT>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre,
+                                                              s_red, &s_dt);
         else
-            tile_stage<Real, 3, 3, 2, FLUX, MODE, BT>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre, s_red,
-                                                     &s_dt);
-        __syncthreads();  // shared memory is reused by the next tile
+            need = tile_stage<Real, 3, 3, 2, FLUX, MODE, BT>(a, ta, d0, d1, smem_raw, stg, nxt, ntiles, &s_bar, pre,
+                                                            s_red, &s_dt);
+        // shared memory is reused by the next tile (with the limiter the
+        // barrier also ORs its test over the tile)
+        if constexpr (MODE & MODE_LIMITED) {
+            const int any = __syncthreads_or(need);
+            if (threadIdx.x == 0) a.tile_flags[tile] = any;
+        } else {
+            __syncthreads();
+        }
         if (MODE != MODE_RESIDUAL && a.last_stage && threadIdx.x == 0)
             tile_maxima_atomic<Real, BT>(a, a.ctl + d0.z, s_red);
     }
