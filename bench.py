@@ -78,8 +78,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI run")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving sweep")
     ap.add_argument("--serve-requests", type=int, default=100, help="requests per arrival-rate point")
-    ap.add_argument("--serve-loads", default="0.5,0.7,0.8,0.9",
-                    help="arrival rates as fractions of the measured saturated request rate")
+    ap.add_argument("--serve-loads", default="0.8",
+                    help="arrival rates as fractions of the measured saturated request rate (the default run "
+                         "keeps one; --workload serving --serve-loads 0.5,0.7,0.8,0.9 sweeps)")
     return ap.parse_args()
 
 
@@ -749,6 +750,11 @@ def main():
         return
     dist.init()
     import torch  # noqa: F401
+
+    if dist.world > 1 and args.workload == "batched":
+        # a scaling run times the headline pack per rank (replicas); the
+        # single-GPU legs (plain, Mach-3 step, serving, CPU) run at N = 1
+        args.no_plain = args.no_step = args.no_serving = args.no_cpu = True
 
     peak, peak_kind = measured_peak()
     line = None
