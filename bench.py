@@ -146,18 +146,58 @@ class Dist:
 
 # ----------------------------------------------------------------- clocks --
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during a region."""
+    """SM clocks and clock-event (throttle) reasons sampled during a region:
+    NVML polled from a host thread every 2 ms (a timed region of a few tens
+    of milliseconds still gets samples), the device found by its PCI bus id
+    so that a remapped CUDA_VISIBLE_DEVICES still names the right GPU;
+    nvidia-smi at 200 ms where the NVML binding is absent.  Read-only."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
+        self.nvml = None
         self.out = []
+        self.samples = []  # (sm MHz, max sm MHz, reason bits) from NVML
+        self.stop = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:
+            pr = torch.cuda.get_device_properties(self.gpu)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+
+    def _poll(self):
+        nv, h = self.nvml
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while True:
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), mx,
+                                     nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+            except Exception:
+                pass
+            if self.stop.wait(0.002):
+                break
 
     def __enter__(self):
+        try:
+            self.nvml = self._nvml_handle()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
@@ -174,6 +214,13 @@ class ClockSampler:
             self.out.append(line.strip())
 
     def __exit__(self, *exc):
+        if self.nvml:
+            self.stop.set()
+            self.thread.join(timeout=5)
+            try:
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -183,6 +230,10 @@ class ClockSampler:
 
     def summary(self):
         sm, mx, reasons = [], None, set()
+        for clk, m, bits in self.samples:
+            sm.append(float(clk))
+            mx = float(m)
+            reasons.update(n for n, b in self.REASONS if bits & b)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.out:
             f = [x.strip() for x in line.split(",")]
@@ -199,7 +250,7 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvml, 2 ms" if self.samples else "nvidia-smi, 200 ms"}
 
 
 # ------------------------------------------------------------ workloads --
@@ -656,6 +707,9 @@ def run_serving(args, dist):
                         f"50/50, triangles log-uniform in [2k, 500k] snapped to {SERVE_LEVELS} mesh sizes "
                         "per kind, vortex P1/P2 50/50 with HLLC, step P1 with LLF and TVB (M=50), final time "
                         "U[0.1, 1.0]; FP32, SSP-RK3, CFL 0.2; 8 GiB pool, 64 slots",
+            "step_flux": "LLF: with Davis wave-speed bounds the HLLC flux goes non-physical at the step corner "
+                         "under P1 + TVB, in FP64 and FP32 alike, so step requests run the limited-flow "
+                         "configuration's LLF",
             "requests_per_point": n, "saturated_req_per_s": round(cap_rate, 3),
             "latency": "completion - arrival, host preprocessing and result read-back included",
             "loop_time": "fractions of each point's wall time the serving loop spent uploading admitted "
