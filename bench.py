@@ -5,27 +5,36 @@ Headline workload (default, --workload batched): 64 independent isentropic-
 vortex solves, vortex strength U[1,5] and free-stream angle U[0, 2 pi)
 (free-stream speed sqrt(2)), seeded (numpy default_rng(4)); periodic
 Delaunay meshes of jittered lattices with triangle counts log-uniform in
-[5k, 200k]; P1 and P2 (Bernoulli 1/2); FP32 state with FP64 geometry and dt;
-HLLC, SSP-RK3, CFL 0.2; 200 steps each; one launch per RK stage over all
-solves, CUDA graph, autotuned launch shape.  Synthetic data, no dataset.
+[5k, 200k]; P1 and P2 (Bernoulli 1/2); FP32 arithmetic with FP64 geometry and
+dt, the state in the FP32C form (cell means as high + low float pairs updated
+in FP64; --headline fp32 times the plain FP32 form instead); HLLC, SSP-RK3,
+CFL 0.2; one launch per RK stage over all solves, CUDA graph, autotuned launch
+shape.  Synthetic data, no dataset.
 
 Beside it, the plain FP64 single solve on the unstructured vortex (periodic
 Delaunay of a 700 x 700 lattice jittered by +-0.3h, seed 2, 980,000
 triangles, P2, 6/3-point rules, HLLC, SSP-RK3) and its FP32 form.
 
 One JSON line on rank 0:
-  value        batched FP32 DOF-stage updates/s, state resident in HBM, K steps
-               timed with CUDA events on the batch's stream, max over ranks;
+  value        batched FP32C DOF-stage updates/s, state resident in HBM, K steps
+               timed with CUDA events on the batch's stream, max over ranks
+               (batched_forms: the FP32, FP32C and FP64 forms);
   plain_fp64   single-solve FP64 DOF-stage/s on the 980k mesh (and its FP32 form);
   roofline     achieved HBM GB/s of the fused stage kernel over all solves:
-               algorithmic bytes per element-stage 4 Nb w (2 + r_s) + 56
-               (r_s = 2/3 mean over SSP-RK3) over the event-timed launch;
+               algorithmic bytes per element-stage 16 rows (2 + r_s) + 56
+               (16-byte rows per element: 2 Nb in FP64, Nb in FP32, Nb + 1 in
+               FP32C; r_s = 2/3 mean over SSP-RK3) over the event-timed launch;
   e2e          the batched metric through the C ABI with host buffers: every
                solve's set_state + K steps + get_state;
   cpu_baseline the reference's own code (oracle/_ref, compiled from its
                sources for the host) on a bounded sample, all host threads;
-  l2           vortex L2(rho) error vs the exact solution: batched FP32 vs FP64
-               per solve after 200 steps, and the 980k solve at t = 2.
+  l2           vortex L2(rho) error vs the exact solution: batched FP32 and FP32C
+               vs FP64 per solve after 200 steps, and the 980k solve at t = 2;
+  step_fp32_vs_fp64  the Mach-3 step (P1, LLF, TVB) in each form: rate, roofline,
+               and the cell-mean density's distance from FP64, with the FP64
+               control run from a perturbed state;
+  serving      the request server under Poisson arrivals: p50/p90/p99 latency,
+               DOF-stage/s, the loop's time split.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 """
