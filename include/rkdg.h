@@ -307,9 +307,12 @@ int rkdg_batch_set_time(rkdg_batch* b, int32_t solve, double t);
 /* Picks the tile size (128 or 256 elements, one thread per element), the
  * persistent grid size and the tile order by timing candidate launch shapes
  * on this batch's live state; returns the chosen CTA count (0: one per
- * tile), tile order (0 solve order, 1 P2 tiles first) and tile size (any
- * pointer may be NULL).  The reference fixes its block size from its
- * configuration file (threadsperblock, src/cudarkdgsolver.cu:22). */
+ * tile), tile order (0 solve order, 1 P2 tiles first, 2 P2 tiles first and
+ * the P2 and P1 tiles of a mixed pack as two concurrent launches of the
+ * single-order kernels) and tile size (any pointer may be NULL).  Every
+ * shape gives the same bits for a given tile size.  The reference fixes its
+ * block size from its configuration file (threadsperblock,
+ * src/cudarkdgsolver.cu:22). */
 int rkdg_batch_autotune(rkdg_batch* b, int32_t* ctas, int32_t* tile_order, int32_t* tile);
 int rkdg_batch_set_shape(rkdg_batch* b, int32_t ctas, int32_t tile_order);
 /* Rebuilds the tile tables for tiles of 128 or 256 elements.  A solve's

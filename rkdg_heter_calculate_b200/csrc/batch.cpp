@@ -39,8 +39,14 @@ struct rkdg_batch {
     StepCtl* ctl = nullptr;
     StepCtl* h_ctl = nullptr;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;    // tile order 2: the P1 tiles' launches, forked and joined
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    int n2tiles = 0;                   // P2 tiles (the first ones in tile orders 1 and 2)
     cudaGraphExec_t graph = nullptr;   // one step
     cudaGraphExec_t graph_n = nullptr; // kGraphSteps steps (fewer graph launches and boundaries)
+    // tile order: 0 = solve order, 1 = P2 tiles first, 2 = P2 tiles first
+    // and the P2 and P1 tiles as two launches of the single-order kernels on
+    // forked streams (mixed packs)
     int ctas = 0, tile_order = 0, tile = kTile;
     std::vector<HostMesh> topo;  // per solve (internal order): T, neighbours, shared edges, tags
     size_t table_bytes = 0;      // device bytes of the tile tables (rebuilt with the tile size)
@@ -108,10 +114,12 @@ void upload_desc(rkdg_batch* b) {
     std::vector<int32_t> d(b->desc_solve.size());
     std::vector<int> idx(b->ntiles);
     std::iota(idx.begin(), idx.end(), 0);
-    if (b->tile_order == 1)  // P2 tiles first: the expensive tiles start early
+    if (b->tile_order != 0)  // P2 tiles first: the expensive tiles start early
         std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
             return b->desc_solve[8 * x + 3] > b->desc_solve[8 * y + 3];
         });
+    b->n2tiles = 0;
+    for (int i = 0; i < b->ntiles; ++i) b->n2tiles += b->desc_solve[8 * i + 3] == 2;
     for (int i = 0; i < b->ntiles; ++i)
         std::memcpy(&d[8 * i], &b->desc_solve[8 * idx[i]], 8 * sizeof(int32_t));
     h2d(b, reinterpret_cast<int32_t*>(b->tdesc), d);
@@ -138,6 +146,28 @@ void coeffs(int rk, int s, double& a, double& c) {
     else a = 1.0 / 3.0, c = 2.0 / 3.0;
 }
 
+// One stage over every tile of the pack: one launch of the kernel for the
+// pack's orders, or in tile order 2 (a mixed pack) the P2 tiles with the
+// P2 kernel on the batch's stream and the P1 tiles with the P1 kernel (more
+// resident CTAs per SM) on a second stream forked from it and joined after
+// them.  A tile's arithmetic is the same in every kernel that runs it.
+void launch_pack_stage(rkdg_batch* b, const StageArgs& a) {
+    if (b->tile_order != 2 || b->ord != 3) {
+        launch_stage(a, b->tiles, b->ord, b->p.nq, b->p.flux, kprec(b), b->ctas, b->stream);
+        return;
+    }
+    TileArgs t2 = b->tiles, t1 = b->tiles;
+    t2.ntiles = b->n2tiles;
+    t1.desc = b->tdesc + 2 * (size_t)b->n2tiles;
+    t1.ntiles = b->ntiles - b->n2tiles;
+    RKDG_CUDA_TRY(cudaEventRecord(b->ev_fork, b->stream));
+    RKDG_CUDA_TRY(cudaStreamWaitEvent(b->stream2, b->ev_fork, 0));
+    if (t2.ntiles > 0) launch_stage(a, t2, 2, b->p.nq, b->p.flux, kprec(b), b->ctas, b->stream);
+    if (t1.ntiles > 0) launch_stage(a, t1, 1, b->p.nq, b->p.flux, kprec(b), b->ctas, b->stream2);
+    RKDG_CUDA_TRY(cudaEventRecord(b->ev_join, b->stream2));
+    RKDG_CUDA_TRY(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
+}
+
 void enqueue_stage(rkdg_batch* b, int s, int in, int u0, int out, bool last) {
     StageArgs a = stage_args(b);
     coeffs(b->p.rk, s, a.a, a.b);
@@ -145,7 +175,7 @@ void enqueue_stage(rkdg_batch* b, int s, int in, int u0, int out, bool last) {
     a.U0 = s == 0 ? nullptr : b->U[u0];
     a.Unew = b->U[out];
     a.last_stage = last ? 1 : 0;
-    launch_stage(a, b->tiles, b->ord, b->p.nq, b->p.flux, kprec(b), b->ctas, b->stream);
+    launch_pack_stage(b, a);
 }
 
 void enqueue_step(rkdg_batch* b) {
@@ -243,6 +273,9 @@ void destroy_batch(rkdg_batch* b) {
                     (void*)b->perm, (void*)b->far, (void*)b->staging, (void*)b->ctl})
         cudaFree(p);
     if (b->h_ctl) cudaFreeHost(b->h_ctl);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    if (b->stream2) cudaStreamDestroy(b->stream2);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -296,6 +329,9 @@ int rkdg_batch_create(int32_t nsolves, const rkdg_mesh_desc* meshes, const int32
         b->order.assign(orders, orders + nsolves);
         b->have_state.assign(nsolves, false);
         RKDG_CUDA_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        RKDG_CUDA_TRY(cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking));
+        RKDG_CUDA_TRY(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+        RKDG_CUDA_TRY(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
         RKDG_CUDA_TRY(cudaMallocHost(&b->h_ctl, sizeof(StepCtl) * nsolves));
         std::memset(b->h_ctl, 0, sizeof(StepCtl) * nsolves);
         if (has2) upload_tables(p.nq, 3);
@@ -476,10 +512,9 @@ int rkdg_batch_time_stage(rkdg_batch* b, int32_t s, int32_t reps, double* ms) {
         cudaEvent_t e0, e1;
         RKDG_CUDA_TRY(cudaEventCreate(&e0));
         RKDG_CUDA_TRY(cudaEventCreate(&e1));
-        launch_stage(a, b->tiles, b->ord, b->p.nq, b->p.flux, kprec(b), b->ctas, b->stream);
+        launch_pack_stage(b, a);
         RKDG_CUDA_TRY(cudaEventRecord(e0, b->stream));
-        for (int i = 0; i < reps; ++i)
-            launch_stage(a, b->tiles, b->ord, b->p.nq, b->p.flux, kprec(b), b->ctas, b->stream);
+        for (int i = 0; i < reps; ++i) launch_pack_stage(b, a);
         RKDG_CUDA_TRY(cudaEventRecord(e1, b->stream));
         RKDG_CUDA_TRY(cudaEventSynchronize(e1));
         float tms = 0;
@@ -492,7 +527,7 @@ int rkdg_batch_time_stage(rkdg_batch* b, int32_t s, int32_t reps, double* ms) {
 
 int rkdg_batch_set_shape(rkdg_batch* b, int32_t ctas, int32_t tile_order) {
     return guarded([&] {
-        if (!b || ctas < 0 || (tile_order != 0 && tile_order != 1))
+        if (!b || ctas < 0 || tile_order < 0 || tile_order > 2)
             throw Error{RKDG_ERR_INVALID, "rkdg_batch_set_shape: bad arguments"};
         RKDG_CUDA_TRY(cudaSetDevice(b->device));
         if (tile_order != b->tile_order) {
@@ -545,7 +580,10 @@ int rkdg_batch_autotune(rkdg_batch* b, int32_t* ctas_out, int32_t* order_out, in
                                                                   b->tiles.max_halo, tile));
             const int wave = prop.multiProcessorCount * per_sm;
             std::vector<int> cand_order = {0};
-            if (b->ord == 3) cand_order.push_back(1);
+            if (b->ord == 3) {
+                cand_order.push_back(1);
+                cand_order.push_back(2);
+            }
             for (int o : cand_order)
                 for (int c : {0, wave, 2 * wave, 4 * wave}) {
                     if (c > 0 && c >= b->ntiles) continue;

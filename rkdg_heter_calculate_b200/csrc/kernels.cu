@@ -814,9 +814,13 @@ __device__ __forceinline__ void limit_element(int e, int ld, Real* __restrict__ 
     store_state<Real, NB>(U, ld, e, out);
 }
 
-// The limiter over tiles (one solve, a pack of solves or the serving pool):
-// tiles of solves whose flag is 0 (when flags is set) or whose control
-// block says done are skipped; P1 and P2 tiles limit their P1 part (P2
+constexpr int kLimGroup = 8;  // tiles per limiter CTA pass
+
+// The limiter over tiles (one solve, a pack of solves or the serving pool),
+// kLimGroup tiles per CTA pass (a pass whose tiles the stage kernel found
+// unchangeable ends after one load of their flags): tiles of solves whose
+// flag is 0 (when flags is set) or whose control block says done are
+// skipped; P1 and P2 tiles limit their P1 part (P2
 // tiles drop their quadratic modes where limited).  Every path runs this one
 // kernel, so a solve limits to the same bits wherever it runs.
 template <typename Real>
@@ -832,20 +836,35 @@ __global__ void __launch_bounds__(kAuxBlock) tiled_limiter_kernel(const TileArgs
                                                               const StepCtl* __restrict__ ctl,
                                                               const int* __restrict__ tile_flags) {
     const int ntiles = ta.ntiles_dev ? *ta.ntiles_dev : ta.ntiles;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        // a tile the stage kernel found unchanged by the limiter (tvb_keeps
-        // for every element) is skipped
-        if (tile_flags && !tile_flags[tile]) continue;
-        const int4 d0 = __ldg(ta.desc + 2 * tile);
-        if ((flags && !flags[d0.z]) || (ctl && ctl[d0.z].done)) continue;
-        const double* f = refs + 4 * d0.z;
-        for (int x = threadIdx.x; x < d0.y; x += blockDim.x) {
-            const int e = d0.x + x;
-            if (d0.w == 2)
-                limit_element<Real, 6>(e, ld, U, conn, lim, jinv, gamma, f[0], f[1], f[2], f[3], tvb_m, tab<Real>(cfg2));
-            else
-                limit_element<Real, 3>(e, ld, U, conn, lim, jinv, gamma, f[0], f[1], f[2], f[3], tvb_m, tab<Real>(cfg1));
+    const int ngroups = (ntiles + kLimGroup - 1) / kLimGroup;
+    __shared__ int s_tiles[kLimGroup];
+    __shared__ int s_n;
+    for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        // the first warp reads the group's tile flags in one load and lists,
+        // in tile order, the tiles the stage kernel found changeable by the
+        // limiter (tvb_keeps failed for an element); the others are skipped
+        if (threadIdx.x < 32) {
+            const int t = g * kLimGroup + (int)threadIdx.x;
+            const bool take = threadIdx.x < kLimGroup && t < ntiles && (tile_flags == nullptr || tile_flags[t]);
+            const unsigned m = __ballot_sync(0xffffffffu, take);
+            if (take) s_tiles[__popc(m & ((1u << threadIdx.x) - 1u))] = t;
+            if (threadIdx.x == 0) s_n = __popc(m);
         }
+        __syncthreads();
+        const int n = s_n;
+        for (int k = 0; k < n; ++k) {
+            const int4 d0 = __ldg(ta.desc + 2 * s_tiles[k]);
+            if ((flags && !flags[d0.z]) || (ctl && ctl[d0.z].done)) continue;
+            const double* f = refs + 4 * d0.z;
+            for (int x = threadIdx.x; x < d0.y; x += blockDim.x) {
+                const int e = d0.x + x;
+                if (d0.w == 2)
+                    limit_element<Real, 6>(e, ld, U, conn, lim, jinv, gamma, f[0], f[1], f[2], f[3], tvb_m, tab<Real>(cfg2));
+                else
+                    limit_element<Real, 3>(e, ld, U, conn, lim, jinv, gamma, f[0], f[1], f[2], f[3], tvb_m, tab<Real>(cfg1));
+            }
+        }
+        __syncthreads();  // s_tiles and s_n are rewritten by the next group
     }
 }
 
@@ -1224,7 +1243,7 @@ void launch_tiled_limiter(const TileArgs& t, int ctas, int ld, void* U, const in
                           const double* refs, int prec, int nq2, double gamma, double tvb_m,
                           const StepCtl* ctl, const int* tile_flags, cudaStream_t stream) {
     const int cfg1 = cfg_index(3, 2), cfg2 = cfg_index(nq2, 3);
-    const int grid = ctas > 0 ? ctas : std::max(1, t.ntiles);
+    const int grid = ctas > 0 ? ctas : std::max(1, (t.ntiles + kLimGroup - 1) / kLimGroup);
     if (prec == RKDG_FP32)
         tiled_limiter_kernel<float><<<grid, kAuxBlock, 0, stream>>>(t, ld, static_cast<float*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl, tile_flags);
     else

@@ -189,12 +189,15 @@ struct TiledSmem {
     __host__ __device__ static constexpr size_t bytes(int hm) { return stage_offset(hm) + stage_rows(hm) * 16; }
 };
 
-// Resident CTAs per SM the register allocation is held to: 24 warps per SM
-// in FP32 (80 registers; 128-element tiles at most 37 KB of shared memory
-// per CTA), 8 (P2, 12 for P1) in FP64, whatever the tile size.
+// Resident CTAs per SM the register allocation is held to: in FP32 24 warps
+// per SM for kernels with P2 tiles (80 registers; 128-element tiles at most
+// 37 KB of shared memory per CTA) and 32 for P1-only kernels (64 registers;
+// their tiles need about 27 KB, and the extra warps hide more of the tile
+// pipeline's latency: 11 % faster on the limited Mach-3 step); in FP64 8
+// (P2) and 12 (P1); whatever the tile size.
 template <typename Real, int ORD, int BT>
 struct TiledOccupancy {
-    static constexpr int warps = sizeof(Real) == 8 ? (ORD == 1 ? 12 : 8) : 24;
+    static constexpr int warps = sizeof(Real) == 8 ? (ORD == 1 ? 12 : 8) : (ORD == 1 ? 32 : 24);
     static constexpr int value = warps * 32 / BT > 0 ? warps * 32 / BT : 1;
 };
 

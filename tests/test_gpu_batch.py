@@ -41,11 +41,16 @@ def solo(m, order, U, far, precision, steps, t_final=0.0):
     return out, t, n
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp32c", "fp64"])
-def test_batch_equals_solo_runs(precision):
+@pytest.mark.parametrize("precision,shape", [("fp32", (0, 0)), ("fp32c", (0, 0)), ("fp64", (0, 0)),
+                                             ("fp32", (0, 2)), ("fp32c", (3, 2)), ("fp64", (0, 2))])
+def test_batch_equals_solo_runs(precision, shape):
+    """Every launch shape: one launch per stage in solve order (0, 0), and
+    the P2 and P1 tiles as two concurrent launches of the single-order
+    kernels, one CTA per tile (0, 2) or three persistent CTAs each (3, 2)."""
     cs = cases()
     b = Batch([c[0] for c in cs], [c[1] for c in cs], precision=precision, flux="hllc", cfl=0.2,
               farfields=[c[3] for c in cs])
+    b.set_shape(*shape)
     for i, c in enumerate(cs):
         b.set_state(i, c[2])
     t, n = b.advance(12)
@@ -64,7 +69,7 @@ def test_batch_final_times_and_autotune():
     for i, c in enumerate(cs):
         b.set_state(i, c[2])
     ctas, order, tile = b.autotune()
-    assert ctas >= 0 and order in (0, 1) and tile in (128, 256)
+    assert ctas >= 0 and order in (0, 1, 2) and tile in (128, 256)
     # a solve alone runs 128-element tiles: bit-for-bit equality holds at the same tile size
     b.set_tile(128)
     tf = np.array([0.05, 0.11, 0.02, 0.3])
