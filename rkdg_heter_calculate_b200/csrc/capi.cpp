@@ -191,12 +191,16 @@ void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out, bool monitor 
     // a partition applies its limiter by rkdg_limit once the halo means of
     // the stage output have been exchanged
     const bool limit = c->p.limiter == RKDG_LIMITER_TVB && c->T_own == c->T;
-    a.tile_flags = limit ? c->d.tile_flags : nullptr;  // the stage's per-tile limiter test
+    // the stage lists the tiles its limiter test finds changeable; the
+    // limiter visits those
+    a.tile_flags = limit ? c->d.tile_flags : nullptr;
+    a.tile_list = limit ? c->d.tile_list : nullptr;
+    a.tile_cap = c->tiles.ntiles;
     launch_stage(a, c->tiles, c->p.order, c->p.nq, c->p.flux, kprec(c), c->ctas, c->stream);
     if (limit)
         launch_tiled_limiter(c->tiles, 0, c->ld, c->d.U[out], c->d.conn, c->d.lim, c->d.jinv, nullptr,
                              c->d.far, kprec(c), c->p.nq, c->p.gamma, c->p.tvb_m, c->d.ctl, c->d.tile_flags,
-                             c->stream);
+                             c->d.tile_list, c->tiles.ntiles, c->stream);
 }
 
 // one full step on the stream with the state in buffer 0 (graph-capturable);
@@ -260,6 +264,7 @@ void destroy_ctx(rkdg_ctx* c) {
     cudaFree(c->d.conn);
     cudaFree(c->d.lim);
     cudaFree(c->d.tile_flags);
+    cudaFree(c->d.tile_list);
     cudaFree(c->d.perm);
     cudaFree(c->d.conv_in);
     cudaFree(c->d.conv_out);
@@ -404,8 +409,13 @@ int create_ctx(const rkdg_mesh_desc* mesh, const rkdg_params* params, int32_t n_
             c->tiles.task = c->d.task;
             c->tiles.max_halo = tt.max_halo;
             c->tiles.ntiles = tt.ntiles;
-            if (params->limiter == RKDG_LIMITER_TVB)
-                c->d.tile_flags = (int*)dev_alloc(c, sizeof(int) * std::max(1, tt.ntiles));
+            if (params->limiter == RKDG_LIMITER_TVB) {  // flags 0 and the list empty between stages
+                const size_t nf = sizeof(int) * std::max(1, tt.ntiles), nl = sizeof(int) * (kListHead + tt.ntiles);
+                c->d.tile_flags = (int*)dev_alloc(c, nf);
+                c->d.tile_list = (int*)dev_alloc(c, nl);
+                RKDG_CUDA_TRY(cudaMemsetAsync(c->d.tile_flags, 0, nf, c->stream));
+                RKDG_CUDA_TRY(cudaMemsetAsync(c->d.tile_list, 0, nl, c->stream));
+            }
             sync(c);  // host tables go out of scope
         }
         c->d.partial = (double*)dev_alloc(c, sizeof(double) * 4 * (totals_partial_count(T) + 1));
@@ -629,7 +639,7 @@ int rkdg_limit(rkdg_ctx* c) {
         RKDG_CUDA_TRY(cudaSetDevice(c->device));
         launch_tiled_limiter(c->tiles, 0, c->ld, c->d.U[c->cur], c->d.conn, c->d.lim, c->d.jinv,
                              nullptr, c->d.far, kprec(c), c->p.nq, c->p.gamma, c->p.tvb_m,
-                             nullptr, nullptr, c->stream);
+                             nullptr, nullptr, nullptr, 0, c->stream);
         sync(c);
     });
 }

@@ -814,15 +814,34 @@ __device__ __forceinline__ void limit_element(int e, int ld, Real* __restrict__ 
     store_state<Real, NB>(U, ld, e, out);
 }
 
-constexpr int kLimGroup = 8;  // tiles per limiter CTA pass
-
-// The limiter over tiles (one solve, a pack of solves or the serving pool),
-// kLimGroup tiles per CTA pass (a pass whose tiles the stage kernel found
-// unchangeable ends after one load of their flags): tiles of solves whose
+// One tile of the limiter (all threads of the CTA): tiles of solves whose
 // flag is 0 (when flags is set) or whose control block says done are
-// skipped; P1 and P2 tiles limit their P1 part (P2
-// tiles drop their quadratic modes where limited).  Every path runs this one
-// kernel, so a solve limits to the same bits wherever it runs.
+// skipped; P1 and P2 tiles limit their P1 part (P2 tiles drop their
+// quadratic modes where limited).
+template <typename Real>
+__device__ __forceinline__ void limit_tile(const TileArgs& ta, int tile, int ld, Real* __restrict__ U,
+                                           const int4* __restrict__ conn, const void* __restrict__ lim,
+                                           const double* __restrict__ jinv, const int* __restrict__ flags,
+                                           const double* __restrict__ refs, double gamma, double tvb_m, int cfg1,
+                                           int cfg2, const StepCtl* __restrict__ ctl) {
+    const int4 d0 = __ldg(ta.desc + 2 * tile);
+    if ((flags && !flags[d0.z]) || (ctl && ctl[d0.z].done)) return;
+    const double* f = refs + 4 * d0.z;
+    for (int x = threadIdx.x; x < d0.y; x += blockDim.x) {
+        const int e = d0.x + x;
+        if (d0.w == 2)
+            limit_element<Real, 6>(e, ld, U, conn, lim, jinv, gamma, f[0], f[1], f[2], f[3], tvb_m, tab<Real>(cfg2));
+        else
+            limit_element<Real, 3>(e, ld, U, conn, lim, jinv, gamma, f[0], f[1], f[2], f[3], tvb_m, tab<Real>(cfg1));
+    }
+}
+
+// The limiter over tiles (one solve, a pack of solves or the serving pool).
+// Every path runs this one kernel, so a solve limits to the same bits
+// wherever it runs.  Without a tile list every tile is visited; with one
+// (the stage kernel's LimitList), only the listed tiles, spread over the
+// CTAs of a persistent grid: most of a flow's tiles cannot change (no
+// element fails tvb_keeps) and cost nothing.
 template <typename Real>
 __global__ void __launch_bounds__(kAuxBlock) tiled_limiter_kernel(const TileArgs ta, int ld,
                                                               Real* __restrict__ U,
@@ -834,37 +853,29 @@ __global__ void __launch_bounds__(kAuxBlock) tiled_limiter_kernel(const TileArgs
                                                               double gamma, double tvb_m,
                                                               int cfg1, int cfg2,
                                                               const StepCtl* __restrict__ ctl,
-                                                              const int* __restrict__ tile_flags) {
-    const int ntiles = ta.ntiles_dev ? *ta.ntiles_dev : ta.ntiles;
-    const int ngroups = (ntiles + kLimGroup - 1) / kLimGroup;
-    __shared__ int s_tiles[kLimGroup];
-    __shared__ int s_n;
-    for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
-        // the first warp reads the group's tile flags in one load and lists,
-        // in tile order, the tiles the stage kernel found changeable by the
-        // limiter (tvb_keeps failed for an element); the others are skipped
-        if (threadIdx.x < 32) {
-            const int t = g * kLimGroup + (int)threadIdx.x;
-            const bool take = threadIdx.x < kLimGroup && t < ntiles && (tile_flags == nullptr || tile_flags[t]);
-            const unsigned m = __ballot_sync(0xffffffffu, take);
-            if (take) s_tiles[__popc(m & ((1u << threadIdx.x) - 1u))] = t;
-            if (threadIdx.x == 0) s_n = __popc(m);
+                                                              int* __restrict__ tile_flags,
+                                                              int* __restrict__ tile_list, int tile_cap) {
+    if (tile_list == nullptr) {
+        const int ntiles = ta.ntiles_dev ? *ta.ntiles_dev : ta.ntiles;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+            limit_tile<Real>(ta, tile, ld, U, conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl);
+        return;
+    }
+    // every CTA reads the count before the last one resets it (the reset
+    // follows every CTA's arrival below)
+    const int n = min(*(volatile int*)tile_list, tile_cap);
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const int tile = tile_list[kListHead + i];
+        limit_tile<Real>(ta, tile, ld, U, conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl);
+        if (threadIdx.x == 0) tile_flags[tile] = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(tile_list + 1, 1) == (int)gridDim.x - 1) {  // the last CTA: empty list for the next stage
+            tile_list[0] = 0;
+            tile_list[1] = 0;
         }
-        __syncthreads();
-        const int n = s_n;
-        for (int k = 0; k < n; ++k) {
-            const int4 d0 = __ldg(ta.desc + 2 * s_tiles[k]);
-            if ((flags && !flags[d0.z]) || (ctl && ctl[d0.z].done)) continue;
-            const double* f = refs + 4 * d0.z;
-            for (int x = threadIdx.x; x < d0.y; x += blockDim.x) {
-                const int e = d0.x + x;
-                if (d0.w == 2)
-                    limit_element<Real, 6>(e, ld, U, conn, lim, jinv, gamma, f[0], f[1], f[2], f[3], tvb_m, tab<Real>(cfg2));
-                else
-                    limit_element<Real, 3>(e, ld, U, conn, lim, jinv, gamma, f[0], f[1], f[2], f[3], tvb_m, tab<Real>(cfg1));
-            }
-        }
-        __syncthreads();  // s_tiles and s_n are rewritten by the next group
     }
 }
 
@@ -1056,8 +1067,6 @@ __global__ void __launch_bounds__(kTotBlock) totals_final_kernel(int n, const do
 // ----------------------------------------------------------- launchers --
 namespace {
 
-// Shared-memory attributes of one instantiation for a halo size; returns the
-// dynamic shared memory per CTA.
 // The device's largest opt-in dynamic + static shared memory per CTA, less
 // the stage kernel's static shared memory (barrier, maxima, dt, tables).
 size_t smem_limit() {
@@ -1070,6 +1079,24 @@ size_t smem_limit() {
     }
     return (size_t)limit - 1024;
 }
+
+}  // namespace
+
+int sm_count() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0, v = 0;
+        RKDG_CUDA_TRY(cudaGetDevice(&dev));
+        RKDG_CUDA_TRY(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+        n = v;
+    }
+    return n;
+}
+
+namespace {
+
+// Shared-memory attributes of one instantiation for a halo size; returns the
+// dynamic shared memory per CTA.
 
 template <typename Real, int NQ2, int FLUX, int MODE, int ORD, int BT>
 size_t prepare_tiled(int max_halo) {
@@ -1241,13 +1268,19 @@ int tiled_max_ctas_per_sm(int prec, int order, int nq, int flux, int max_halo, i
 void launch_tiled_limiter(const TileArgs& t, int ctas, int ld, void* U, const int4* conn,
                           const void* lim, const double* jinv, const int* flags,
                           const double* refs, int prec, int nq2, double gamma, double tvb_m,
-                          const StepCtl* ctl, const int* tile_flags, cudaStream_t stream) {
+                          const StepCtl* ctl, int* tile_flags, int* tile_list, int tile_cap,
+                          cudaStream_t stream) {
     const int cfg1 = cfg_index(3, 2), cfg2 = cfg_index(nq2, 3);
-    const int grid = ctas > 0 ? ctas : std::max(1, (t.ntiles + kLimGroup - 1) / kLimGroup);
+    if (tile_list != nullptr && tile_flags == nullptr)
+        throw Error{RKDG_ERR_INVALID, "a limiter tile list needs its tile flags"};
+    // one CTA per tile, or a persistent grid (the caller's, else four CTAs
+    // per SM) over a tile list
+    int grid = ctas > 0 ? ctas : std::max(1, t.ntiles);
+    if (tile_list != nullptr && ctas <= 0) grid = std::max(1, std::min(t.ntiles, 4 * sm_count()));
     if (prec == RKDG_FP32)
-        tiled_limiter_kernel<float><<<grid, kAuxBlock, 0, stream>>>(t, ld, static_cast<float*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl, tile_flags);
+        tiled_limiter_kernel<float><<<grid, kAuxBlock, 0, stream>>>(t, ld, static_cast<float*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl, tile_flags, tile_list, tile_cap);
     else
-        tiled_limiter_kernel<double><<<grid, kAuxBlock, 0, stream>>>(t, ld, static_cast<double*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl, tile_flags);
+        tiled_limiter_kernel<double><<<grid, kAuxBlock, 0, stream>>>(t, ld, static_cast<double*>(U), conn, lim, jinv, flags, refs, gamma, tvb_m, cfg1, cfg2, ctl, tile_flags, tile_list, tile_cap);
     RKDG_CUDA_TRY(cudaGetLastError());
 }
 

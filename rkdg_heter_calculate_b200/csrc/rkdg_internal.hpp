@@ -166,6 +166,7 @@ struct DeviceArrays {
     int4* conn = nullptr;       // [ld]
     void* lim = nullptr;        // [3][ld] (alpha, beta) of the limiter (when enabled)
     int* tile_flags = nullptr;  // [ntiles] the stage kernel's per-tile limiter test (when enabled)
+    int* tile_list = nullptr;   // [2 + ntiles] the tiles the limiter must visit (LimitList)
     int32_t* perm = nullptr;    // [T]
     double* conv_in = nullptr;  // [T][36]
     double* conv_out = nullptr; // [T][36]
@@ -180,6 +181,14 @@ struct DeviceArrays {
     uint16_t* task = nullptr;
     size_t bytes = 0;
 };
+
+// The tiles a stage's TVB limiter must visit, built by the stage kernel:
+// int[2 + cap] = {count, CTAs done, tile ids...}.  A tile whose limiter test
+// fails (tvb_keeps false for an element) sets its flag (tile_flags, 0 -> 1)
+// and appends itself once; the limiter visits the listed tiles, clears their
+// flags, and its last CTA to finish resets count and done, so every flag is
+// 0 and the list empty when the next stage starts.
+constexpr int kListHead = 2;
 
 struct TileArgs {
     const int4* code;   // [elements] per-edge source codes
@@ -207,7 +216,9 @@ struct StageArgs {
     int last_stage;      // compute wave max / error (and the monitor when asked) in the epilogue
     int monitor;         // last stage: also form the residual monitor max |d mean| (rho, rhoE)
     int lo_row;          // RKDG_FP32C: state row of the cell means' low parts (in U, U0, Unew), else -1
-    int* tile_flags;     // with the TVB limiter: per tile of the launch, 1 if the limiter may change an element
+    int* tile_flags;     // with the TVB limiter: per tile of the launch, 1 while the tile is in tile_list
+    int* tile_list;      // with tile_flags: the LimitList the stage appends its limiter-changeable tiles to
+    int tile_cap;        // entries of tile_list
     const int* limiter_on;  // per solve: the test is made only for solves with the limiter (null: all)
     double tvb_m;        // the TVB constant of that test
 };
@@ -252,6 +263,7 @@ bool tiled_fits(int prec, int order, int flux, int max_halo, int tile);
 // resident CTAs per SM of the tiled stage kernel (order 3: mixed pack) for
 // tiles of `tile` elements
 int tiled_max_ctas_per_sm(int prec, int order, int nq, int flux, int max_halo, int tile = kTile);
+int sm_count();  // SMs of the current device
 // TVB limiter over tiles; flags[solve] (may be null: all on) enables it per
 // solve, solves whose control block (ctl may be null) says done are skipped,
 // and tiles whose tile_flags entry (may be null) is 0 -- the stage kernel
@@ -260,7 +272,8 @@ int tiled_max_ctas_per_sm(int prec, int order, int nq, int flux, int max_halo, i
 void launch_tiled_limiter(const TileArgs& t, int ctas, int ld, void* U, const int4* conn,
                           const void* lim, const double* jinv, const int* flags,
                           const double* refs, int prec, int nq2, double gamma, double tvb_m,
-                          const StepCtl* ctl, const int* tile_flags, cudaStream_t stream);
+                          const StepCtl* ctl, int* tile_flags, int* tile_list, int tile_cap,
+                          cudaStream_t stream);
 // Caller layout [4][nb][ldh] FP64 <-> HBM state packs.  lo_row >= 0: the
 // state is RKDG_FP32C and row lo_row holds the low part of each cell mean
 // (import splits the FP64 mean into high and low floats, export and the

@@ -131,6 +131,7 @@ struct rkdg_server {
     double* far = nullptr;
     int* flags = nullptr;
     int* tile_flags = nullptr;   // [2][tcap] the stage kernel's per-tile limiter test, per list
+    int* tile_list = nullptr;    // [2][kListHead + tcap] the tiles each list's limiter visits
     double* staging = nullptr;
     StepCtl* h_ctl = nullptr;
     cudaStream_t stream = nullptr;
@@ -238,9 +239,12 @@ void enqueue_step(rkdg_server* s) {
         for (int f = 0; f < 2; ++f) {
             cudaStream_t st_f = f == RKDG_FLUX_HLLC ? s->stream2 : s->stream;
             a.tile_flags = s->tile_flags + f * s->tcap;
+            a.tile_list = s->tile_list + f * (kListHead + s->tcap);
+            a.tile_cap = (int)s->tcap;
             launch_stage(a, s->tiles[f], 3, s->p.nq, f, kprec(s), s->ctas[f], st_f);
             launch_tiled_limiter(s->tiles[f], s->ctas[f], s->ld, s->U[pl[2]], s->conn, s->lim, s->jinv, s->flags,
-                                 s->far, kprec(s), s->p.nq, s->p.gamma, s->p.tvb_m, s->ctl, a.tile_flags, st_f);
+                                 s->far, kprec(s), s->p.nq, s->p.gamma, s->p.tvb_m, s->ctl, a.tile_flags,
+                                 a.tile_list, a.tile_cap, st_f);
         }
         RKDG_CUDA_TRY(cudaEventRecord(s->ev_join, s->stream2));
         RKDG_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
@@ -501,7 +505,8 @@ void destroy_server(rkdg_server* s) {
     if (s->graph) cudaGraphExecDestroy(s->graph);
     for (void* p : {s->U[0], s->U[1], s->U[2], (void*)s->jinv, (void*)s->tcode, (void*)s->conn, (void*)s->lim,
                     (void*)s->perm, (void*)s->halo, (void*)s->task, (void*)s->desc, (void*)s->ntiles_dev,
-                    (void*)s->ctl, (void*)s->far, (void*)s->flags, (void*)s->tile_flags, (void*)s->staging})
+                    (void*)s->ctl, (void*)s->far, (void*)s->flags, (void*)s->tile_flags, (void*)s->tile_list,
+                    (void*)s->staging})
         cudaFree(p);
     if (s->h_ctl) cudaFreeHost(s->h_ctl);
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
@@ -597,7 +602,10 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
         h2d(s, s->far, f.data(), f.size());
         s->flags = (int*)salloc(s, sizeof(int) * max_slots);
         s->tile_flags = (int*)salloc(s, sizeof(int) * 2 * (size_t)s->tcap);
+        s->tile_list = (int*)salloc(s, sizeof(int) * 2 * (kListHead + (size_t)s->tcap));
         RKDG_CUDA_TRY(cudaMemsetAsync(s->flags, 0, sizeof(int) * max_slots, s->stream));
+        RKDG_CUDA_TRY(cudaMemsetAsync(s->tile_flags, 0, sizeof(int) * 2 * (size_t)s->tcap, s->stream));
+        RKDG_CUDA_TRY(cudaMemsetAsync(s->tile_list, 0, sizeof(int) * 2 * (kListHead + (size_t)s->tcap), s->stream));
         s->staging = (double*)salloc(s, sizeof(double) * 24 * (size_t)s->max_T);
         RKDG_CUDA_TRY(cudaMallocHost(&s->h_ctl, sizeof(StepCtl) * max_slots));
         s->elems.reset(s->cap);

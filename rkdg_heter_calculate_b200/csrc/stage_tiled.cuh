@@ -913,7 +913,6 @@ __global__ void __launch_bounds__(BT, TiledOccupancy<Real, ORD, BT>::value)
         parity ^= 1u;
         if (done) {  // finished solve: pass the tile on
             if (threadIdx.x == 0 && nxt < ntiles) stage_copy<Real, BT>(a, __ldg(ta.desc + 2 * nxt), stg, &s_bar);
-            if ((MODE & MODE_LIMITED) && threadIdx.x == 0) a.tile_flags[tile] = 0;
             continue;
         }
         bool need;
@@ -927,7 +926,10 @@ __global__ void __launch_bounds__(BT, TiledOccupancy<Real, ORD, BT>::value)
         // barrier also ORs its test over the tile)
         if constexpr (MODE & MODE_LIMITED) {
             const int any = __syncthreads_or(need);
-            if (threadIdx.x == 0) a.tile_flags[tile] = any;
+            if (threadIdx.x == 0 && any && atomicExch(a.tile_flags + tile, 1) == 0) {
+                const int slot = atomicAdd(a.tile_list, 1);
+                if (slot < a.tile_cap) a.tile_list[kListHead + slot] = tile;
+            }
         } else {
             __syncthreads();
         }
