@@ -86,6 +86,14 @@ constexpr int64_t kElemAlign = 32;
 int64_t elem_span(int T) { return (T + kElemAlign - 1) / kElemAlign * kElemAlign; }
 constexpr int kPoolHalo = 160;  // halo entries per tile the pool's kernels stage
 
+// The pool's active tiles are kept in four lists, one per (flux, order):
+// list 2 flux + 0 holds P2 tiles, 2 flux + 1 P1 tiles, so each list runs the
+// single-order kernel for its tiles (P1 kernels hold more warps per SM).
+constexpr int kLists = 4;
+int list_of(int flux, int order) { return 2 * flux + (order == 2 ? 0 : 1); }
+int list_flux(int l) { return l / 2; }
+int list_order(int l) { return l % 2 == 0 ? 2 : 1; }
+
 struct Request {
     int64_t id = 0;
     int order = 2, nb = 6, T = 0;
@@ -112,7 +120,7 @@ struct Request {
 
 struct rkdg_server {
     rkdg_params p{};
-    int device = 0, word = 4, max_slots = 0, ctas[2] = {0, 0};
+    int device = 0, word = 4, max_slots = 0, ctas[kLists] = {0, 0, 0, 0};
     int64_t cap = 0, hcap = 0, kcap = 0, tcap = 0, max_T = 0;
     int ld = 0;
     size_t bytes = 0;
@@ -126,19 +134,19 @@ struct rkdg_server {
     int2* halo = nullptr;
     uint16_t* task = nullptr;
     int4* desc = nullptr;
-    int* ntiles_dev = nullptr;   // [2]: active tiles of the LLF and HLLC lists
+    int* ntiles_dev = nullptr;   // [kLists]: active tiles of each list
     StepCtl* ctl = nullptr;
     double* far = nullptr;
     int* flags = nullptr;
-    int* tile_flags = nullptr;   // [2][tcap] the stage kernel's per-tile limiter test, per list
-    int* tile_list = nullptr;    // [2][kListHead + tcap] the tiles each list's limiter visits
+    int* tile_flags = nullptr;   // [kLists][tcap] the stage kernel's per-tile limiter test, per list
+    int* tile_list = nullptr;    // [kLists][kListHead + tcap] the tiles each list's limiter visits
     double* staging = nullptr;
     StepCtl* h_ctl = nullptr;
     cudaStream_t stream = nullptr;
-    cudaStream_t stream2 = nullptr;  // the HLLC tiles' launches, forked and joined in the step graph
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t side[kLists - 1] = {nullptr, nullptr, nullptr};  // lists 1.., forked and joined per stage
+    cudaEvent_t ev_fork = nullptr, ev_join[kLists - 1] = {nullptr, nullptr, nullptr};
     cudaGraphExec_t graph = nullptr;
-    TileArgs tiles[2]{};  // indexed by flux: the LLF and the HLLC requests' tiles
+    TileArgs tiles[kLists]{};  // per list (flux, order)
     // host state
     RangeAlloc elems, halos, tasks;
     std::vector<int> free_slots;
@@ -154,7 +162,7 @@ struct rkdg_server {
     int fatal_code = RKDG_OK;
     int fault_after = -1;      // rkdg_server_inject_fault: chunks left before a simulated failure
     bool tiles_dirty = false;
-    int ntiles[2] = {0, 0};
+    int ntiles[kLists] = {0, 0, 0, 0};
     // stats
     double dof_updates = 0, busy = 0;
     double t_admit = 0, t_retire = 0;  // engine seconds spent uploading and retiring requests
@@ -208,10 +216,10 @@ void coeffs(int rk, int st, double& a, double& c) {
 }
 
 // One step of every solve in flight: per RK stage, the stage kernel and the
-// limiter over the LLF requests' tiles on the server's stream and over the
-// HLLC requests' tiles on a second stream forked from it (the two lists
-// hold different solves, so the launches overlap where one list runs out),
-// joined before the next stage.
+// limiter over each tile list (flux, order), the first on the server's
+// stream and the others on streams forked from it (the lists hold different
+// solves, so the launches overlap where one runs out), joined before the
+// next stage.
 void enqueue_step(rkdg_server* s) {
     launch_step_begin(s->ctl, s->max_slots, s->stream);
     const int plan[3][3] = {{0, 0, 1}, {1, 0, 2}, {2, 0, 0}};
@@ -235,19 +243,21 @@ void enqueue_step(rkdg_server* s) {
         a.tvb_m = s->p.tvb_m;
         a.limiter_on = s->flags;
         RKDG_CUDA_TRY(cudaEventRecord(s->ev_fork, s->stream));
-        RKDG_CUDA_TRY(cudaStreamWaitEvent(s->stream2, s->ev_fork, 0));
-        for (int f = 0; f < 2; ++f) {
-            cudaStream_t st_f = f == RKDG_FLUX_HLLC ? s->stream2 : s->stream;
-            a.tile_flags = s->tile_flags + f * s->tcap;
-            a.tile_list = s->tile_list + f * (kListHead + s->tcap);
+        for (int l = 1; l < kLists; ++l) RKDG_CUDA_TRY(cudaStreamWaitEvent(s->side[l - 1], s->ev_fork, 0));
+        for (int l = 0; l < kLists; ++l) {
+            cudaStream_t st_l = l == 0 ? s->stream : s->side[l - 1];
+            a.tile_flags = s->tile_flags + l * s->tcap;
+            a.tile_list = s->tile_list + l * (kListHead + s->tcap);
             a.tile_cap = (int)s->tcap;
-            launch_stage(a, s->tiles[f], 3, s->p.nq, f, kprec(s), s->ctas[f], st_f);
-            launch_tiled_limiter(s->tiles[f], s->ctas[f], s->ld, s->U[pl[2]], s->conn, s->lim, s->jinv, s->flags,
+            launch_stage(a, s->tiles[l], list_order(l), s->p.nq, list_flux(l), kprec(s), s->ctas[l], st_l);
+            launch_tiled_limiter(s->tiles[l], s->ctas[l], s->ld, s->U[pl[2]], s->conn, s->lim, s->jinv, s->flags,
                                  s->far, kprec(s), s->p.nq, s->p.gamma, s->p.tvb_m, s->ctl, a.tile_flags,
-                                 a.tile_list, a.tile_cap, st_f);
+                                 a.tile_list, a.tile_cap, st_l);
         }
-        RKDG_CUDA_TRY(cudaEventRecord(s->ev_join, s->stream2));
-        RKDG_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
+        for (int l = 1; l < kLists; ++l) {
+            RKDG_CUDA_TRY(cudaEventRecord(s->ev_join[l - 1], s->side[l - 1]));
+            RKDG_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev_join[l - 1], 0));
+        }
     }
 }
 
@@ -314,24 +324,21 @@ void relocate(const Request& r, std::vector<int32_t>& d) {
     }
 }
 
-// Rewrites the two active tile lists (per flux; P2 tiles first, then P1:
-// the expensive tiles start early in the persistent pass) and measures the
-// CFL wave speed of the newly admitted solves over their own tiles only, so
-// the solves already in flight keep the value their last stage computed.
+// Rewrites the active tile lists (per flux and order) and measures the CFL
+// wave speed of the newly admitted solves over their own tiles only, so the
+// solves already in flight keep the value their last stage computed.
 void rebuild_tiles(rkdg_server* s, const std::vector<std::shared_ptr<Request>>& fresh) {
-    std::vector<int32_t> d[2], dn;
-    for (int f = 0; f < 2; ++f)
-        for (int pass = 0; pass < 2; ++pass)
-            for (auto& r : s->active)
-                if (r && r->flux == f && (pass == 0) == (r->order == 2)) relocate(*r, d[f]);
+    std::vector<int32_t> d[kLists], dn;
+    for (auto& r : s->active)
+        if (r) relocate(*r, d[list_of(r->flux, r->order)]);
     for (auto& r : fresh) relocate(*r, dn);
-    for (int f = 0; f < 2; ++f) {
-        s->ntiles[f] = (int)(d[f].size() / 8);
-        h2d(s, reinterpret_cast<int32_t*>(const_cast<int4*>(s->tiles[f].desc)), d[f].data(), d[f].size());
+    for (int l = 0; l < kLists; ++l) {
+        s->ntiles[l] = (int)(d[l].size() / 8);
+        h2d(s, reinterpret_cast<int32_t*>(const_cast<int4*>(s->tiles[l].desc)), d[l].data(), d[l].size());
     }
-    h2d(s, s->ntiles_dev, s->ntiles, 2);
+    h2d(s, s->ntiles_dev, s->ntiles, kLists);
     if (!dn.empty()) {
-        int4* scratch = s->desc + 4 * s->tcap;
+        int4* scratch = s->desc + 2 * kLists * s->tcap;
         h2d(s, reinterpret_cast<int32_t*>(scratch), dn.data(), dn.size());
         TileArgs t = s->tiles[0];
         t.desc = scratch;
@@ -510,8 +517,10 @@ void destroy_server(rkdg_server* s) {
         cudaFree(p);
     if (s->h_ctl) cudaFreeHost(s->h_ctl);
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
-    if (s->ev_join) cudaEventDestroy(s->ev_join);
-    if (s->stream2) cudaStreamDestroy(s->stream2);
+    for (int l = 0; l < kLists - 1; ++l) {
+        if (s->ev_join[l]) cudaEventDestroy(s->ev_join[l]);
+        if (s->side[l]) cudaStreamDestroy(s->side[l]);
+    }
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -548,10 +557,11 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
         // limiter geometry, permutation, ~1 halo entry, 2 task entries, descriptors
         // bytes per pooled element: 3 state buffers (P2 rows), J^-1, tile
         // codes, connectivity, limiter geometry, permutation, one halo entry,
-        // three flux tasks, tile descriptors; plus the FP64 staging buffer
-        // of the largest admissible request and a fixed reserve
+        // three flux tasks, tile descriptors, flags and lists (2 bytes: 192
+        // per tile); plus the FP64 staging buffer of the largest admissible
+        // request and a fixed reserve
         const size_t per_elem = (size_t)3 * 16 * state_rows(p.precision, 6) + 32 + 16 + 16 +
-                                (kernel_prec(p.precision) == RKDG_FP64 ? 48 : 24) + 4 + 8 + 6 + 1;
+                                (kernel_prec(p.precision) == RKDG_FP64 ? 48 : 24) + 4 + 8 + 6 + 2;
         const size_t fixed = (size_t)64 << 20, stage_per_elem = 24 * sizeof(double);
         if (budget < fixed + 4096 * (per_elem + stage_per_elem))
             throw Error{RKDG_ERR_NOMEM, "HBM budget too small"};
@@ -567,9 +577,11 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
         s->kcap = 3 * s->cap;
         s->tcap = s->cap / 128 + 2 * (int64_t)max_slots + 16;
         RKDG_CUDA_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
-        RKDG_CUDA_TRY(cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking));
         RKDG_CUDA_TRY(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
-        RKDG_CUDA_TRY(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+        for (int l = 0; l < kLists - 1; ++l) {
+            RKDG_CUDA_TRY(cudaStreamCreateWithFlags(&s->side[l], cudaStreamNonBlocking));
+            RKDG_CUDA_TRY(cudaEventCreateWithFlags(&s->ev_join[l], cudaEventDisableTiming));
+        }
         upload_tables(6, 3);
         upload_tables(3, 2);
         for (int k = 0; k < 3; ++k) {
@@ -584,9 +596,10 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
         s->perm = (int32_t*)salloc(s, sizeof(int32_t) * (size_t)s->cap);
         s->halo = (int2*)salloc(s, sizeof(int2) * (size_t)s->hcap + kTablePad);
         s->task = (uint16_t*)salloc(s, sizeof(uint16_t) * (size_t)s->kcap + kTablePad);
-        s->desc = (int4*)salloc(s, sizeof(int32_t) * 24 * (size_t)s->tcap);  // two lists + admission scratch
-        s->ntiles_dev = (int*)salloc(s, 2 * sizeof(int));
-        RKDG_CUDA_TRY(cudaMemsetAsync(s->ntiles_dev, 0, 2 * sizeof(int), s->stream));
+        // the lists' descriptors and the admission scratch, 2 int4 per tile each
+        s->desc = (int4*)salloc(s, sizeof(int4) * 2 * (kLists + 1) * (size_t)s->tcap);
+        s->ntiles_dev = (int*)salloc(s, kLists * sizeof(int));
+        RKDG_CUDA_TRY(cudaMemsetAsync(s->ntiles_dev, 0, kLists * sizeof(int), s->stream));
         s->ctl = (StepCtl*)salloc(s, sizeof(StepCtl) * max_slots);
         std::vector<StepCtl> c(max_slots);
         for (auto& x : c) {
@@ -601,11 +614,12 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
             for (int v = 0; v < 4; ++v) f[4 * i + v] = p.farfield[v];
         h2d(s, s->far, f.data(), f.size());
         s->flags = (int*)salloc(s, sizeof(int) * max_slots);
-        s->tile_flags = (int*)salloc(s, sizeof(int) * 2 * (size_t)s->tcap);
-        s->tile_list = (int*)salloc(s, sizeof(int) * 2 * (kListHead + (size_t)s->tcap));
+        s->tile_flags = (int*)salloc(s, sizeof(int) * kLists * (size_t)s->tcap);
+        s->tile_list = (int*)salloc(s, sizeof(int) * kLists * (kListHead + (size_t)s->tcap));
         RKDG_CUDA_TRY(cudaMemsetAsync(s->flags, 0, sizeof(int) * max_slots, s->stream));
-        RKDG_CUDA_TRY(cudaMemsetAsync(s->tile_flags, 0, sizeof(int) * 2 * (size_t)s->tcap, s->stream));
-        RKDG_CUDA_TRY(cudaMemsetAsync(s->tile_list, 0, sizeof(int) * 2 * (kListHead + (size_t)s->tcap), s->stream));
+        RKDG_CUDA_TRY(cudaMemsetAsync(s->tile_flags, 0, sizeof(int) * kLists * (size_t)s->tcap, s->stream));
+        RKDG_CUDA_TRY(cudaMemsetAsync(s->tile_list, 0, sizeof(int) * kLists * (kListHead + (size_t)s->tcap),
+                                      s->stream));
         s->staging = (double*)salloc(s, sizeof(double) * 24 * (size_t)s->max_T);
         RKDG_CUDA_TRY(cudaMallocHost(&s->h_ctl, sizeof(StepCtl) * max_slots));
         s->elems.reset(s->cap);
@@ -614,17 +628,18 @@ int rkdg_server_create(const rkdg_params* params, size_t budget, int32_t max_slo
         for (int i = max_slots - 1; i >= 0; --i) s->free_slots.push_back(i);
         s->active.assign(max_slots, nullptr);
         // persistent grid, and a graph of one step whose tile count is read on the device
-        for (int f = 0; f < 2; ++f) {
-            const int per_sm = std::max(1, tiled_max_ctas_per_sm(kernel_prec(p.precision), 3, p.nq, f, kPoolHalo));
-            s->ctas[f] = prop.multiProcessorCount * per_sm;
-            TileArgs& t = s->tiles[f];
+        for (int l = 0; l < kLists; ++l) {
+            const int per_sm = std::max(1, tiled_max_ctas_per_sm(kernel_prec(p.precision), list_order(l), p.nq,
+                                                                 list_flux(l), kPoolHalo));
+            s->ctas[l] = prop.multiProcessorCount * per_sm;
+            TileArgs& t = s->tiles[l];
             t.code = s->tcode;
-            t.desc = s->desc + 2 * f * s->tcap;
+            t.desc = s->desc + 2 * l * s->tcap;
             t.halo = s->halo;
             t.task = s->task;
             t.max_halo = kPoolHalo;
             t.ntiles = (int)s->tcap;
-            t.ntiles_dev = s->ntiles_dev + f;
+            t.ntiles_dev = s->ntiles_dev + l;
         }
         RKDG_CUDA_TRY(cudaStreamSynchronize(s->stream));
         cudaGraph_t g;

@@ -99,7 +99,7 @@ def test_budget_and_slots_bound_admission():
     reqs = requests()
     big = max(r[0].ntri for r in reqs)
     # a pool of about 1.2x the largest request: the rest queue until memory frees
-    per_elem = 3 * 24 * 4 + 107 + 192   # FP32 pool bytes per element, staging included
+    per_elem = 3 * 24 * 4 + 108 + 192   # FP32 pool bytes per element, staging included
     budget = 64 * MB + int(1.2 * big) * per_elem
     with Server(budget, max_slots=3, precision="fp32", **SERVER) as srv:
         cap = srv.stats()["capacity_elements"]
@@ -117,7 +117,7 @@ def test_budget_and_slots_bound_admission():
 
 def test_oversized_request_rejected():
     reqs = requests()
-    per_elem = 3 * 24 * 4 + 107 + 192   # FP32 pool bytes per element, staging included
+    per_elem = 3 * 24 * 4 + 108 + 192   # FP32 pool bytes per element, staging included
     with Server(64 * MB + 4300 * per_elem, max_slots=2, precision="fp32", **SERVER) as srv:
         step = reqs[4]
         assert step[0].ntri > srv.stats()["capacity_elements"]
