@@ -2,9 +2,11 @@
 (oracle/_ref/gpu/librkdg_ref_gpu.so, made by `make -C oracle libref_gpu`
 from the reference checkout; see ref_gpu_harness.cu).
 
-Measurement and test infrastructure: the "reference on the GPU" timing in
-bench.py and the check that the reference's kernels, run on the device,
-agree with its host-compiled build.  The product library never calls it.
+Test infrastructure: the check that the reference's kernels, run on the
+device, agree with its host-compiled build, the residual comparison with
+this library, the byte comparison of the solution writer, and the step-rate
+comparison printed by tests/test_gpu_reference_kernels.py.  The product
+library and the benchmark never call it.
 """
 from __future__ import annotations
 
