@@ -65,7 +65,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "vortex", "serving", "step"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "vortex", "serving", "step", "decomp"])
+    ap.add_argument("--decomp-parts", default="1,2,4",
+                    help="--workload decomp at N = 1: part counts sharing the GPU (under torchrun: one per rank)")
     ap.add_argument("--no-step", action="store_true", help="skip the Mach-3 step FP32/FP64 comparison")
     ap.add_argument("--step-h", type=int, default=400, help="1/h of the Mach-3 step lattice")
     ap.add_argument("--step-times", default="0.05,0.5", help="output times of the Mach-3 step runs")
@@ -495,6 +497,68 @@ def run_plain(args, dist, peak, peak_kind, K):
     return out, T
 
 
+# ------------------------------------------------- domain decomposition --
+def run_decomp(args, dist):
+    """One mesh decomposed into parts (the unstructured vortex of the plain
+    workload, P2, HLLC, SSP-RK3, CFL 0.2, the first form of --precision).
+    At N = 1 the parts of each count in --decomp-parts share the GPU
+    (LocalTransport: rows between the parts' buffers, events between their
+    streams); under torchrun each rank holds one part of an N-way split and
+    moves rows with NCCL (TorchTransport).  Each run: W warm-up steps, then
+    K steps of DecomposedSolve.advance_device (halo transfers, the
+    wave-speed all-reduce and the stages in stream order), timed from a CUDA
+    event before the first enqueue to one after every part's stream has
+    drained, max over ranks; the single context's advance on the same mesh
+    beside it."""
+    import torch
+
+    from rkdg_heter_calculate_b200 import meshgen, vortex
+    from rkdg_heter_calculate_b200.decomp import (DecomposedSolve, DevicePart, LocalTransport, Partition,
+                                                  TorchTransport)
+
+    prec = precisions(args)[0]
+    K, W = args.steps, args.warmup
+    mesh = meshgen.periodic_delaunay(args.lattice, L=10.0, jitter=0.3, seed=2)
+    T = mesh.ntri
+    U0 = vortex.project_native(mesh, lambda X, Y: vortex.exact(X, Y, 0.0), 6, n=4)
+    kw = dict(order=2, nq=6, ng=3, flux="hllc", rk=3, precision=prec, gamma=GAMMA, cfl=0.2, farfield=FAR_C2)
+    out = {"workload": f"unstructured isentropic vortex, periodic Delaunay of a {args.lattice}x{args.lattice} "
+                       f"lattice jittered +-0.3h (seed 2), {T} triangles, P2, HLLC, SSP-RK3, CFL 0.2, {prec}",
+           "triangles": T, "steps": K, "warmup": W, "runs": []}
+    s = solver_for(mesh, prec)
+    s.setFreedom(U0, basis="native")
+    s.advance(W)
+    ms1 = event_time(s.stream(), lambda: s.advance(K), dist)
+    s.close()
+    out["single_context"] = {"dof_stage_per_s": T * 72 * K / (ms1 * 1e-3), "ms_per_step": ms1 / K}
+    counts = [dist.world] if dist.world > 1 else [int(x) for x in args.decomp_parts.split(",")]
+    for k in counts:
+        P = Partition(mesh, k)
+        mine = [dist.rank] if dist.world > 1 else list(range(k))
+        parts = {p: DevicePart(P, p, **kw) for p in mine}
+        for p, part in parts.items():
+            part.set_state(P.split(U0, p), basis="native")
+        solve = DecomposedSolve(parts, TorchTransport() if dist.world > 1 else LocalTransport(), rk=3)
+        solve.advance_device(W)
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for part in parts.values():
+            part.stream().wait_event(e0)
+        solve.advance_device(K)  # returns once every part's stream has drained
+        e1.record()
+        torch.cuda.synchronize()
+        ms = dist.max(e0.elapsed_time(e1))
+        halo = int(sum(P.halo[p].size for p in range(k)))
+        out["runs"].append({"parts": k, "ranks": dist.world, "dof_stage_per_s": T * 72 * K / (ms * 1e-3),
+                            "ms_per_step": ms / K, "halo_copies": halo,
+                            "vs_single_context": ms1 / ms})
+        for part in parts.values():
+            part.close()
+    return out
+
+
 # ------------------------------------------------------ Mach-3 step (C3) --
 def run_step(args, dist, peak, peak_kind):
     """Mach-3 wind-tunnel step: jittered Delaunay mesh, h = 1/400 (seed 3),
@@ -892,6 +956,10 @@ def main():
         step = run_step(args, dist, *measured_peak())
         if dist.rank == 0:
             print(json.dumps({"workload": "step", "n_gpus": dist.world, "step_fp32_vs_fp64": step}), flush=True)
+    elif args.workload == "decomp":
+        dec = run_decomp(args, dist)
+        if dist.rank == 0:
+            print(json.dumps({"workload": "decomp", "n_gpus": dist.world, "decomp": dec}), flush=True)
     elif args.workload == "serving":
         serving = run_serving(args, dist)
         if dist.rank == 0:

@@ -245,6 +245,32 @@ int rkdg_gather_rows(rkdg_ctx* ctx, const int32_t* d_index, int32_t n, int32_t n
 int rkdg_scatter_rows(rkdg_ctx* ctx, const int32_t* d_index, int32_t n, int32_t nrows, const void* d_buf);
 /* Waits for the context's stream and reports any error its kernels flagged. */
 int rkdg_sync(rkdg_ctx* ctx);
+/* Stream-ordered steps of a partition: every call below only enqueues work
+ * on the context's stream (no host round trip; errors surface at rkdg_sync
+ * or rkdg_part_time), so a decomposed step runs with the halo transfers
+ * (NCCL send/recv) and one all-reduce on the same streams.  Per step, on
+ * every partition: refresh the halo copies; rkdg_part_wave(ctx, d_w, 0)
+ * writes the partition's CFL wave-speed maximum over its owned elements
+ * (one double, device memory); the caller reduces it to the maximum over
+ * all partitions (an all-reduce MAX) and hands it back with
+ * rkdg_part_wave(ctx, d_w, 1); rkdg_part_begin_step forms dt = cfl / that
+ * maximum, clips it to the final time set by rkdg_part_set_final_time,
+ * advances the device-resident time and step count and keeps the state as
+ * U^n; then per RK stage a halo refresh and rkdg_part_stage (which never
+ * applies the limiter), and with the TVB limiter a means refresh and
+ * rkdg_part_limit.  Every partition forms the same dt.  A finished solve
+ * (time at its final time) skips later steps.  This replaces the
+ * reference's per-step dt read-back and its host-staged MPI exchange
+ * (src/rkdgadvance.cpp:165-168, 287-409), and the dt reduction it left
+ * commented out (src/rkdgadvance.cpp:226-234). */
+int rkdg_part_set_final_time(rkdg_ctx* ctx, double t_final);
+int rkdg_part_wave(rkdg_ctx* ctx, double* d_wave, int32_t to_context);
+int rkdg_part_begin_step(rkdg_ctx* ctx);
+int rkdg_part_stage(rkdg_ctx* ctx, int32_t stage);
+int rkdg_part_limit(rkdg_ctx* ctx);
+/* Waits, reports flagged errors, and returns the time, the step count and
+ * whether the final time has been reached (any pointer may be NULL). */
+int rkdg_part_time(rkdg_ctx* ctx, double* t, int32_t* steps, int32_t* done);
 
 /* ---- output ------------------------------------------------------------ */
 /* Writes the cell means as the reference's Tecplot solution.plt

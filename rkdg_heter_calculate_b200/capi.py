@@ -117,6 +117,12 @@ def lib():
             "rkdg_gather_rows": (C.c_int, [vp, vp, C.c_int32, C.c_int32, vp]),
             "rkdg_scatter_rows": (C.c_int, [vp, vp, C.c_int32, C.c_int32, vp]),
             "rkdg_sync": (C.c_int, [vp]),
+            "rkdg_part_set_final_time": (C.c_int, [vp, C.c_double]),
+            "rkdg_part_wave": (C.c_int, [vp, vp, C.c_int32]),
+            "rkdg_part_begin_step": (C.c_int, [vp]),
+            "rkdg_part_stage": (C.c_int, [vp, C.c_int32]),
+            "rkdg_part_limit": (C.c_int, [vp]),
+            "rkdg_part_time": (C.c_int, [vp, _dp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
             "rkdg_server_status": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
             "rkdg_server_timing": (C.c_int, [vp, _dp, _dp, _dp, C.POINTER(C.c_int64)]),
             "rkdg_server_inject_fault": (C.c_int, [vp, C.c_int32]),

@@ -180,7 +180,7 @@ void stage_coeffs(int rk, int s, double& a, double& b) {
     }
 }
 
-void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out, bool monitor = true) {
+void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out, bool monitor = true, bool part_stage = false) {
     StageArgs a = base_args(c);
     stage_coeffs(c->p.rk, s, a.a, a.b);
     a.U = c->d.U[in];
@@ -190,7 +190,7 @@ void launch_one_stage(rkdg_ctx* c, int s, int in, int u0, int out, bool monitor 
     a.monitor = monitor ? 1 : 0;
     // a partition applies its limiter by rkdg_limit once the halo means of
     // the stage output have been exchanged
-    const bool limit = c->p.limiter == RKDG_LIMITER_TVB && c->T_own == c->T;
+    const bool limit = c->p.limiter == RKDG_LIMITER_TVB && c->T_own == c->T && !part_stage;
     // the stage lists the tiles its limiter test finds changeable; the
     // limiter visits those
     a.tile_flags = limit ? c->d.tile_flags : nullptr;
@@ -239,6 +239,15 @@ cudaGraphExec_t capture_steps(rkdg_ctx* c, int steps, bool monitor) {
 
 void check_error_flag(rkdg_ctx* c) {
     throw_ctl_error(c->h_ctl->error, "solve");
+}
+
+// the buffer a stage writes: the last stage of a step overwrites U^n in
+// place (each element reads its own U^n first), the others a free buffer
+int stage_output(const rkdg_ctx* c, int s) {
+    if (s == c->p.rk - 1 && s > 0 && c->old != c->cur) return c->old;
+    int out = 0;
+    while (out == c->cur || out == c->old) ++out;
+    return out;
 }
 
 // One line of the residual history for the step just taken (the control
@@ -473,6 +482,84 @@ int rkdg_scatter_rows(rkdg_ctx* c, const int32_t* d_index, int32_t n, int32_t nr
     });
 }
 
+int rkdg_part_set_final_time(rkdg_ctx* c, double t_final) {
+    return guarded([&] {
+        if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        pull_ctl(c);
+        c->h_ctl->t_final = t_final > 0 ? t_final : 0.0;
+        c->h_ctl->dt_fixed = 0.0;
+        c->h_ctl->done = 0;
+        push_ctl(c);
+        sync(c);
+    });
+}
+
+int rkdg_part_wave(rkdg_ctx* c, double* d_wave, int32_t to_context) {
+    return guarded([&] {
+        if (!c || !d_wave) throw Error{RKDG_ERR_INVALID, "rkdg_part_wave: bad arguments"};
+        require_state(c);
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        // the maximum is kept as the bits of a non-negative double
+        unsigned long long* w = &c->d.ctl->wave_bits;
+        if (to_context) {
+            RKDG_CUDA_TRY(cudaMemcpyAsync(w, d_wave, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+            c->wave_valid = true;
+        } else {
+            ensure_wave(c);
+            RKDG_CUDA_TRY(cudaMemcpyAsync(d_wave, w, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        }
+    });
+}
+
+int rkdg_part_begin_step(rkdg_ctx* c) {
+    return guarded([&] {
+        if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        require_state(c);
+        if (!c->wave_valid) throw Error{RKDG_ERR_STATE, "rkdg_part_begin_step: no wave-speed maximum (rkdg_part_wave)"};
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        launch_step_begin(c->d.ctl, 1, c->stream);
+        c->old = c->cur;
+        c->wave_valid = false;
+    });
+}
+
+int rkdg_part_stage(rkdg_ctx* c, int32_t s) {
+    return guarded([&] {
+        if (!c || s < 0 || s >= c->p.rk) throw Error{RKDG_ERR_INVALID, "rkdg_part_stage: bad stage index"};
+        require_state(c);
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        const int out = stage_output(c, s);
+        launch_one_stage(c, s, c->cur, c->old, out, true, true);
+        c->cur = out;
+        c->wave_valid = (s == c->p.rk - 1);
+    });
+}
+
+int rkdg_part_limit(rkdg_ctx* c) {
+    return guarded([&] {
+        if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        require_state(c);
+        if (c->p.limiter != RKDG_LIMITER_TVB) throw Error{RKDG_ERR_INVALID, "context created without limiter"};
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        launch_tiled_limiter(c->tiles, 0, c->ld, c->d.U[c->cur], c->d.conn, c->d.lim, c->d.jinv,
+                             nullptr, c->d.far, kprec(c), c->p.nq, c->p.gamma, c->p.tvb_m,
+                             c->d.ctl, nullptr, nullptr, 0, c->stream);
+    });
+}
+
+int rkdg_part_time(rkdg_ctx* c, double* t, int32_t* steps, int32_t* done) {
+    return guarded([&] {
+        if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        pull_ctl(c);
+        check_error_flag(c);
+        if (t) *t = c->h_ctl->t;
+        if (steps) *steps = c->h_ctl->step;
+        if (done) *done = c->h_ctl->done;
+    });
+}
+
 int rkdg_sync(rkdg_ctx* c) {
     return guarded([&] {
         if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
@@ -616,13 +703,7 @@ int rkdg_stage(rkdg_ctx* c, int32_t s, double dt) {
         c->h_ctl->dt = dt;
         c->h_ctl->done = 0;
         push_ctl(c);
-        int out;
-        if (s == c->p.rk - 1 && s > 0 && c->old != c->cur) {
-            out = c->old;  // in place on U^n: each element reads its own U^n first
-        } else {
-            out = 0;
-            while (out == c->cur || out == c->old) ++out;
-        }
+        const int out = stage_output(c, s);
         launch_one_stage(c, s, c->cur, c->old, out);
         c->cur = out;
         // only a last stage leaves the CFL measure of the state it wrote

@@ -20,10 +20,20 @@ TVB limiter the halo means of each stage output are refreshed before
 rkdg_limit.  The transport is pluggable: `TorchTransport` uses
 torch.distributed point-to-point operations (NCCL between GPUs, gloo on the
 host), `LocalTransport` moves rows between parts held by one process.
+
+`DecomposedSolve.step` is the host-driven loop (each stage call and dt
+returns to the host; any part object with the DevicePart methods, the
+oracle's included).  `DecomposedSolve.advance_device` runs whole steps in
+stream order on the device parts: the halo transfers, an all-reduce of the
+CFL wave-speed maximum and the stages are enqueued on the parts' streams
+with no host round trip until the end (rkdg_part_wave, rkdg_part_begin_step,
+rkdg_part_stage, rkdg_part_limit).
 """
 from __future__ import annotations
 
 import numpy as np
+
+import ctypes as C
 
 from . import capi, meshgen
 
@@ -177,27 +187,91 @@ class DevicePart:
     def sync(self):
         capi.check(capi.lib().rkdg_sync(self.s.h))
 
+    # -- stream-ordered steps (advance_device)
+    def set_final_time(self, t_final: float):
+        capi.check(capi.lib().rkdg_part_set_final_time(self.s.h, float(t_final)))
+
+    def wave_out(self, buf):
+        """The part's CFL wave-speed maximum into buf (a one-element float64
+        device tensor), in stream order."""
+        capi.check(capi.lib().rkdg_part_wave(self.s.h, buf.data_ptr(), 0))
+
+    def wave_in(self, buf):
+        capi.check(capi.lib().rkdg_part_wave(self.s.h, buf.data_ptr(), 1))
+
+    def begin_step(self):
+        capi.check(capi.lib().rkdg_part_begin_step(self.s.h))
+
+    def stage_async(self, st: int):
+        capi.check(capi.lib().rkdg_part_stage(self.s.h, st))
+
+    def limit_async(self):
+        capi.check(capi.lib().rkdg_part_limit(self.s.h))
+
+    def time(self):
+        """(time, steps, done) after waiting for the part's stream."""
+        t, n, d = C.c_double(), C.c_int32(), C.c_int32()
+        capi.check(capi.lib().rkdg_part_time(self.s.h, C.byref(t), C.byref(n), C.byref(d)))
+        return t.value, n.value, bool(d.value)
+
     def close(self):
         self.s.close()
 
 
 class LocalTransport:
     """Every part held by this process: rows move between the parts'
-    buffers on one device, dt is the minimum over them."""
+    buffers on one device, dt is the minimum over them.  With sync=False
+    the parts' streams are ordered by events instead of host waits."""
 
-    def exchange(self, parts: dict, means_only: bool):
+    def exchange(self, parts: dict, means_only: bool, sync: bool = True):
         bufs = {}
+        done = {}
         for p, part in parts.items():
             for q in part.send:
                 bufs[(p, q)] = part.pack(q, means_only)
-            part.sync()
+            if sync:
+                part.sync()
+            elif hasattr(part, "stream"):
+                done[p] = _record(part.stream())
         for p, part in parts.items():
             for q in part.recv:
+                if not sync and q in done:
+                    part.stream().wait_event(done[q])
                 part.unpack(q, means_only, bufs[(q, p)])
-            part.sync()
+                if not sync and q in done:
+                    # the allocator may reuse a buffer only after both
+                    # streams have finished with it
+                    bufs[(q, p)].record_stream(parts[q].stream())
+                    bufs[(q, p)].record_stream(part.stream())
+            if sync:
+                part.sync()
 
     def min(self, x: float) -> float:
         return x
+
+    def max_device(self, parts: dict, bufs: dict):
+        """bufs[p] (one float64 each, written on part p's stream) all become
+        their maximum, in stream order."""
+        import torch
+
+        side = torch.cuda.current_stream()
+        for p, part in parts.items():
+            side.wait_event(_record(part.stream()))
+        with torch.cuda.stream(side):
+            m = torch.stack([bufs[p] for p in parts]).max(dim=0).values
+            for p in parts:
+                bufs[p].copy_(m)
+        ev = _record(side)
+        for part in parts.values():
+            part.stream().wait_event(ev)
+
+
+def _record(stream):
+    import torch
+
+    ev = torch.cuda.Event()
+    ev.record(stream)
+    return ev
 
 
 class TorchTransport:
@@ -212,7 +286,7 @@ class TorchTransport:
         self.dist = dist
         self.group = group
 
-    def exchange(self, parts: dict, means_only: bool):
+    def exchange(self, parts: dict, means_only: bool, sync: bool = True):
         import contextlib
 
         import torch
@@ -232,7 +306,17 @@ class TorchTransport:
                     w.wait()
             for q, buf in incoming.items():
                 part.unpack(q, means_only, buf)
-        part.sync()
+        if sync:
+            part.sync()
+
+    def max_device(self, parts: dict, bufs: dict):
+        """The one part's bufs[p] becomes the maximum over all ranks: an
+        all-reduce on the part's stream (NCCL keeps it in stream order)."""
+        import torch
+
+        (p, part), = parts.items()
+        with torch.cuda.stream(part.stream()):
+            self.dist.all_reduce(bufs[p], op=self.dist.ReduceOp.MAX, group=self.group)
 
     def min(self, x: float) -> float:
         import torch
@@ -278,3 +362,36 @@ class DecomposedSolve:
         for _ in range(nsteps):
             t += self.step()
         return t
+
+    def advance_device(self, nsteps: int, t_final: float = 0.0):
+        """nsteps steps (fewer once t_final > 0 is reached) in stream order
+        on device parts; returns (time, steps) of the solve.  Every part
+        forms dt = cfl / (the maximum of the parts' wave speeds), equal to
+        the minimum of their own CFL steps that `step` takes."""
+        import torch
+
+        parts = self.parts
+        bufs = {p: torch.zeros(1, dtype=torch.float64, device=part.send_device()) for p, part in parts.items()}
+        for part in parts.values():
+            part.set_final_time(t_final)
+        for _ in range(nsteps):
+            self.transport.exchange(parts, False, sync=False)
+            for p, part in parts.items():
+                part.wave_out(bufs[p])
+            self.transport.max_device(parts, bufs)
+            for p, part in parts.items():
+                part.wave_in(bufs[p])
+                part.begin_step()
+            for st in range(self.rk):
+                if st > 0:
+                    self.transport.exchange(parts, False, sync=False)
+                for part in parts.values():
+                    part.stage_async(st)
+                if self.limiter:
+                    self.transport.exchange(parts, True, sync=False)
+                    for part in parts.values():
+                        part.limit_async()
+        out = [part.time() for part in parts.values()]
+        for part in parts.values():
+            part.sync()
+        return out[0][0], out[0][1]

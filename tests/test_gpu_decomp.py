@@ -6,7 +6,10 @@ decomposed run matches the oracle and the single-context run to 1e-12 in
 FP64 (each part tiles its own elements, so interface fluxes are formed from
 the other side than in the single context: equal to rounding, not bit for
 bit), and the FP32C form stays within FP32 rounding of its single-context
-run.  Between GPUs the same loop moves the rows with NCCL
+run.  The stream-ordered loop (DecomposedSolve.advance_device: halo
+transfers, the wave-speed all-reduce and the stages enqueued with no host
+round trip) equals the host-driven loop and lands on a final time like the
+single context.  Between GPUs the same loops move the rows with NCCL
 (decomp.TorchTransport); the host tests cover that transport with gloo."""
 import ctypes as C
 
@@ -30,13 +33,16 @@ def solver_kw(kw, limiter, precision):
                 tvb_m=kw.get("tvb_m", 50.0), precision=precision)
 
 
-def decomposed(mesh, kw, limiter, U0, precision, nparts=3):
+def decomposed(mesh, kw, limiter, U0, precision, nparts=3, device_loop=False, t_final=0.0):
     P = Partition(mesh, nparts)
     parts = {p: DevicePart(P, p, **solver_kw(kw, limiter, precision)) for p in range(nparts)}
     for p, part in parts.items():
         part.set_state(P.split(U0, p))
     solve = DecomposedSolve(parts, LocalTransport(), rk=kw["rk"], limiter=limiter)
-    dts = [solve.step() for _ in range(NSTEPS)]
+    if device_loop:
+        dts = solve.advance_device(NSTEPS if t_final <= 0 else 10 ** 6, t_final=t_final)  # (t, steps)
+    else:
+        dts = [solve.step() for _ in range(NSTEPS)]
     U = P.join({p: part.state() for p, part in parts.items()})
     for part in parts.values():
         part.close()
@@ -61,6 +67,30 @@ def test_device_parts_match_oracle_and_single_context(kind):
     assert rel_err(U, ref) < 1e-12
     one, _ = single_context(mesh, kw, limiter, U0, "fp64")
     assert rel_err(U, one) < 1e-12
+
+
+@pytest.mark.parametrize("kind", ["vortex", "step"])
+def test_device_loop_equals_host_loop(kind):
+    """advance_device (no host round trip per step) against the host-driven
+    step loop: the same time and the same states (FP64)."""
+    mesh, kw, limiter, U0 = case(kind)
+    host, dts = decomposed(mesh, kw, limiter, U0, "fp64")
+    dev, (t, n) = decomposed(mesh, kw, limiter, U0, "fp64", device_loop=True)
+    assert n == NSTEPS
+    assert t == pytest.approx(sum(dts), rel=1e-13)
+    assert rel_err(dev, host) < 1e-12
+
+
+def test_device_loop_lands_on_final_time():
+    mesh, kw, limiter, U0 = case("vortex")
+    one = CUDARkdgSolver(mesh, **solver_kw(kw, limiter, "fp32"))
+    one.setFreedom(U0)
+    t1, n1 = one.advance(10 ** 6, t_final=0.05)
+    ref = one.copyFreedomToHost()
+    one.close()
+    dev, (t, n) = decomposed(mesh, kw, limiter, U0, "fp32", device_loop=True, t_final=0.05)
+    assert t == t1 == 0.05 and n == n1
+    assert rel_err(dev, ref) < 1e-5
 
 
 def test_fp32c_parts_track_single_context():
