@@ -539,21 +539,23 @@ def run_decomp(args, dist):
         for p, part in parts.items():
             part.set_state(P.split(U0, p), basis="native")
         solve = DecomposedSolve(parts, TorchTransport() if dist.world > 1 else LocalTransport(), rk=3)
-        solve.advance_device(W)
-        dist.barrier()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for part in parts.values():
-            part.stream().wait_event(e0)
-        solve.advance_device(K)  # returns once every part's stream has drained
-        e1.record()
-        torch.cuda.synchronize()
-        ms = dist.max(e0.elapsed_time(e1))
         halo = int(sum(P.halo[p].size for p in range(k)))
-        out["runs"].append({"parts": k, "ranks": dist.world, "dof_stage_per_s": T * 72 * K / (ms * 1e-3),
-                            "ms_per_step": ms / K, "halo_copies": halo,
-                            "vs_single_context": ms1 / ms})
+        # the enqueued loop, and (parts in one process) the captured step replayed
+        for graph in ([False, True] if dist.world == 1 else [False]):
+            solve.advance_device(W, graph=graph)
+            dist.barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for part in parts.values():
+                part.stream().wait_event(e0)
+            solve.advance_device(K, graph=graph)  # returns once every part's stream has drained
+            e1.record()
+            torch.cuda.synchronize()
+            ms = dist.max(e0.elapsed_time(e1))
+            out["runs"].append({"parts": k, "ranks": dist.world, "graph": graph,
+                                "dof_stage_per_s": T * 72 * K / (ms * 1e-3), "ms_per_step": ms / K,
+                                "halo_copies": halo, "vs_single_context": ms1 / ms})
         for part in parts.values():
             part.close()
     return out

@@ -137,11 +137,11 @@ class DevicePart:
         dev = torch.device("cuda", torch.cuda.current_device())
         self.send = {q: torch.tensor(v, device=dev) for q, v in partition.send[p].items()}
         self.recv = {q: torch.tensor(v, device=dev) for q, v in partition.recv[p].items()}
+        self._bufs = {}  # (q, incoming, means_only) -> exchange buffer, allocated once
+        self._stream = torch.cuda.ExternalStream(self.s.stream())
 
     def stream(self):
-        import torch
-
-        return torch.cuda.ExternalStream(self.s.stream())
+        return self._stream
 
     def set_state(self, U, basis="reference"):
         self.s.setFreedom(U, basis=basis)
@@ -162,10 +162,17 @@ class DevicePart:
         self.s.limit()
 
     def buffer(self, q: int, incoming: bool, means_only: bool):
+        """The exchange buffer for rows to (or from) part q: allocated on
+        first use and reused by every later exchange, so a captured step
+        replays on the same memory (the transports order the reuse)."""
         import torch
 
-        n = (self.recv if incoming else self.send)[q].numel()
-        return torch.empty((n, self.rows[means_only], 16), dtype=torch.uint8, device=self.send_device())
+        key = (q, incoming, means_only)
+        if key not in self._bufs:
+            n = (self.recv if incoming else self.send)[q].numel()
+            self._bufs[key] = torch.empty((n, self.rows[means_only], 16), dtype=torch.uint8,
+                                          device=self.send_device())
+        return self._bufs[key]
 
     def send_device(self):
         import torch
@@ -223,27 +230,36 @@ class LocalTransport:
     buffers on one device, dt is the minimum over them.  With sync=False
     the parts' streams are ordered by events instead of host waits."""
 
+    def __init__(self):
+        self._read = {}  # part -> event after its last unpacks (the senders' buffers are free again)
+
     def exchange(self, parts: dict, means_only: bool, sync: bool = True):
+        """Rows between the parts' buffers.  With sync=False no host waits:
+        each part packs on its stream once every receiver has read the
+        previous exchange's buffers, and unpacks once its senders have
+        packed (events between the streams)."""
+        dev = not sync and all(hasattr(part, "stream") for part in parts.values())
         bufs = {}
         done = {}
         for p, part in parts.items():
+            if dev:
+                for q in part.send:
+                    if q in self._read:
+                        part.stream().wait_event(self._read[q])
             for q in part.send:
                 bufs[(p, q)] = part.pack(q, means_only)
-            if sync:
-                part.sync()
-            elif hasattr(part, "stream"):
+            if dev:
                 done[p] = _record(part.stream())
+            elif sync:
+                part.sync()
         for p, part in parts.items():
             for q in part.recv:
-                if not sync and q in done:
+                if dev:
                     part.stream().wait_event(done[q])
                 part.unpack(q, means_only, bufs[(q, p)])
-                if not sync and q in done:
-                    # the allocator may reuse a buffer only after both
-                    # streams have finished with it
-                    bufs[(q, p)].record_stream(parts[q].stream())
-                    bufs[(q, p)].record_stream(part.stream())
-            if sync:
+            if dev:
+                self._read[p] = _record(part.stream())
+            elif sync:
                 part.sync()
 
     def min(self, x: float) -> float:
@@ -251,17 +267,19 @@ class LocalTransport:
 
     def max_device(self, parts: dict, bufs: dict):
         """bufs[p] (one float64 each, written on part p's stream) all become
-        their maximum, in stream order."""
+        their maximum, in stream order (on the first part's stream)."""
         import torch
 
-        side = torch.cuda.current_stream()
-        for p, part in parts.items():
-            side.wait_event(_record(part.stream()))
-        with torch.cuda.stream(side):
-            m = torch.stack([bufs[p] for p in parts]).max(dim=0).values
+        first = next(iter(parts.values())).stream()
+        for part in parts.values():
+            first.wait_event(_record(part.stream()))
+        with torch.cuda.stream(first):
+            m = bufs[next(iter(parts))]
+            for p in parts:
+                torch.maximum(m, bufs[p], out=m)
             for p in parts:
                 bufs[p].copy_(m)
-        ev = _record(side)
+        ev = _record(first)
         for part in parts.values():
             part.stream().wait_event(ev)
 
@@ -363,40 +381,101 @@ class DecomposedSolve:
             t += self.step()
         return t
 
-    def advance_device(self, nsteps: int, t_final: float = 0.0):
+    def _enqueue_device_step(self, bufs):
+        parts = self.parts
+        self.transport.exchange(parts, False, sync=False)
+        for p, part in parts.items():
+            part.wave_out(bufs[p])
+        self.transport.max_device(parts, bufs)
+        for p, part in parts.items():
+            part.wave_in(bufs[p])
+            part.begin_step()
+        for st in range(self.rk):
+            if st > 0:
+                self.transport.exchange(parts, False, sync=False)
+            for part in parts.values():
+                part.stage_async(st)
+            if self.limiter:
+                self.transport.exchange(parts, True, sync=False)
+                for part in parts.values():
+                    part.limit_async()
+
+    def advance_device(self, nsteps: int, t_final: float = 0.0, graph: bool = False):
         """nsteps steps (fewer once t_final > 0 is reached) in stream order
         on device parts; returns (time, steps) of the solve.  Every part
         forms dt = cfl / (the maximum of the parts' wave speeds), equal to
-        the minimum of their own CFL steps that `step` takes."""
+        the minimum of their own CFL steps that `step` takes.  With graph
+        (parts held by this process, LocalTransport), one step is captured
+        as a CUDA graph (the parts' streams forked from and joined to the
+        capturing stream) and replayed: one host call per step.  A whole
+        step returns the parts' buffer rotation to its start, so every
+        replay is the next step."""
         import torch
 
         parts = self.parts
-        bufs = {p: torch.zeros(1, dtype=torch.float64, device=part.send_device()) for p, part in parts.items()}
+        if graph and not isinstance(self.transport, LocalTransport):
+            raise ValueError("graph replay needs every part in this process (LocalTransport)")
+        if getattr(self, "_wave_bufs", None) is None:
+            self._wave_bufs = {p: torch.zeros(1, dtype=torch.float64, device=part.send_device())
+                               for p, part in parts.items()}
+        bufs = self._wave_bufs
         for part in parts.values():
             part.set_final_time(t_final)
+        cur = torch.cuda.current_stream()
+
+        def join_parts():  # the parts' streams wait for the replays so far
+            ev = _record(cur)
+            for part in parts.values():
+                part.stream().wait_event(ev)
+
+        g = None
         for n in range(nsteps):
             # with a final time, every 16 steps one host read of the
             # device-resident time ends the loop once the solve is done
             # (every part has the same time)
-            if t_final > 0 and n > 0 and n % 16 == 0 and next(iter(parts.values())).time()[2]:
-                break
-            self.transport.exchange(parts, False, sync=False)
-            for p, part in parts.items():
-                part.wave_out(bufs[p])
-            self.transport.max_device(parts, bufs)
-            for p, part in parts.items():
-                part.wave_in(bufs[p])
-                part.begin_step()
-            for st in range(self.rk):
-                if st > 0:
-                    self.transport.exchange(parts, False, sync=False)
-                for part in parts.values():
-                    part.stage_async(st)
-                if self.limiter:
-                    self.transport.exchange(parts, True, sync=False)
+            if t_final > 0 and n > 0 and n % 16 == 0:
+                if g is not None:
+                    join_parts()
+                if next(iter(parts.values())).time()[2]:
+                    break
+            if graph and n >= 1:  # the first step runs eagerly: buffers and the wave maximum exist
+                if g is None:
+                    g = self._capture(bufs)
                     for part in parts.values():
-                        part.limit_async()
+                        cur.wait_event(_record(part.stream()))
+                g.replay()
+            else:
+                self._enqueue_device_step(bufs)
+        if g is not None:
+            join_parts()
         out = [part.time() for part in parts.values()]
         for part in parts.values():
             part.sync()
         return out[0][0], out[0][1]
+
+    def _capture(self, bufs):
+        """One device step as a CUDA graph.  The parts' streams join the
+        capture through events from the capturing stream and rejoin it at
+        the end; the exchange buffers are the parts' persistent ones."""
+        import torch
+
+        parts = self.parts
+        if getattr(self, "_graph", None) is not None:
+            return self._graph
+        torch.cuda.synchronize()  # nothing in flight on the parts' streams while they join the capture
+        if isinstance(self.transport, LocalTransport):
+            self.transport._read = {}  # a capture may wait only on events recorded inside it
+        cap = torch.cuda.Stream()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=cap, capture_error_mode="thread_local"):
+            fork = _record(cap)
+            for part in parts.values():
+                part.stream().wait_event(fork)
+            self._enqueue_device_step(bufs)
+            for part in parts.values():
+                cap.wait_event(_record(part.stream()))
+        # events recorded inside the capture order only the graph's own work
+        if isinstance(self.transport, LocalTransport):
+            self.transport._read = {}
+        self._graph = g
+        return g
