@@ -397,9 +397,11 @@ def run_batched(args, dist, peak, peak_kind):
         clocks = cs.summary()
         value = dist.sum(dofs * 3 * K) / (ms * 1e-3)
         alg = sum(m.ntri * bytes_per_elem_stage(nb, prec) for m, nb in zip(meshes, nbs))
+        label = ("tiled_stage_kernel (one RK stage: the P2 tiles and the P1 tiles as two concurrent launches; "
+                 "time and bytes per stage)" if torder == 2 else
+                 "tiled_stage_kernel (P1+P2 tiles, one launch per stage)")
         roof = roofline(b.time_stage(0, 10), b.time_stage(1, 10), b.time_stage(2, 10), alg, peak, peak_kind,
-                        "tiled_stage_kernel (P1+P2 tiles, one launch per stage)",
-                        measured_traffic(f"tiled_stage_kernel_batched_{prec}.md")
+                        label, measured_traffic(f"tiled_stage_kernel_batched_{prec}.md")
                         if args.nsolves == 64 else None)
         e2e = None
         if not args.no_e2e:
