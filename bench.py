@@ -352,6 +352,13 @@ def measured_traffic(profile):
     return None
 
 
+def stage_times(obj, trials=3, reps=10):
+    """Event-timed mean launch time of each RK stage (reps back-to-back
+    launches on the solver's stream), the best of a few trials: the same
+    best-of convention as the measured HBM peak it is divided into."""
+    return [min(obj.time_stage(k, reps) for _ in range(trials)) for k in range(3)]
+
+
 def roofline(t0, t1, t2, alg_bytes, peak, peak_kind, kernel, traffic=None):
     t_avg = (t0 + t1 + t2) / 3.0  # SSP-RK3: stage 1 without U^n, stages 2-3 with; 3 adds the epilogue
     achieved = alg_bytes / (t_avg * 1e-3) / 1e9
@@ -360,6 +367,7 @@ def roofline(t0, t1, t2, alg_bytes, peak, peak_kind, kernel, traffic=None):
             "peak_kind": peak_kind,
             "ms_per_launch": {"stage_without_U0": round(t0, 5), "stage_with_U0": round(t1, 5),
                               "last_stage": round(t2, 5)},
+            "timing": "CUDA events: mean of 10 back-to-back launches per RK stage, best of 3 trials",
             "algorithmic_bytes_per_launch": alg_bytes}
 
 
@@ -400,7 +408,7 @@ def run_batched(args, dist, peak, peak_kind):
         label = ("tiled_stage_kernel (one RK stage: the P2 tiles and the P1 tiles as two concurrent launches; "
                  "time and bytes per stage)" if torder == 2 else
                  "tiled_stage_kernel (P1+P2 tiles, one launch per stage)")
-        roof = roofline(b.time_stage(0, 10), b.time_stage(1, 10), b.time_stage(2, 10), alg, peak, peak_kind,
+        roof = roofline(*stage_times(b), alg, peak, peak_kind,
                         label, measured_traffic(f"tiled_stage_kernel_batched_{prec}.md")
                         if args.nsolves == 64 else None)
         e2e = None
@@ -465,7 +473,7 @@ def run_plain(args, dist, peak, peak_kind, K):
         s.advance(args.warmup)
         ms = event_time(s.stream(), lambda: s.advance(K), dist)
         value = dist.sum(T * 24 * 3 * K) / (ms * 1e-3)
-        roof = roofline(s.time_stage(0, 10), s.time_stage(1, 10), s.time_stage(2, 10), T * bytes_per_elem_stage(6, prec),
+        roof = roofline(*stage_times(s), T * bytes_per_elem_stage(6, prec),
                         peak, peak_kind, "tiled_stage_kernel (P2)")
         e2e = None
         if not args.no_e2e:
@@ -602,7 +610,7 @@ def run_step(args, dist, peak, peak_kind):
             ms += event_time(s.stream(), lambda: box.update(r=s.advance(10 ** 8, t_final=tt)), dist)
             steps += box["r"][1]
             out[tt] = s.copyFreedomToHost(basis="native")[0, 0]
-        stage_ms = [s.time_stage(k, 10) for k in range(3)] if name in ("fp32", "fp32c", "fp64") else None
+        stage_ms = stage_times(s) if name in ("fp32", "fp32c", "fp64") else None
         s.close()
         res[name] = {"rho": out, "steps": steps, "ms": ms, "stage_ms": stage_ms}
 
