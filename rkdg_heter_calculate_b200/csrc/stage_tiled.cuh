@@ -106,19 +106,17 @@ __global__ void wait_selftest_kernel(uint64_t limit_ns, unsigned long long* out)
 }
 
 // Shared memory of one CTA: the work area (edge normals, edge codes, flux
-// tasks, own traces and means, and in FP64 the halo traces and means, as
-// 4-vectors), sized for the largest tile layout the kernel dispatches (P1
-// tiles of a mixed pack use a prefix), then the staging area.  The staging
-// area first receives the tile's own state rows by bulk copy (SROWS rows of
-// 16 bytes per element); once phase A has read them, the halo neighbours'
-// states by 16-byte gathers ([SROWS][hm] rows).  FP32 (HALO_IN_STAGING):
-// each halo thread overwrites its own neighbour's first NG (+1 with means)
-// rows with that neighbour's traces (and mean), which phase B reads, and the
-// next tile's rows are copied in after phase B; this keeps a CTA within the
-// shared memory of six per SM.  FP64 keeps the halo traces in the work area
-// and copies the next tile's rows in as soon as the halo states are read.
-// J^-1 and the edge codes are read per thread (L2 hits, prefetched with the
-// rows) while the rows arrive.
+// tasks, own traces and means, as 4-vectors), sized for the largest tile
+// layout the kernel dispatches (P1 tiles of a mixed pack use a prefix),
+// then the staging area.  The staging area first receives the tile's own
+// state rows by bulk copy (SROWS rows of 16 bytes per element); once phase A
+// has read them, the halo neighbours' states by 16-byte gathers ([SROWS][hm]
+// rows).  Each halo thread then overwrites its own neighbour's first rows
+// with that neighbour's traces (and mean: put_htr), which phase B reads, and
+// the next tile's rows are copied in after phase B.  This keeps an FP32 CTA
+// within the shared memory of six per SM (P2) and an FP64 one within that of
+// three (P2) or four (P1).  J^-1 and the edge codes are read per thread (L2
+// hits, prefetched with the rows) while the rows arrive.
 template <typename Real>
 struct alignas(16) Vec4 {
     Real x, y, z, w;
@@ -176,11 +174,9 @@ struct TiledSmem {
     static constexpr int NG = ORD == 1 ? 2 : 3;
     static constexpr int SROWS = (ORD == 1 ? 3 : 6) * (int)(sizeof(Real) / 4);
     static constexpr int MEANS = FLUX == RKDG_FLUX_LLF ? 1 : 0;
-    static constexpr bool HALO_IN_STAGING = sizeof(Real) == 4;
-    __host__ __device__ static constexpr size_t work(int hm) {
+    __host__ __device__ static constexpr size_t work(int) {
         return TiledLayout<Real, BT>::code_off + sizeof(int4) * BT + sizeof(uint16_t) * 3 * BT +
-               sizeof(Vec4<Real>) * ((size_t)3 * NG * BT + MEANS * BT +
-                                     (HALO_IN_STAGING ? 0 : (size_t)(NG + MEANS) * hm));
+               sizeof(Vec4<Real>) * ((size_t)3 * NG * BT + MEANS * BT);
     }
     __host__ __device__ static constexpr size_t stage_offset(int hm) { return (work(hm) + 127) / 128 * 128; }
     __host__ __device__ static constexpr size_t stage_rows(int hm) {
@@ -193,11 +189,13 @@ struct TiledSmem {
 // per SM for kernels with P2 tiles (80 registers; 128-element tiles at most
 // 37 KB of shared memory per CTA) and 32 for P1-only kernels (64 registers;
 // their tiles need about 27 KB, and the extra warps hide more of the tile
-// pipeline's latency: 11 % faster on the limited Mach-3 step); in FP64 8
-// (P2) and 12 (P1); whatever the tile size.
+// pipeline's latency: 11 % faster on the limited Mach-3 step); in FP64 12
+// (P2: 168 registers, about 100 B of spills per thread, 17 % faster than
+// 8 warps at 236 registers) and 16 (P1: 128 registers); whatever the tile
+// size.
 template <typename Real, int ORD, int BT>
 struct TiledOccupancy {
-    static constexpr int warps = sizeof(Real) == 8 ? (ORD == 1 ? 12 : 8) : (ORD == 1 ? 32 : 24);
+    static constexpr int warps = sizeof(Real) == 8 ? (ORD == 1 ? 16 : 12) : (ORD == 1 ? 32 : 24);
     static constexpr int value = warps * 32 / BT > 0 ? warps * 32 / BT : 1;
 };
 
@@ -247,6 +245,33 @@ __device__ __forceinline__ void stage_prefetch(const StageArgs& a, const TileArg
         const uintptr_t b = reinterpret_cast<uintptr_t>(ta.task + dd.z) & ~uintptr_t(15);
         const uintptr_t e = (reinterpret_cast<uintptr_t>(ta.task + dd.z + dd.w) + 15) & ~uintptr_t(15);
         bulk_prefetch_l2(reinterpret_cast<const void*>(b), (uint32_t)(e - b));
+    }
+}
+
+// A halo neighbour's trace (slot g < NG) or cell mean (slot NG) in the
+// staging area, over that neighbour's own staged state rows (entry h of the
+// [rows][HM] gather): FP32 one 16-byte row per slot (row g), FP64 two (rows
+// 2g and 2g + 1).  Each halo thread writes only its own entry, after it has
+// read the rows there.
+template <typename Real>
+__device__ __forceinline__ void put_htr(unsigned char* stg, int HM, int g, int h, const Real t[4]) {
+    if constexpr (sizeof(Real) == 8) {
+        double2* p = reinterpret_cast<double2*>(stg);
+        p[(2 * g) * HM + h] = make_double2(t[0], t[1]);
+        p[(2 * g + 1) * HM + h] = make_double2(t[2], t[3]);
+    } else {
+        reinterpret_cast<float4*>(stg)[g * HM + h] = make_float4(t[0], t[1], t[2], t[3]);
+    }
+}
+template <typename Real>
+__device__ __forceinline__ void get_htr(const unsigned char* stg, int HM, int g, int h, Real t[4]) {
+    if constexpr (sizeof(Real) == 8) {
+        const double2* p = reinterpret_cast<const double2*>(stg);
+        const double2 a = p[(2 * g) * HM + h], b = p[(2 * g + 1) * HM + h];
+        t[0] = a.x, t[1] = a.y, t[2] = b.x, t[3] = b.y;
+    } else {
+        const float4 a = reinterpret_cast<const float4*>(stg)[g * HM + h];
+        t[0] = a.x, t[1] = a.y, t[2] = a.z, t[3] = a.w;
     }
 }
 
@@ -359,11 +384,8 @@ __device__ __forceinline__ bool tile_stage(const StageArgs& a, const TileArgs& t
     V4* s_tr = reinterpret_cast<V4*>(s_task + 3 * BT);                     // [3][NG][BT] own traces
     constexpr int MEANS = FLUX == RKDG_FLUX_LLF ? 1 : 0;                   // LLF needs cell means
     V4* s_mean = s_tr + 3 * NG * BT;                                       // [BT] (LLF)
-    // halo traces [NG][HM] and means [HM]: FP32 in the staging rows (trace g
-    // of halo h in row g, entry h, of that neighbour's own staged state)
-    constexpr bool HALO_IN_STAGING = TiledSmem<Real, 3, FLUX, BT>::HALO_IN_STAGING;
-    V4* s_htr = HALO_IN_STAGING ? reinterpret_cast<V4*>(stg) : s_mean + MEANS * BT;
-    V4* s_hmean = s_htr + NG * HM;
+    // halo traces and means: in the staging rows, over each neighbour's own
+    // staged state (put_htr / get_htr)
     constexpr bool PK = sizeof(Real) == 4;  // FP32: lane-pair arithmetic, paired tables
     const Tab2& t2 = c_tab_f2[CFG];
     using SE = typename std::conditional<PK, float2, Real>::type;
@@ -540,7 +562,7 @@ __device__ __forceinline__ bool tile_stage(const StageArgs& a, const TileArgs& t
                         mfull[v] = un[0][v] + refv[v];
                         if constexpr (!DEV) un[0][v] = mfull[v];
                     }
-                    if constexpr (MEANS) put4(s_hmean + h, mfull);
+                    if constexpr (MEANS) put_htr<Real>(stg, HM, NG, h, mfull);
                 }
                 const int he = hh[r].y;
                 Real c0[4];
@@ -565,20 +587,16 @@ __device__ __forceinline__ bool tile_stage(const StageArgs& a, const TileArgs& t
                             t[v] = s;
                         }
                     }
-                    put4(s_htr + g * HM + h, t);
+                    put_htr<Real>(stg, HM, g, h, t);
                 }
             }
         }
     }
-    __syncthreads();  // halo traces complete (FP64: halo states read)
+    __syncthreads();  // halo traces complete
     int4 nd0 = make_int4(0, 0, 0, 0);
     if (tid == 0 && nxt < ntiles) {  // the CTA's next tile (only this thread reads its descriptor)
         nd0 = __ldg(ta.desc + 2 * nxt);
-        if constexpr (!HALO_IN_STAGING) {
-            fence_proxy_async();
-            stage_copy<Real, BT>(a, nd0, stg, bar);
-        }
-        stage_prefetch<Real, HALO_IN_STAGING>(a, ta, nd0, __ldg(ta.desc + 2 * nxt + 1));
+        stage_prefetch<Real, true>(a, ta, nd0, __ldg(ta.desc + 2 * nxt + 1));
     }
 
     // ------------------------------------------------------------ phase B
@@ -597,7 +615,8 @@ __device__ __forceinline__ bool tile_stage(const StageArgs& a, const TileArgs& t
             if constexpr (MEANS) {
                 get4(s_mean + le, mL);
                 if (kind == EDGE_BOUNDARY) ghost<Real>(se, mL, far, nx, ny, mR);
-                else get4(kind == EDGE_HALO ? s_hmean + idx : s_mean + idx, mR);
+                else if (kind == EDGE_HALO) get_htr<Real>(stg, HM, NG, idx, mR);
+                else get4(s_mean + idx, mR);
             }
             Real alpha = Real(0);
             if constexpr (FLUX == RKDG_FLUX_LLF) {
@@ -618,12 +637,12 @@ __device__ __forceinline__ bool tile_stage(const StageArgs& a, const TileArgs& t
                 get4(slot, uL);
                 // the neighbour's point NG-1-g on its edge se pairs with ours
                 // (src/kernelfunctions.cu:545-549)
-                V4* nslot = kind == EDGE_HALO ? s_htr + (NG - 1 - g) * HM + idx
-                                              : s_tr + (se * NG + NG - 1 - g) * BT + idx;
+                V4* nslot = s_tr + (se * NG + NG - 1 - g) * BT + idx;  // an in-tile neighbour's slot
                 if (kind == EDGE_BOUNDARY) {
                     if constexpr (DEV) ghost_dev<Real>(se, uL, rs, nx, ny, uR);
                     else ghost<Real>(se, uL, far, nx, ny, uR);
                 }
+                else if (kind == EDGE_HALO) get_htr<Real>(stg, HM, NG - 1 - g, idx, uR);
                 else get4(nslot, uR);
                 Real fh[4], fn[4];  // the flux out of this side and into the neighbour
                 if (FLUX == RKDG_FLUX_LLF) {
@@ -675,8 +694,8 @@ __device__ __forceinline__ bool tile_stage(const StageArgs& a, const TileArgs& t
             }
         }
     }
-    __syncthreads();  // fluxes complete; FP32: halo traces read, the staging area takes the next tile's rows
-    if (HALO_IN_STAGING && tid == 0 && nxt < ntiles) {
+    __syncthreads();  // fluxes complete, halo traces read: the staging area takes the next tile's rows
+    if (tid == 0 && nxt < ntiles) {
         fence_proxy_async();
         stage_copy<Real, BT>(a, nd0, stg, bar);
     }
@@ -888,8 +907,8 @@ __global__ void __launch_bounds__(BT, TiledOccupancy<Real, ORD, BT>::value)
     if (threadIdx.x == 0) {
         const int4 fd = __ldg(ta.desc + 2 * tile);
         stage_copy<Real, BT>(a, fd, stg, &s_bar);
-        // FP64 (two CTAs per SM) gains from the first tile's table prefetch,
-        // FP32 (six) loses
+        // the first tile's table prefetch: a gain for FP64 (measured at two
+        // CTAs per SM), a loss for FP32
         if constexpr (sizeof(Real) == 8) stage_prefetch<Real, false>(a, ta, fd, __ldg(ta.desc + 2 * tile + 1));
     }
     const double2* jinv2 = reinterpret_cast<const double2*>(a.jinv);
