@@ -161,9 +161,10 @@ __device__ __forceinline__ void acc_rows(float R[NB][4], const float f[4], const
 
 template <typename Real, int BT>
 struct TiledLayout {
-    // edge normals per element: FP32 (Nx, Ny) per edge, the length formed
-    // where used; FP64 (Nx, Ny, length)
-    static constexpr int NC = sizeof(Real) == 4 ? 2 : 3;
+    // edge normals per element: (Nx, Ny) per edge, the length formed where
+    // used (as it was formed when stored: the same bits); this keeps an FP64
+    // P2 CTA with the LLF means within the shared memory of three per SM
+    static constexpr int NC = 2;
     static constexpr size_t code_off = (sizeof(Real) * 3 * NC * BT + 15) / 16 * 16;
 };
 
@@ -346,7 +347,7 @@ __device__ __forceinline__ TilePre<Real> tile_pre(const StageArgs& a, const Tile
     // residual is accumulated scaled by 2 area (= 1 / det J^-1): the volume
     // term through 2 area J^-1 = (-N_1; -N_2), the surface term through the
     // table 2 w_g psi_i, and the factor det J^-1 applied once in the update.
-    Real* s_nrm = reinterpret_cast<Real*>(smem_raw);  // [3][NC][BT] Nx, Ny (, len)
+    Real* s_nrm = reinterpret_cast<Real*>(smem_raw);  // [3][NC][BT] Nx, Ny
     t.det = r0.x * r1.y - r0.y * r1.x;
     t.inv_area = (Real)(2.0 * t.det);
     // FP64 forms them in FP64; FP32 from the rounded J^-1 rows (a few ulp,
@@ -360,7 +361,6 @@ __device__ __forceinline__ TilePre<Real> tile_pre(const StageArgs& a, const Tile
         Nx[k] = cx[k] * area2, Ny[k] = cy[k] * area2;
         s_nrm[(NC * k + 0) * BT + tid] = Nx[k];
         s_nrm[(NC * k + 1) * BT + tid] = Ny[k];
-        if constexpr (NC == 3) s_nrm[(NC * k + 2) * BT + tid] = sqrt_(Nx[k] * Nx[k] + Ny[k] * Ny[k]);
     }
     t.j00 = -Nx[1], t.j01 = -Ny[1], t.j10 = -Nx[2], t.j11 = -Ny[2];
     return t;
@@ -378,14 +378,17 @@ __device__ __forceinline__ bool tile_stage(const StageArgs& a, const TileArgs& t
     const Tab<Real>& tb = tab<Real>(CFG);
     const int HM = ta.max_halo;
     constexpr int NC = TiledLayout<Real, BT>::NC;
-    Real* s_nrm = reinterpret_cast<Real*>(smem_raw);                       // [3][NC][BT] Nx, Ny (, len)
+    Real* s_nrm = reinterpret_cast<Real*>(smem_raw);                       // [3][NC][BT] Nx, Ny
     int4* s_code = reinterpret_cast<int4*>(smem_raw + TiledLayout<Real, BT>::code_off);  // [BT]
     uint16_t* s_task = reinterpret_cast<uint16_t*>(s_code + BT);           // [3 BT] flux tasks
     V4* s_tr = reinterpret_cast<V4*>(s_task + 3 * BT);                     // [3][NG][BT] own traces
     constexpr int MEANS = FLUX == RKDG_FLUX_LLF ? 1 : 0;                   // LLF needs cell means
     V4* s_mean = s_tr + 3 * NG * BT;                                       // [BT] (LLF)
     // halo traces and means: in the staging rows, over each neighbour's own
-    // staged state (put_htr / get_htr)
+    // staged state (put_htr / get_htr; FP32 also through these pointers,
+    // trace g of halo h in row g, entry h)
+    V4* s_htr = reinterpret_cast<V4*>(stg);
+    V4* s_hmean = s_htr + NG * HM;
     constexpr bool PK = sizeof(Real) == 4;  // FP32: lane-pair arithmetic, paired tables
     const Tab2& t2 = c_tab_f2[CFG];
     using SE = typename std::conditional<PK, float2, Real>::type;
@@ -608,13 +611,14 @@ __device__ __forceinline__ bool tile_stage(const StageArgs& a, const TileArgs& t
             const int kind = c & 3, se = (c >> 2) & 3, idx = c >> 4;
             // physical normal N (|N| = edge length) and unit normal of edge k
             const Real Nx = s_nrm[(NC * k + 0) * BT + le], Ny = s_nrm[(NC * k + 1) * BT + le];
-            const Real len = NC == 3 ? s_nrm[(NC * k + 2) * BT + le] : sqrt_(Nx * Nx + Ny * Ny);
+            const Real len = sqrt_(Nx * Nx + Ny * Ny);
             const Real il = rcp_(len);
             const Real nx = Nx * il, ny = Ny * il;
             Real mL[4], mR[4];
             if constexpr (MEANS) {
                 get4(s_mean + le, mL);
                 if (kind == EDGE_BOUNDARY) ghost<Real>(se, mL, far, nx, ny, mR);
+                else if constexpr (sizeof(Real) == 4) get4(kind == EDGE_HALO ? s_hmean + idx : s_mean + idx, mR);
                 else if (kind == EDGE_HALO) get_htr<Real>(stg, HM, NG, idx, mR);
                 else get4(s_mean + idx, mR);
             }
@@ -637,12 +641,13 @@ __device__ __forceinline__ bool tile_stage(const StageArgs& a, const TileArgs& t
                 get4(slot, uL);
                 // the neighbour's point NG-1-g on its edge se pairs with ours
                 // (src/kernelfunctions.cu:545-549)
-                V4* nslot = s_tr + (se * NG + NG - 1 - g) * BT + idx;  // an in-tile neighbour's slot
+                V4* nslot = sizeof(Real) == 4 && kind == EDGE_HALO ? s_htr + (NG - 1 - g) * HM + idx
+                                                                   : s_tr + (se * NG + NG - 1 - g) * BT + idx;
                 if (kind == EDGE_BOUNDARY) {
                     if constexpr (DEV) ghost_dev<Real>(se, uL, rs, nx, ny, uR);
                     else ghost<Real>(se, uL, far, nx, ny, uR);
                 }
-                else if (kind == EDGE_HALO) get_htr<Real>(stg, HM, NG - 1 - g, idx, uR);
+                else if (sizeof(Real) == 8 && kind == EDGE_HALO) get_htr<Real>(stg, HM, NG - 1 - g, idx, uR);
                 else get4(nslot, uR);
                 Real fh[4], fn[4];  // the flux out of this side and into the neighbour
                 if (FLUX == RKDG_FLUX_LLF) {
@@ -825,7 +830,7 @@ __device__ __forceinline__ bool tile_stage(const StageArgs& a, const TileArgs& t
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const Real Nx = s_nrm[(NC * k + 0) * BT + tid], Ny = s_nrm[(NC * k + 1) * BT + tid];
-                len[k] = NC == 3 ? s_nrm[(NC * k + 2) * BT + tid] : sqrt_(Nx * Nx + Ny * Ny);
+                len[k] = sqrt_(Nx * Nx + Ny * Ny);
             }
             wv = (Real)wave_of<Real>(m, gamma, len, inv_area, bad);
             if (bad) atomicOr(&ctl->error, 1);
