@@ -488,12 +488,17 @@ def run_plain(args, dist, peak, peak_kind, K):
             t = time.perf_counter()
             s.setFreedom(host)  # reference basis and layout
             s.set_time(0.0)
+            t1 = time.perf_counter()
             s.advance(K)
+            t2 = time.perf_counter()
             capi.check(capi.lib().rkdg_get_state(s.h, capi.dptr(res), T, capi.BASIS_REFERENCE))
-            wall = dist.max(time.perf_counter() - t)
+            t3 = time.perf_counter()
+            wall = dist.max(t3 - t)
             e2e = {"value": dist.sum(T * 24 * 3 * K) / wall, "unit": UNIT,
                    "h2d_bytes_per_step": host.nbytes / K, "d2h_bytes_per_step": host.nbytes / K,
-                   "timed": "set_state (pinned host, reference basis) + K steps + get_state"}
+                   "timed": "set_state (pinned host, reference basis) + K steps + get_state",
+                   "phases_ms": {"set_state": round((t1 - t) * 1e3, 2), "advance": round((t2 - t1) * 1e3, 2),
+                                 "get_state": round((t3 - t2) * 1e3, 2)}}
         acc = None
         if not args.no_accuracy:
             s.setFreedom(U0, basis="native")

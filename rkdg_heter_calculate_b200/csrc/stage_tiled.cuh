@@ -192,11 +192,14 @@ struct TiledSmem {
 // their tiles need about 27 KB, and the extra warps hide more of the tile
 // pipeline's latency: 11 % faster on the limited Mach-3 step); in FP64 12
 // (P2: 168 registers, about 100 B of spills per thread, 17 % faster than
-// 8 warps at 236 registers) and 16 (P1: 128 registers); whatever the tile
-// size.
-template <typename Real, int ORD, int BT>
+// 8 warps at 236 registers on large meshes) and 16 (P1: 128 registers);
+// whatever the tile size.  LAT (FP64 only): 8 and 12 warps without spills,
+// for launches whose tiles all fit on the device at once, where a tile's
+// latency rather than the throughput of many sets the time.
+template <typename Real, int ORD, int BT, int LAT = 0>
 struct TiledOccupancy {
-    static constexpr int warps = sizeof(Real) == 8 ? (ORD == 1 ? 16 : 12) : (ORD == 1 ? 32 : 24);
+    static constexpr int warps = sizeof(Real) == 8 ? (LAT ? (ORD == 1 ? 12 : 8) : (ORD == 1 ? 16 : 12))
+                                                   : (ORD == 1 ? 32 : 24);
     static constexpr int value = warps * 32 / BT > 0 ? warps * 32 / BT : 1;
 };
 
@@ -895,8 +898,8 @@ __device__ __forceinline__ void tile_maxima_atomic(const StageArgs& a, StepCtl* 
 // BT: elements per tile = threads per CTA.
 // A barrier wait that times out sets bit 1 of the solve's error word and
 // ends the CTA (all threads together).
-template <typename Real, int NQ2, int FLUX, int MODE, int ORD, int BT>
-__global__ void __launch_bounds__(BT, TiledOccupancy<Real, ORD, BT>::value)
+template <typename Real, int NQ2, int FLUX, int MODE, int ORD, int BT, int LAT = 0>
+__global__ void __launch_bounds__(BT, TiledOccupancy<Real, ORD, BT, LAT>::value)
     tiled_stage_kernel(const StageArgs a, const TileArgs ta) {
     using SM = TiledSmem<Real, ORD, FLUX, BT>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
