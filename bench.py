@@ -41,6 +41,8 @@ One JSON line on rank 0:
 from __future__ import annotations
 
 import argparse
+import contextlib
+import gc
 import json
 import math
 import os
@@ -324,6 +326,19 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
+@contextlib.contextmanager
+def no_gc():
+    """Python's cyclic collector paused over a timed region: a collection
+    over the bench's large heap would otherwise be timed as the library's."""
+    was = gc.isenabled()
+    gc.disable()
+    try:
+        yield
+    finally:
+        if was:
+            gc.enable()
+
+
 def event_time(stream_ptr, fn, dist):
     import torch
 
@@ -332,9 +347,10 @@ def event_time(stream_ptr, fn, dist):
     e1 = torch.cuda.Event(enable_timing=True)
     dist.barrier()
     torch.cuda.synchronize()
-    e0.record(st)
-    fn()
-    e1.record(st)
+    with no_gc():
+        e0.record(st)
+        fn()
+        e1.record(st)
     torch.cuda.synchronize()
     dist.barrier()
     return dist.max(e0.elapsed_time(e1))
@@ -419,14 +435,16 @@ def run_batched(args, dist, peak, peak_kind):
                 b.set_state(i, h)
             b.advance(2)
             dist.barrier()
-            t = time.perf_counter()
-            for i, (_, h) in enumerate(hosts):
-                capi.check(capi.lib().rkdg_batch_set_state(b.h, i, capi.dptr(h), h.shape[2]))
-                b.set_time(i, 0.0)
-            b.advance(K)
-            for i, (_, h) in enumerate(outs):
-                capi.check(capi.lib().rkdg_batch_get_state(b.h, i, capi.dptr(h), h.shape[2]))
-            wall = dist.max(time.perf_counter() - t)
+            with no_gc():
+                t = time.perf_counter()
+                for i, (_, h) in enumerate(hosts):
+                    capi.check(capi.lib().rkdg_batch_set_state(b.h, i, capi.dptr(h), h.shape[2]))
+                    b.set_time(i, 0.0)
+                b.advance(K)
+                for i, (_, h) in enumerate(outs):
+                    capi.check(capi.lib().rkdg_batch_get_state(b.h, i, capi.dptr(h), h.shape[2]))
+                wall = time.perf_counter() - t
+            wall = dist.max(wall)
             nbytes = sum(h.nbytes for _, h in hosts)
             e2e = {"value": dist.sum(dofs * 3 * K) / wall, "unit": UNIT,
                    "h2d_bytes_per_step": nbytes / K, "d2h_bytes_per_step": nbytes / K,
@@ -485,14 +503,15 @@ def run_plain(args, dist, peak, peak_kind, K):
             s.advance(2)
             s.copyFreedomToHost()
             dist.barrier()
-            t = time.perf_counter()
-            s.setFreedom(host)  # reference basis and layout
-            s.set_time(0.0)
-            t1 = time.perf_counter()
-            s.advance(K)
-            t2 = time.perf_counter()
-            capi.check(capi.lib().rkdg_get_state(s.h, capi.dptr(res), T, capi.BASIS_REFERENCE))
-            t3 = time.perf_counter()
+            with no_gc():
+                t = time.perf_counter()
+                s.setFreedom(host)  # reference basis and layout
+                s.set_time(0.0)
+                t1 = time.perf_counter()
+                s.advance(K)
+                t2 = time.perf_counter()
+                capi.check(capi.lib().rkdg_get_state(s.h, capi.dptr(res), T, capi.BASIS_REFERENCE))
+                t3 = time.perf_counter()
             wall = dist.max(t3 - t)
             e2e = {"value": dist.sum(T * 24 * 3 * K) / wall, "unit": UNIT,
                    "h2d_bytes_per_step": host.nbytes / K, "d2h_bytes_per_step": host.nbytes / K,
