@@ -1140,8 +1140,8 @@ void launch_tiled(const StageArgs& a, const TileArgs& t, int ctas, cudaStream_t 
 // Tile sizes the stage kernel is built for: 128 everywhere, 256 for the
 // stage (not the residual) kernels the batch autotuner may pick.  FP64
 // launches of one CTA per tile whose tiles all fit on the device at once
-// run the latency form (fewer warps per SM, no register spills: a 28,800-
-// triangle P2 mesh steps 25 % faster than in the throughput form).
+// run the latency form (fewer warps per SM, no register spills: 3,200- and
+// 28,800-triangle P2 meshes step 3-4 % faster than in the throughput form).
 template <typename Real, int NQ2, int FLUX, int MODE, int ORD>
 void launch_tiled_bt(const StageArgs& a, const TileArgs& t, int ctas, cudaStream_t s) {
     if (t.tile == 128) {
