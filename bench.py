@@ -572,10 +572,15 @@ def run_decomp(args, dist):
         parts = {p: DevicePart(P, p, **kw) for p in mine}
         for p, part in parts.items():
             part.set_state(P.split(U0, p), basis="native")
-        solve = DecomposedSolve(parts, TorchTransport() if dist.world > 1 else LocalTransport(), rk=3)
         halo = int(sum(P.halo[p].size for p in range(k)))
-        # the enqueued loop, and (parts in one process) the captured step replayed
-        for graph in ([False, True] if dist.world == 1 else [False]):
+        # the enqueued loop, and (parts in one process) the captured step
+        # replayed, with each stage's transfers beside its interior tiles
+        # (overlap) or before the whole stage
+        shapes = ([(False, False), (True, False), (True, True)] if dist.world == 1 else
+                  [(False, True), (False, False)])
+        for graph, overlap in shapes:
+            solve = DecomposedSolve(parts, TorchTransport() if dist.world > 1 else LocalTransport(), rk=3,
+                                    overlap=overlap)
             solve.advance_device(W, graph=graph)
             dist.barrier()
             torch.cuda.synchronize()
@@ -587,7 +592,7 @@ def run_decomp(args, dist):
             e1.record()
             torch.cuda.synchronize()
             ms = dist.max(e0.elapsed_time(e1))
-            out["runs"].append({"parts": k, "ranks": dist.world, "graph": graph,
+            out["runs"].append({"parts": k, "ranks": dist.world, "graph": graph, "overlap": overlap,
                                 "dof_stage_per_s": T * 72 * K / (ms * 1e-3), "ms_per_step": ms / K,
                                 "halo_copies": halo, "vs_single_context": ms1 / ms})
         for part in parts.values():

@@ -267,6 +267,17 @@ int rkdg_part_set_final_time(rkdg_ctx* ctx, double t_final);
 int rkdg_part_wave(rkdg_ctx* ctx, double* d_wave, int32_t to_context);
 int rkdg_part_begin_step(rkdg_ctx* ctx);
 int rkdg_part_stage(rkdg_ctx* ctx, int32_t stage);
+/* The same stage in two halves, so that the halo refresh overlaps work:
+ * rkdg_part_stage_begin launches the partition's tiles that read no halo
+ * copy (they need only the owned elements' current state), and
+ * rkdg_part_stage_end, once the halo copies are current, the rest, which
+ * completes the stage.  Per stage: start the transfers (gather, send and
+ * receive), begin, finish the transfers (scatter), end.  The result equals
+ * rkdg_part_stage's bit for bit.  The reference exchanges the whole
+ * interface through the host before each stage and then runs every
+ * element (src/rkdgadvance.cpp:287-409). */
+int rkdg_part_stage_begin(rkdg_ctx* ctx, int32_t stage);
+int rkdg_part_stage_end(rkdg_ctx* ctx, int32_t stage);
 int rkdg_part_limit(rkdg_ctx* ctx);
 /* Waits, reports flagged errors, and returns the time, the step count and
  * whether the final time has been reached (any pointer may be NULL). */

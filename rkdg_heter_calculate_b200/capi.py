@@ -121,6 +121,8 @@ def lib():
             "rkdg_part_wave": (C.c_int, [vp, vp, C.c_int32]),
             "rkdg_part_begin_step": (C.c_int, [vp]),
             "rkdg_part_stage": (C.c_int, [vp, C.c_int32]),
+            "rkdg_part_stage_begin": (C.c_int, [vp, C.c_int32]),
+            "rkdg_part_stage_end": (C.c_int, [vp, C.c_int32]),
             "rkdg_part_limit": (C.c_int, [vp]),
             "rkdg_part_time": (C.c_int, [vp, _dp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
             "rkdg_server_status": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),

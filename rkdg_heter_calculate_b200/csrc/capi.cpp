@@ -45,6 +45,9 @@ struct rkdg_ctx {
     StepCtl* h_ctl = nullptr;  // pinned mirror of the device control block
     TileArgs tiles{};
     int ctas = 0;     // tiled grid size (0: one CTA per tile)
+    int n_int_tiles = 0;     // a partition's tiles that read no halo copy (they come first)
+    int pending_stage = -1;  // rkdg_part_stage_begin's stage until rkdg_part_stage_end
+    int pending_out = -1;
     std::unique_ptr<std::ofstream> reslog;  // residual history file (rkdg_set_residual_log)
     bool graph_monitor = false;  // the captured step forms the residual monitor
 };
@@ -250,6 +253,24 @@ int stage_output(const rkdg_ctx* c, int s) {
     return out;
 }
 
+// Stage s of a partition over its tiles [first, last) of the list (the
+// interior tiles come first), writing buffer out; the limiter is left to
+// the caller (rkdg_part_limit), as in rkdg_part_stage.
+void launch_part_tiles(rkdg_ctx* c, int s, int out, int first, int last) {
+    if (last <= first) return;
+    StageArgs a = base_args(c);
+    stage_coeffs(c->p.rk, s, a.a, a.b);
+    a.U = c->d.U[c->cur];
+    a.U0 = s == 0 ? nullptr : c->d.U[c->old];
+    a.Unew = c->d.U[out];
+    a.last_stage = s == c->p.rk - 1;
+    a.monitor = 1;
+    TileArgs t = c->tiles;
+    t.desc = c->tiles.desc + 2 * (size_t)first;
+    t.ntiles = last - first;
+    launch_stage(a, t, c->p.order, c->p.nq, c->p.flux, kprec(c), c->ctas, c->stream);
+}
+
 // One line of the residual history for the step just taken (the control
 // block on the host is current): the step number and log10 of the largest
 // cell-mean density change over the step relative to the far-field density.
@@ -399,6 +420,23 @@ int create_ctx(const rkdg_mesh_desc* mesh, const rkdg_params* params, int32_t n_
         }
         {
             TileTables tt = build_tiles(c->mesh, 0, 0, params->order, 0, 0, c->T_own);
+            c->n_int_tiles = tt.ntiles;
+            if (c->T_own < c->T) {
+                // a partition: the tiles none of whose halo entries is a halo
+                // copy first (they can run while the copies are refreshed),
+                // then the rest; a tile's arithmetic does not depend on its
+                // place in the list
+                std::vector<int32_t> inner, outer;
+                for (int t = 0; t < tt.ntiles; ++t) {
+                    const int32_t* d = &tt.desc[8 * (size_t)t];
+                    bool reads_copy = false;
+                    for (int h = 0; h < d[5] && !reads_copy; ++h) reads_copy = tt.halo[2 * (size_t)(d[4] + h)] >= c->T_own;
+                    (reads_copy ? outer : inner).insert((reads_copy ? outer : inner).end(), d, d + 8);
+                }
+                c->n_int_tiles = (int)(inner.size() / 8);
+                inner.insert(inner.end(), outer.begin(), outer.end());
+                tt.desc.swap(inner);
+            }
             c->d.tcode = (int4*)dev_alloc(c, sizeof(int32_t) * tt.code.size());
             c->d.tdesc = (int4*)dev_alloc(c, sizeof(int32_t) * tt.desc.size());
             c->d.halo = (int2*)dev_alloc(c, sizeof(int32_t) * std::max<size_t>(2, tt.halo.size()) + kTablePad);
@@ -531,6 +569,32 @@ int rkdg_part_stage(rkdg_ctx* c, int32_t s) {
         RKDG_CUDA_TRY(cudaSetDevice(c->device));
         const int out = stage_output(c, s);
         launch_one_stage(c, s, c->cur, c->old, out, true, true);
+        c->cur = out;
+        c->wave_valid = (s == c->p.rk - 1);
+    });
+}
+
+int rkdg_part_stage_begin(rkdg_ctx* c, int32_t s) {
+    return guarded([&] {
+        if (!c || s < 0 || s >= c->p.rk) throw Error{RKDG_ERR_INVALID, "rkdg_part_stage_begin: bad stage index"};
+        require_state(c);
+        if (c->pending_stage >= 0) throw Error{RKDG_ERR_STATE, "rkdg_part_stage_begin: a stage is already open"};
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        const int out = stage_output(c, s);
+        launch_part_tiles(c, s, out, 0, c->n_int_tiles);
+        c->pending_stage = s;
+        c->pending_out = out;
+    });
+}
+
+int rkdg_part_stage_end(rkdg_ctx* c, int32_t s) {
+    return guarded([&] {
+        if (!c || s != c->pending_stage)
+            throw Error{RKDG_ERR_STATE, "rkdg_part_stage_end: not the stage rkdg_part_stage_begin opened"};
+        RKDG_CUDA_TRY(cudaSetDevice(c->device));
+        const int out = c->pending_out;
+        c->pending_stage = -1;
+        launch_part_tiles(c, s, out, c->n_int_tiles, c->tiles.ntiles);
         c->cur = out;
         c->wave_valid = (s == c->p.rk - 1);
     });

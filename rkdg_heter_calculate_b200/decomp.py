@@ -212,6 +212,14 @@ class DevicePart:
     def stage_async(self, st: int):
         capi.check(capi.lib().rkdg_part_stage(self.s.h, st))
 
+    def stage_begin(self, st: int):
+        """The tiles that read no halo copy (may run while the copies are
+        being refreshed)."""
+        capi.check(capi.lib().rkdg_part_stage_begin(self.s.h, st))
+
+    def stage_end(self, st: int):
+        capi.check(capi.lib().rkdg_part_stage_end(self.s.h, st))
+
     def limit_async(self):
         capi.check(capi.lib().rkdg_part_limit(self.s.h))
 
@@ -238,6 +246,10 @@ class LocalTransport:
         each part packs on its stream once every receiver has read the
         previous exchange's buffers, and unpacks once its senders have
         packed (events between the streams)."""
+        self.exchange_end(parts, means_only, self.exchange_begin(parts, means_only, sync), sync)
+
+    def exchange_begin(self, parts: dict, means_only: bool, sync: bool = False):
+        """The packing half of an exchange; returns what exchange_end takes."""
         dev = not sync and all(hasattr(part, "stream") for part in parts.values())
         bufs = {}
         done = {}
@@ -252,6 +264,11 @@ class LocalTransport:
                 done[p] = _record(part.stream())
             elif sync:
                 part.sync()
+        return bufs, done, dev
+
+    def exchange_end(self, parts: dict, means_only: bool, pending, sync: bool = False):
+        """The unpacking half: every part's halo rows written."""
+        bufs, done, dev = pending
         for p, part in parts.items():
             for q in part.recv:
                 if dev:
@@ -305,13 +322,21 @@ class TorchTransport:
         self.group = group
 
     def exchange(self, parts: dict, means_only: bool, sync: bool = True):
+        self.exchange_end(parts, means_only, self.exchange_begin(parts, means_only, sync), sync)
+
+    def _stream_ctx(self, part):
         import contextlib
 
         import torch
 
+        return torch.cuda.stream(part.stream()) if hasattr(part, "stream") else contextlib.nullcontext()
+
+    def exchange_begin(self, parts: dict, means_only: bool, sync: bool = False):
+        """Packs this rank's rows and starts the batch of sends and receives
+        (on the part's stream: NCCL runs them beside what the stream does
+        next); returns what exchange_end takes."""
         (p, part), = parts.items()
-        ctx = torch.cuda.stream(part.stream()) if hasattr(part, "stream") else contextlib.nullcontext()
-        with ctx:
+        with self._stream_ctx(part):
             ops, incoming = [], {}
             for q in sorted(set(part.send) | set(part.recv)):
                 if q in part.send:
@@ -319,9 +344,17 @@ class TorchTransport:
                 if q in part.recv:
                     incoming[q] = part.buffer(q, True, means_only)
                     ops.append(self.dist.P2POp(self.dist.irecv, incoming[q], q, self.group))
-            if ops:
-                for w in self.dist.batch_isend_irecv(ops):
-                    w.wait()
+            works = self.dist.batch_isend_irecv(ops) if ops else []
+        return works, incoming
+
+    def exchange_end(self, parts: dict, means_only: bool, pending, sync: bool = False):
+        """Waits for the transfers (the part's stream waits, not the host)
+        and writes the received rows into the halo copies."""
+        (p, part), = parts.items()
+        works, incoming = pending
+        with self._stream_ctx(part):
+            for w in works:
+                w.wait()
             for q, buf in incoming.items():
                 part.unpack(q, means_only, buf)
         if sync:
@@ -349,13 +382,19 @@ class DecomposedSolve:
     """The time loop over the parts this process holds ({part: DevicePart}
     or any object with the same methods), with halo exchanges through
     `transport`.  Every process takes the same exchange and reduction steps
-    in the same order."""
+    in the same order.  overlap (the device loop): run each stage's halo
+    transfers beside the tiles that need no halo copy; by default on for
+    transfers between devices (TorchTransport), off for parts that share a
+    device, where the rows move by kernels on that device and the second
+    launch per stage costs more than it hides (measured on one B200: 0.357
+    against 0.342 ms per step with two parts of a 980,000-triangle mesh)."""
 
-    def __init__(self, parts: dict, transport, rk: int = 3, limiter: bool = False):
+    def __init__(self, parts: dict, transport, rk: int = 3, limiter: bool = False, overlap=None):
         self.parts = parts
         self.transport = transport
         self.rk = rk
         self.limiter = limiter
+        self.overlap = isinstance(transport, TorchTransport) if overlap is None else bool(overlap)
 
     def step(self) -> float:
         # halo copies current (so every part's dt sees true neighbour
@@ -382,21 +421,45 @@ class DecomposedSolve:
         return t
 
     def _enqueue_device_step(self, bufs):
-        parts = self.parts
-        self.transport.exchange(parts, False, sync=False)
-        for p, part in parts.items():
-            part.wave_out(bufs[p])
-        self.transport.max_device(parts, bufs)
-        for p, part in parts.items():
-            part.wave_in(bufs[p])
-            part.begin_step()
+        """One step in stream order.  With overlap, each stage's halo
+        refresh runs beside the tiles that read no halo copy: start the
+        transfers, launch those tiles, finish the transfers, launch the
+        rest (two launches per stage instead of one)."""
+        parts, tr = self.parts, self.transport
+        if not self.overlap:
+            tr.exchange(parts, False, sync=False)
+            for p, part in parts.items():
+                part.wave_out(bufs[p])
+            tr.max_device(parts, bufs)
+            for p, part in parts.items():
+                part.wave_in(bufs[p])
+                part.begin_step()
+            for st in range(self.rk):
+                if st > 0:
+                    tr.exchange(parts, False, sync=False)
+                for part in parts.values():
+                    part.stage_async(st)
+                if self.limiter:
+                    tr.exchange(parts, True, sync=False)
+                    for part in parts.values():
+                        part.limit_async()
+            return
         for st in range(self.rk):
-            if st > 0:
-                self.transport.exchange(parts, False, sync=False)
+            pending = tr.exchange_begin(parts, False)
+            if st == 0:  # the step's dt from the state at its start (owned elements)
+                for p, part in parts.items():
+                    part.wave_out(bufs[p])
+                tr.max_device(parts, bufs)
+                for p, part in parts.items():
+                    part.wave_in(bufs[p])
+                    part.begin_step()
             for part in parts.values():
-                part.stage_async(st)
+                part.stage_begin(st)
+            tr.exchange_end(parts, False, pending)
+            for part in parts.values():
+                part.stage_end(st)
             if self.limiter:
-                self.transport.exchange(parts, True, sync=False)
+                tr.exchange(parts, True, sync=False)
                 for part in parts.values():
                     part.limit_async()
 

@@ -33,12 +33,13 @@ def solver_kw(kw, limiter, precision):
                 tvb_m=kw.get("tvb_m", 50.0), precision=precision)
 
 
-def decomposed(mesh, kw, limiter, U0, precision, nparts=3, device_loop=False, t_final=0.0, graph=False):
+def decomposed(mesh, kw, limiter, U0, precision, nparts=3, device_loop=False, t_final=0.0, graph=False,
+               overlap=None):
     P = Partition(mesh, nparts)
     parts = {p: DevicePart(P, p, **solver_kw(kw, limiter, precision)) for p in range(nparts)}
     for p, part in parts.items():
         part.set_state(P.split(U0, p))
-    solve = DecomposedSolve(parts, LocalTransport(), rk=kw["rk"], limiter=limiter)
+    solve = DecomposedSolve(parts, LocalTransport(), rk=kw["rk"], limiter=limiter, overlap=overlap)
     if device_loop:
         dts = solve.advance_device(NSTEPS if t_final <= 0 else 10 ** 6, t_final=t_final, graph=graph)  # (t, steps)
     else:
@@ -69,27 +70,68 @@ def test_device_parts_match_oracle_and_single_context(kind):
     assert rel_err(U, one) < 1e-12
 
 
-@pytest.mark.parametrize("kind", ["vortex", "step"])
-def test_device_loop_equals_host_loop(kind):
-    """advance_device (no host round trip per step) against the host-driven
-    step loop: the same time and the same states (FP64)."""
+@pytest.mark.parametrize("kind,overlap", [("vortex", False), ("step", False), ("vortex", True), ("step", True)])
+def test_device_loop_equals_host_loop(kind, overlap):
+    """advance_device (no host round trip per step; with overlap, each
+    stage's halo transfers beside its interior tiles) against the
+    host-driven step loop: the same time and the same states (FP64)."""
     mesh, kw, limiter, U0 = case(kind)
     host, dts = decomposed(mesh, kw, limiter, U0, "fp64")
-    dev, (t, n) = decomposed(mesh, kw, limiter, U0, "fp64", device_loop=True)
+    dev, (t, n) = decomposed(mesh, kw, limiter, U0, "fp64", device_loop=True, overlap=overlap)
     assert n == NSTEPS
     assert t == pytest.approx(sum(dts), rel=1e-13)
     assert rel_err(dev, host) < 1e-12
 
 
-@pytest.mark.parametrize("kind", ["vortex", "step"])
-def test_graph_replay_equals_device_loop(kind):
+@pytest.mark.parametrize("kind,overlap", [("vortex", False), ("step", False), ("step", True)])
+def test_graph_replay_equals_device_loop(kind, overlap):
     """One decomposed step captured as a CUDA graph and replayed: the same
     bits as the enqueued loop."""
     mesh, kw, limiter, U0 = case(kind)
-    a, (ta, na) = decomposed(mesh, kw, limiter, U0, "fp32", device_loop=True)
-    b, (tb, nb) = decomposed(mesh, kw, limiter, U0, "fp32", device_loop=True, graph=True)
+    a, (ta, na) = decomposed(mesh, kw, limiter, U0, "fp32", device_loop=True, overlap=overlap)
+    b, (tb, nb) = decomposed(mesh, kw, limiter, U0, "fp32", device_loop=True, graph=True, overlap=overlap)
     assert (ta, na) == (tb, nb)
     np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("kind", ["vortex", "step"])
+def test_split_stage_equals_whole_stage(kind):
+    """rkdg_part_stage_begin + rkdg_part_stage_end (the tiles that read no
+    halo copy, then the rest) give the bits of rkdg_part_stage."""
+    mesh, kw, limiter, U0 = case(kind)
+    P = Partition(mesh, 3)
+    out = []
+    for split in (False, True):
+        parts = {p: DevicePart(P, p, **solver_kw(kw, limiter, "fp64")) for p in range(3)}
+        for p, part in parts.items():
+            part.set_state(P.split(U0, p))
+        tr = LocalTransport()
+        bufs = {p: torch.zeros(1, dtype=torch.float64, device="cuda") for p in parts}
+        for _ in range(2):
+            tr.exchange(parts, False)
+            for p, part in parts.items():
+                part.wave_out(bufs[p])
+            tr.max_device(parts, bufs)
+            for p, part in parts.items():
+                part.wave_in(bufs[p])
+                part.begin_step()
+            for st in range(kw["rk"]):
+                if st > 0:
+                    tr.exchange(parts, False)
+                for part in parts.values():
+                    if split:
+                        part.stage_begin(st)
+                        part.stage_end(st)
+                    else:
+                        part.stage_async(st)
+                if limiter:
+                    tr.exchange(parts, True)
+                    for part in parts.values():
+                        part.limit_async()
+        out.append(P.join({p: part.state() for p, part in parts.items()}))
+        for part in parts.values():
+            part.close()
+    np.testing.assert_array_equal(out[0], out[1])
 
 
 def test_device_loop_lands_on_final_time():
