@@ -555,6 +555,7 @@ int rkdg_part_begin_step(rkdg_ctx* c) {
         if (!c) throw Error{RKDG_ERR_INVALID, "null context"};
         require_state(c);
         if (!c->wave_valid) throw Error{RKDG_ERR_STATE, "rkdg_part_begin_step: no wave-speed maximum (rkdg_part_wave)"};
+        if (c->pending_stage >= 0) throw Error{RKDG_ERR_STATE, "rkdg_part_begin_step: a stage is still open"};
         RKDG_CUDA_TRY(cudaSetDevice(c->device));
         launch_step_begin(c->d.ctl, 1, c->stream);
         c->old = c->cur;
@@ -566,6 +567,7 @@ int rkdg_part_stage(rkdg_ctx* c, int32_t s) {
     return guarded([&] {
         if (!c || s < 0 || s >= c->p.rk) throw Error{RKDG_ERR_INVALID, "rkdg_part_stage: bad stage index"};
         require_state(c);
+        if (c->pending_stage >= 0) throw Error{RKDG_ERR_STATE, "rkdg_part_stage: a stage is still open"};
         RKDG_CUDA_TRY(cudaSetDevice(c->device));
         const int out = stage_output(c, s);
         launch_one_stage(c, s, c->cur, c->old, out, true, true);
@@ -665,6 +667,7 @@ int rkdg_set_state(rkdg_ctx* c, const double* U, int32_t ld, int32_t basis) {
                                         c->stream));
         c->cur = 0;
         c->old = 0;
+        c->pending_stage = -1;
         launch_import(c->T, c->ld, c->d.staging, c->T,
                       basis == RKDG_BASIS_REFERENCE ? c->d.conv_in : nullptr, c->d.perm, c->d.U[0],
                       c->p.order, kprec(c), c->p.farfield, lo_row(c), c->stream);
